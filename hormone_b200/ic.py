@@ -1,0 +1,213 @@
+"""Initial conditions (host side), returned as primitive arrays.
+
+Each function returns a dict of interior arrays with shape (nz, ny, nx)
+(x fastest, as HORMONE's Fortran arrays are laid out) for d, p, v1..3,
+b1..3 and phi.  The conversion to total energy is done by ``to_state``
+exactly as src/main/initialcondition.f90:132-141 does it.
+
+Transcendentals are evaluated with Python's ``math`` module (the C library,
+one call per distinct argument) so that values match a Fortran build that
+calls the same library.
+"""
+from __future__ import annotations
+
+import math
+from typing import Dict
+
+import numpy as np
+
+from .grid import centres
+
+PI = math.acos(-1.0)  # src/main/modules.f90:86
+
+
+def _zeros(cfg):
+    n = cfg["n"]
+    return np.zeros((n[2], n[1], n[0]), dtype=np.float64)
+
+
+def _blank(cfg) -> Dict[str, np.ndarray]:
+    return {k: _zeros(cfg) for k in ("d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi")}
+
+
+def shocktube(cfg, grid) -> Dict[str, np.ndarray]:
+    """src/init/shocktube.f90:14-192 for sodshock_* and briowushock_*."""
+    st = cfg["simtype"]
+    direction = {"x": 0, "y": 1, "z": 2}[st[-1]]
+    kind = st[:-2]
+    dl, dr, pl, pr = 1.0, 0.125, 1.0, 0.1
+    left = dict(v1=0.0, v2=0.0, v3=0.0, b1=0.0, b2=0.0, b3=0.0)
+    right = dict(left)
+    if kind == "briowushock":
+        bvals = {0: ((0.75, 0.75), (1.0, -1.0), (0.0, 0.0)),
+                 1: ((0.0, 0.0), (0.75, 0.75), (1.0, -1.0)),
+                 2: ((1.0, -1.0), (0.0, 0.0), (0.75, 0.75))}[direction]
+        for c in range(3):
+            left[f"b{c + 1}"], right[f"b{c + 1}"] = bvals[c]
+    elif kind != "sodshock":
+        raise ValueError(f"unknown shock tube {st}")
+    return riemann(cfg, direction, dict(d=dl, p=pl, **left), dict(d=dr, p=pr, **right))
+
+
+def riemann(cfg, direction: int, left: dict, right: dict) -> Dict[str, np.ndarray]:
+    """Two-state split along ``direction`` at index (is+ie)/2 (shocktube.f90:109-183)."""
+    out = _blank(cfg)
+    n = cfg["n"][direction]
+    half = (1 + n) // 2  # Fortran (is_global+ie_global)/2 with is=1
+    idx = np.arange(n)
+    is_left = (idx + 1) <= half
+    shape = [1, 1, 1]
+    shape[2 - direction] = n
+    mask = is_left.reshape(shape)
+    for key in ("d", "p", "v1", "v2", "v3", "b1", "b2", "b3"):
+        out[key] = np.where(mask, np.float64(left.get(key, 0.0)), np.float64(right.get(key, 0.0))) * np.ones_like(out[key])
+    return out
+
+
+def orszagtang(cfg, grid) -> Dict[str, np.ndarray]:
+    """src/init/orszagtang.f90:14-80 (2-D planes xy, yz, xz)."""
+    g = cfg["gamma"]
+    n = cfg["n"]
+    out = _blank(cfg)
+    out["d"][:] = g * g / (4.0 * PI)
+    out["p"][:] = g / (4.0 * PI)
+    s4 = math.sqrt(4.0 * PI)
+    if n[2] == 1:  # xy plane: (a, b) = (x, y)
+        a_ax, b_ax, va, vb, ba, bb = 0, 1, "v1", "v2", "b1", "b2"
+    elif n[1] == 1:  # xz plane
+        a_ax, b_ax, va, vb, ba, bb = 0, 2, "v1", "v3", "b1", "b3"
+    elif n[0] == 1:  # yz plane
+        a_ax, b_ax, va, vb, ba, bb = 1, 2, "v2", "v3", "b2", "b3"
+    else:
+        raise ValueError("orszagtang needs a 2-D grid")
+    xa, xb = centres(grid, a_ax), centres(grid, b_ax)
+    sin2b = np.array([math.sin(2.0 * PI * v) for v in xb])
+    sin2a = np.array([math.sin(2.0 * PI * v) for v in xa])
+    sin4a = np.array([math.sin(4.0 * PI * v) for v in xa])
+    va_1d = np.array([-s for s in sin2b])
+    ba_1d = np.array([-s / s4 for s in sin2b])
+    bb_1d = np.array([s / s4 for s in sin4a])
+
+    def bcast(vec, ax):
+        shape = [1, 1, 1]
+        shape[2 - ax] = len(vec)
+        return np.broadcast_to(vec.reshape(shape), out["d"].shape)
+
+    out[va] = np.array(bcast(va_1d, b_ax))
+    out[vb] = np.array(bcast(sin2a, a_ax))
+    out[ba] = np.array(bcast(ba_1d, b_ax))
+    out[bb] = np.array(bcast(bb_1d, a_ax))
+    return out
+
+
+def orszagtang3d(cfg, grid, seed: int = 20261203, amp: float = 1e-3) -> Dict[str, np.ndarray]:
+    """3-D Orszag-Tang-type vortex (not in the reference, which refuses 3-D):
+    the xy-plane fields of orszagtang.f90:29-41 on every z plane, plus seeded
+    uniform noise of amplitude ``amp`` on vz and Bz."""
+    g = cfg["gamma"]
+    out = _blank(cfg)
+    out["d"][:] = g * g / (4.0 * PI)
+    out["p"][:] = g / (4.0 * PI)
+    s4 = math.sqrt(4.0 * PI)
+    x, y = centres(grid, 0), centres(grid, 1)
+    sy = np.array([math.sin(2.0 * PI * v) for v in y])
+    sx = np.array([math.sin(2.0 * PI * v) for v in x])
+    s4x = np.array([math.sin(4.0 * PI * v) for v in x])
+    out["v1"][:] = (-sy)[None, :, None]
+    out["v2"][:] = sx[None, None, :]
+    out["b1"][:] = np.array([-s / s4 for s in sy])[None, :, None]
+    out["b2"][:] = np.array([s / s4 for s in s4x])[None, None, :]
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out["v3"][:] = rng.uniform(-amp, amp, size=out["d"].shape)
+    out["b3"][:] = rng.uniform(-amp, amp, size=out["d"].shape)
+    return out
+
+
+def kelvin_helmholtz(cfg, grid, rho_ratio: float, bx: float, width: float = 0.05, ptb: float = 0.01):
+    """Periodic tanh shear layer (BASELINE's KH boxes; the reference's own
+    KHtests.f90 uses an exponential profile and passive scalars instead):
+    vx = 0.5*tanh((|y|-0.25)/width), rho = 1 outside and ``rho_ratio`` inside
+    the layer, p = 2.5, vy = ptb*sin(4 pi x), Bx = ``bx``."""
+    out = _blank(cfg)
+    x, y = centres(grid, 0), centres(grid, 1)
+    t = np.array([math.tanh((abs(v) - 0.25) / width) for v in y])
+    out["v1"][:] = (0.5 * t)[None, :, None]
+    out["d"][:] = (1.0 + (rho_ratio - 1.0) * 0.5 * (1.0 - t))[None, :, None]
+    out["v2"][:] = np.array([ptb * math.sin(4.0 * PI * v) for v in x])[None, None, :]
+    out["p"][:] = 2.5
+    out["b1"][:] = bx
+    return out
+
+
+def polytrope_n1(cfg, grid, rho_floor: float = 1e-6):
+    """n=1 polytrope of unit radius centred on the origin (G=1, K=2/pi):
+    rho = sin(pi r)/(pi r) inside r<1, ``rho_floor`` outside; p = K rho^2;
+    the analytic potential phi = -(4/pi)(1+rho) inside, -4/(pi r) outside.
+    Returns (prims, grvphi)."""
+    out = _blank(cfg)
+    K = 2.0 / PI
+    x, y, z = centres(grid, 0), centres(grid, 1), centres(grid, 2)
+    r = np.sqrt(x[None, None, :] ** 2 + y[None, :, None] ** 2 + z[:, None, None] ** 2)
+    inside = r < 1.0
+    pr = np.where(inside, PI * r, 1.0)
+    rho = np.where(inside, np.sin(pr) / pr, rho_floor)
+    rho = np.where(r == 0.0, 1.0, rho)
+    out["d"][:] = rho
+    out["p"][:] = K * rho * rho
+    rs = np.where(r > 0.0, r, 1.0)
+    phi = np.where(inside, -(4.0 / PI) * (1.0 + rho), -4.0 / (PI * rs))
+    return out, phi
+
+
+def sedov(cfg, grid, energy: float = 1.0, radius: float = 0.05, rho0: float = 1.0, p0: float = 1e-5):
+    """Cartesian Sedov-type blast: ``energy`` spread evenly over the cells
+    whose centres lie within ``radius`` of the box centre."""
+    out = _blank(cfg)
+    cs = [centres(grid, a) for a in range(3)]
+    mids = [0.5 * (cfg["extent"][a][0] + cfg["extent"][a][1]) for a in range(3)]
+    r2 = ((cs[0] - mids[0])[None, None, :] ** 2 + (cs[1] - mids[1])[None, :, None] ** 2
+          + (cs[2] - mids[2])[:, None, None] ** 2)
+    inside = r2 < radius * radius
+    if not inside.any():
+        inside = r2 == r2.min()
+    dv = 1.0
+    for a in range(3):
+        dv *= grid[a]["dxi"][2]
+    vol = inside.sum() * dv
+    out["d"][:] = rho0
+    out["p"][:] = np.where(inside, (cfg["gamma"] - 1.0) * energy / vol, p0)
+    return out
+
+
+def to_state(cfg, prims: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """Total energy and conserved variables from the initial primitives.
+
+    e = eint + (d*0.5)*|v|^2 + 0.5*|B|^2 with eint = p/(gamma-1)
+    (initialcondition.f90:136-141, eos.f90:287-289); U as conserve.f90:13-50.
+    Returns dict with 'prim' = (d, v1, v2, v3, e, b1, b2, b3, phi) stacked and
+    'u' the nvar conserved planes.
+    """
+    g1 = cfg["gamma"] - 1.0
+    d = prims["d"]
+    v1, v2, v3 = prims["v1"], prims["v2"], prims["v3"]
+    b1, b2, b3 = prims["b1"], prims["b2"], prims["b3"]
+    eint = prims["p"] / g1
+    vv = v1 * v1 + v2 * v2 + v3 * v3
+    bb = b1 * b1 + b2 * b2 + b3 * b3
+    e = eint + d * 0.5 * vv + 0.5 * bb
+    prim = np.stack([d, v1, v2, v3, e, b1, b2, b3, prims["phi"]])
+    u = [d, d * v1, d * v2, d * v3, e]
+    if cfg["mag_on"]:
+        u += [b1, b2, b3]
+        if cfg["dim"] > 1:
+            u.append(prims["phi"])
+    return {"prim": np.ascontiguousarray(prim), "u": np.ascontiguousarray(np.stack(u))}
+
+
+def make(cfg, grid, **kw):
+    st = cfg["simtype"]
+    if st.startswith(("sodshock", "briowushock")):
+        return shocktube(cfg, grid)
+    if st.startswith("orszagtang"):
+        return orszagtang(cfg, grid)
+    raise ValueError(f"no initial condition for simtype {st}")
