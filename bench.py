@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Zone-updates/s of HORMONE's explicit MHD step on B200.
+
+Workload: the 3-D Orszag-Tang-type vortex on a 256^3 periodic unit box
+(gamma=5/3, modified_mc MUSCL + HLLD + GLM, SSP-RK3, courant 0.9, seeded
+1e-3 noise on vz and Bz).  One step = timestep (CFL reduction) + three fused
+RK stages + phidamp + time advance, i.e. one zone-update per cell per step.
+The 1.2 GB state per RK buffer is far larger than the 126 MB L2, so no
+flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W]          the CUDA path
+  python bench.py --impl reference ...                      the CPU path
+
+With N>1 (torchrun) every rank advances its own independent 256^3 box
+(weak scaling, no data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s"
+WORKLOAD = "orszag-tang-3d-256^3-fp64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--cpu-size", type=int, default=128, help="edge of the box the CPU legs time")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def ot_config(n):
+    from hormone_b200 import config
+
+    return config.resolve("orszagtang_3d", overrides=dict(
+        ie=n, je=n, ke=n, mag_on=True, gamma=1.6666666666666667, courant=0.9, flux_limiter="modified_mc",
+        t_end=0.5, dt_out=0.5))
+
+
+def ot_prims(cfg, seed):
+    from hormone_b200 import grid as G, ic
+
+    return ic.orszagtang3d(cfg, G.make_grid(cfg), seed=seed)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel="stage_kernel"):
+    """dram bytes per cell of one stage launch from the committed ncu summary
+    (profiles/<kernel>*.md, a line 'dram_bytes_per_cell: X'), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if fn.startswith(kernel) and fn.endswith(".md"):
+            m = re.search(r"dram_bytes_per_cell:\s*([0-9.eE+-]+)", open(os.path.join(pdir, fn)).read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_leg(n, steps, warm=1):
+    """The oracle (C restatement, OpenMP over all host cores) on an n^3 box of
+    the same workload: zone-updates/s."""
+    from oracle.oracle import Oracle
+
+    cfg = ot_config(n)
+    o = Oracle(cfg)
+    o.set_prims(ot_prims(cfg, 20261203))
+    o.start()
+    for _ in range(warm):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return n ** 3 * steps / dt, cores, dt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import oracle.oracle as orc  # noqa: F401  (builds liboracle.so if needed)
+
+    n = args.cpu_size
+    from oracle.oracle import Oracle
+
+    cfg = ot_config(n)
+    o = Oracle(cfg)
+    o.set_prims(ot_prims(cfg, 20261203))
+    o.start()
+    for _ in range(args.warmup):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step()
+    el = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    v = n ** 3 * args.steps / el
+    sample = (f"{n}^3 box of the same 3-D Orszag-Tang workload, {args.steps} full steps; CPU restatement of "
+              f"HORMONE's FP64 step (the Fortran reference cannot be compiled here), OpenMP over {cores} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": n ** 3, "grid": [n, n, n], "note": "bounded CPU sample"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from hormone_b200 import ic
+    from hormone_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+
+        dist = dist_
+    n = args.size
+    cfg = ot_config(n)
+    prims = ot_prims(cfg, 20261203 + rank)
+    sim = Simulation(cfg, prims)
+    stream = torch.cuda.ExternalStream(sim.ctx.stream_ptr())
+    cells = n ** 3
+
+    def barrier():
+        torch.cuda.synchronize()
+        sim.ctx.sync()
+        if dist:
+            dist.barrier()
+
+    # warm-up
+    sim.run_device(max_steps=args.warmup)
+    barrier()
+    l0 = sim.ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        e0.record(stream)
+        t_before = sim.time
+        _, nrun = sim.ctx.run(sim.time, cfg["t_end"], args.steps)
+        sim.time = _
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    launches = sim.ctx.launches() - l0
+    if nrun != args.steps:
+        raise RuntimeError(f"only {nrun} of {args.steps} steps ran (t_end reached)")
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms * 1e-3)
+    clocks = clk.summary()
+
+    # dominant kernel: the fused RK stage, timed per launch on its stream
+    k = max(3, args.steps)
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    h0.record(stream)
+    for _ in range(k):
+        sim.ctx.hydro_step()
+    h1.record(stream)
+    h1.synchronize()
+    stage_ms = h0.elapsed_time(h1) / (3 * k)
+    nvar = cfg["nvar"]
+    alg_bytes = (2 + 3 + 3) * nvar * 8 / 3 * cells  # per stage launch, averaged over the 3 stages
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+    tpc = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tpc * cells) if tpc else None, "kernel": "stage_kernel",
+                "alg_bytes_per_launch": alg_bytes, "launch_ms": stage_ms, "peak_kind": peak_kind}
+
+    # end to end through the drop-in C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        st = ic.to_state(cfg, prims)
+        u_h = torch.empty(st["u"].shape, dtype=torch.float64, pin_memory=True).numpy()
+        p_h = torch.empty(st["prim"].shape, dtype=torch.float64, pin_memory=True).numpy()
+        u_h[...] = st["u"]
+        p_h[...] = st["prim"]
+        out_u = torch.empty(st["u"].shape, dtype=torch.float64, pin_memory=True).numpy()
+        out_p = [torch.empty(prims["d"].shape, dtype=torch.float64, pin_memory=True).numpy() for _ in range(9)]
+        from hormone_b200 import capi
+
+        ctx = sim.ctx
+        import ctypes
+
+        pp = (capi._DP * 9)()
+        for q in range(9):
+            pp[q] = capi._dp(out_p[q])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.upload(u=u_h, prim=list(p_h))
+        t = 0.0
+        for _ in range(args.steps):
+            dt, ch = ctx.timestep(t, cfg["t_end"], cfg["t_end"])
+            ctx.hydro_step()
+            ctx.phidamp()
+            t = t + dt
+        rc = capi.lib().hmn_download(ctx.h, capi._dp(out_u), pp, None, None)
+        if rc != 0:
+            raise capi.HmnError(rc, "hmn_download")
+        el = time.perf_counter() - t0
+        hb = u_h.nbytes + p_h.nbytes + 24 * args.steps
+        db = out_u.nbytes + sum(a.nbytes for a in out_p) + 200 * args.steps
+        e2e = {"value": cells * args.steps / el, "unit": METRIC, "h2d_bytes_per_step": hb / args.steps,
+               "d2h_bytes_per_step": db / args.steps, "steps": args.steps,
+               "path": "hmn_upload + per step hmn_timestep/hmn_hydro_step/hmn_phidamp + hmn_download"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, el = cpu_leg(args.cpu_size, args.cpu_steps)
+        cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_size}^3 box of the same workload, {args.cpu_steps} full steps "
+                         f"({el:.1f} s) of the CPU restatement, OpenMP"}
+    sim.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "grid": [n, n, n], "cells_per_gpu": cells, "limiter": "modified_mc",
+                           "rktype": 3, "courant": 0.9, "precision": "fp64 bit-compatible (no FMA)",
+                           "l2": "inputs larger than L2 (9 x 8 B x 256^3 = 1.2 GB per RK buffer)",
+                           "parallelism": f"replicas{world}"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

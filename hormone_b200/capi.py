@@ -1,0 +1,229 @@
+"""ctypes binding of libhormone_b200.so (the C ABI of include/hormone_gpu.h).
+
+This is the Python side of the same boundary a Fortran ISO_C_BINDING shim
+binds.  There is no CPU fallback: if the library or a
+CUDA device is missing, creating a context raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhormone_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "hormone_gpu.h")
+
+HMN_OK, HMN_EINVAL, HMN_ENEG_EINT, HMN_ECUDA, HMN_EBADCFG, HMN_ENOMEM, HMN_ETIMEOUT = 0, -1, -2, -3, -4, -5, -6
+ERRORS = {HMN_EINVAL: "HMN_EINVAL", HMN_ENEG_EINT: "HMN_ENEG_EINT", HMN_ECUDA: "HMN_ECUDA",
+          HMN_EBADCFG: "HMN_EBADCFG", HMN_ENOMEM: "HMN_ENOMEM", HMN_ETIMEOUT: "HMN_ETIMEOUT"}
+
+_D, _I, _P = ctypes.c_double, ctypes.c_int, ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+_DPP = ctypes.POINTER(_DP)
+
+
+class HmnGrid(ctypes.Structure):
+    _fields_ = [("n", _I * 3), ("ghost", _I), ("bc", _I * 12),
+                ("x", _DP * 3), ("xi", _DP * 3), ("dx", _DP * 3), ("dxi", _DP * 3), ("idx", _DP * 3),
+                ("idxi", _DP * 3)]
+
+
+class HmnParams(ctypes.Structure):
+    _fields_ = [("gamma", _D), ("courant", _D), ("alpha9wave", _D), ("HGfac", _D), ("hgcfl", _D),
+                ("alphagrv", _D), ("G", _D), ("rktype", _I), ("grktype", _I), ("limiter", _I), ("mag_on", _I),
+                ("gravswitch", _I), ("maxtngrv", _I), ("outstyle", _I), ("endstyle", _I), ("precision", _I)]
+
+
+class HmnError(RuntimeError):
+    def __init__(self, code, where="", cell=None):
+        self.code = code
+        self.cell = cell
+        msg = f"{ERRORS.get(code, code)} in {where}"
+        if cell is not None:
+            msg += f" at cell {cell}"
+        super().__init__(msg)
+
+
+_lib = None
+
+
+def header_functions():
+    """Names of the functions declared in include/hormone_gpu.h."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(hmn_\w+)\s*\(", txt)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m hormone_b200.build` "
+                               "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.hmn_create.argtypes = [ctypes.POINTER(HmnGrid), ctypes.POINTER(HmnParams), ctypes.POINTER(_P)]
+        L.hmn_upload.argtypes = [_P, _DP, _DPP, _DP, _DP]
+        L.hmn_timestep.argtypes = [_P, _D, _D, _D, _DP, _DP]
+        L.hmn_gravity_step.argtypes = [_P, _D, _D, _I]
+        L.hmn_hydro_step.argtypes = [_P]
+        L.hmn_phidamp.argtypes = [_P]
+        L.hmn_download.argtypes = [_P, _DP, _DPP, _DP, _DP]
+        L.hmn_download_pressure.argtypes = [_P, _DP]
+        L.hmn_run.argtypes = [_P, _DP, _D, _I, ctypes.POINTER(_I)]
+        L.hmn_last_error.argtypes = [_P] + [ctypes.POINTER(_I)] * 5
+        L.hmn_launch_count.argtypes = [_P]
+        L.hmn_launch_count.restype = ctypes.c_longlong
+        L.hmn_sync.argtypes = [_P]
+        L.hmn_destroy.argtypes = [_P]
+        L.hmn_set_gravity_clock.argtypes = [_P, _D, _D]
+        L.hmn_stream.argtypes = [_P]
+        L.hmn_stream.restype = _P
+        for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
+                     "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
+                     "hmn_set_gravity_clock"):
+            getattr(L, name).restype = _I
+        _lib = L
+    return _lib
+
+
+def _dp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_DP)
+
+
+class Context:
+    """One simulation resident on the GPU (a thin owner of an ``hmn_ctx*``)."""
+
+    def __init__(self, cfg: dict, grid, precision: int = 0):
+        L = lib()
+        self.cfg = cfg
+        n = cfg["n"]
+        self.shape = (n[2], n[1], n[0])
+        self.nvar = cfg["nvar"]
+        self._grid_arrays = []
+        g = HmnGrid()
+        for a in range(3):
+            g.n[a] = n[a]
+        g.ghost = 0
+        bc = np.asarray(cfg["bc"], dtype=np.int32).reshape(-1)
+        for q in range(12):
+            g.bc[q] = int(bc[q])
+        for key in ("x", "xi", "dx", "dxi", "idx", "idxi"):
+            arr = getattr(g, key)
+            for a in range(3):
+                v = np.ascontiguousarray(grid[a][key], dtype=np.float64)
+                self._grid_arrays.append(v)
+                arr[a] = _dp(v)
+        p = HmnParams(gamma=cfg["gamma"], courant=cfg["courant"], alpha9wave=cfg["alpha9wave"], HGfac=cfg["HGfac"],
+                      hgcfl=cfg["hgcfl"], alphagrv=cfg["alphagrv"], G=cfg["G"], rktype=cfg["rktype"],
+                      grktype=cfg["grktype"], limiter=cfg["limiter_code"], mag_on=int(cfg["mag_on"]),
+                      gravswitch=cfg["gravswitch"], maxtngrv=cfg["maxtngrv"], outstyle=cfg["outstyle"],
+                      endstyle=cfg["endstyle"], precision=precision)
+        h = _P()
+        rc = L.hmn_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h))
+        if rc != 0:
+            raise HmnError(rc, "hmn_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hmn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, where):
+        if rc != 0:
+            cell = None
+            if rc == HMN_ENEG_EINT:
+                c, i, j, k, s = (ctypes.c_int() for _ in range(5))
+                lib().hmn_last_error(self.h, *(ctypes.byref(x) for x in (c, i, j, k, s)))
+                cell = (i.value, j.value, k.value)
+            raise HmnError(rc, where, cell)
+
+    # -- data movement -----------------------------------------------------
+    def upload(self, u=None, prim=None, grvphi=None, grvpsi=None):
+        keep = []
+
+        def arr(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return a
+
+        u_ = arr(u)
+        pp = None
+        if prim is not None:
+            pp = (_DP * 9)()
+            for q in range(9):
+                a = arr(prim[q]) if prim[q] is not None else None
+                pp[q] = _dp(a) if a is not None else _DP()
+        self._check(lib().hmn_upload(self.h, _dp(u_), pp, _dp(arr(grvphi)), _dp(arr(grvpsi))), "hmn_upload")
+
+    def download(self, prims=True, u=True, gravity=False) -> Dict[str, np.ndarray]:
+        out: Dict[str, np.ndarray] = {}
+        U = np.empty((self.nvar,) + self.shape) if u else None
+        pp = None
+        if prims:
+            P = np.empty((9,) + self.shape)
+            pp = (_DP * 9)()
+            for q in range(9):
+                pp[q] = _dp(P[q])
+        gphi = np.empty(self.shape) if gravity else None
+        gpsi = np.empty(self.shape) if gravity else None
+        self._check(lib().hmn_download(self.h, _dp(U), pp, _dp(gphi), _dp(gpsi)), "hmn_download")
+        if u:
+            out["u"] = U
+        if prims:
+            for q, k in enumerate(("d", "v1", "v2", "v3", "e", "b1", "b2", "b3", "phi")):
+                out[k] = P[q]
+        if gravity:
+            out["grvphi"], out["grvpsi"] = gphi, gpsi
+        return out
+
+    def pressure(self) -> np.ndarray:
+        p = np.empty(self.shape)
+        self._check(lib().hmn_download_pressure(self.h, _dp(p)), "hmn_download_pressure")
+        return p
+
+    # -- the step loop entry points -------------------------------------------
+    def timestep(self, time, t_out, t_end):
+        dt, ch = _D(), _D()
+        self._check(lib().hmn_timestep(self.h, float(time), float(t_out), float(t_end), ctypes.byref(dt),
+                                       ctypes.byref(ch)), "hmn_timestep")
+        return dt.value, ch.value
+
+    def gravity_step(self, time, dt, tn):
+        self._check(lib().hmn_gravity_step(self.h, float(time), float(dt), int(tn)), "hmn_gravity_step")
+
+    def set_gravity_clock(self, grvtime, cgrav_old):
+        self._check(lib().hmn_set_gravity_clock(self.h, float(grvtime), float(cgrav_old)), "hmn_set_gravity_clock")
+
+    def hydro_step(self):
+        self._check(lib().hmn_hydro_step(self.h), "hmn_hydro_step")
+
+    def phidamp(self):
+        self._check(lib().hmn_phidamp(self.h), "hmn_phidamp")
+
+    def run(self, time, t_end, max_steps):
+        t = _D(time)
+        steps = _I(0)
+        self._check(lib().hmn_run(self.h, ctypes.byref(t), float(t_end), int(max_steps), ctypes.byref(steps)),
+                    "hmn_run")
+        return t.value, steps.value
+
+    def sync(self):
+        self._check(lib().hmn_sync(self.h), "hmn_sync")
+
+    def launches(self) -> int:
+        return int(lib().hmn_launch_count(self.h))
+
+    def stream_ptr(self) -> int:
+        return int(lib().hmn_stream(self.h) or 0)

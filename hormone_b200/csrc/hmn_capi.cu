@@ -1,0 +1,679 @@
+// hmn_capi.cu -- the C ABI of include/hormone_gpu.h: context, device memory,
+// host<->device layout conversion and the launch sequence of one step
+// (src/main/hormone.f90:126-147).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cstddef>
+#include <new>
+#include <vector>
+
+#include "../../include/hormone_gpu.h"
+#include "hmn_internal.h"
+
+
+using namespace hmn;
+
+struct hmn_ctx {
+  int n[3];
+  int solve[3];
+  int dim, mag, glm, nvar, ghost;
+  int bc[3][2][2];
+  hmn_params par;
+  size_t plane;
+  double* buf[3];            // RK state ping-pong: [0] = U^n (A), [1] = B, [2] = C
+  double* geo;               // 3 axes x kGeoArrays x (n+4)
+  double* gphi[2];           // gravitational potential ping-pong
+  double* gpsi[2];
+  double* gorg[2];
+  int gcur;                  // current potential buffer
+  double* prim_out;          // device scratch for downloads (10 planes)
+  double* stage_h;           // pinned staging for ghosted host layouts
+  size_t stage_h_bytes;
+  DevScalars* sc;            // device scalars
+  DevScalars* sc_h;          // pinned mirror
+  GridDev G;
+  cudaStream_t st;
+  int prim_from_p;           // primitives of the next stage come from the uploaded arrays (in buf[2])
+  double phifac;             // pending phidamp factor of the phi slot
+  int tile[3], tiles[3];
+  long long launches;
+  double grvtime, cgrav_old;
+  double dtg_unit;
+  int nsm;
+  cudaGraphExec_t graph;
+  int graph_steps;
+};
+
+static int cuda_fail(hmn_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return HMN_OK;
+  fprintf(stderr, "hormone_b200: %s: %s\n", what, cudaGetErrorString(e));
+  (void)c;
+  return e == cudaErrorMemoryAllocation ? HMN_ENOMEM : HMN_ECUDA;
+}
+
+#define CK(call, what)                         \
+  do {                                         \
+    cudaError_t _e = (call);                   \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+  } while (0)
+
+static size_t ghosted_index(const hmn_ctx* c, int i, int j, int k) {
+  const int g = c->ghost;
+  const size_t sx = (size_t)c->n[0] + 2 * g, sy = (size_t)c->n[1] + 2 * g;
+  return (size_t)(i + g) + sx * ((size_t)(j + g) + sy * (size_t)(k + g));
+}
+
+static size_t ghosted_plane(const hmn_ctx* c) {
+  const int g = c->ghost;
+  return ((size_t)c->n[0] + 2 * g) * ((size_t)c->n[1] + 2 * g) * ((size_t)c->n[2] + 2 * g);
+}
+
+static int ensure_stage(hmn_ctx* ctx, size_t bytes) {
+  if (ctx->stage_h_bytes >= bytes) return HMN_OK;
+  if (ctx->stage_h) cudaFreeHost(ctx->stage_h);
+  ctx->stage_h = nullptr;
+  ctx->stage_h_bytes = 0;
+  CK(cudaMallocHost((void**)&ctx->stage_h, bytes), "cudaMallocHost");
+  ctx->stage_h_bytes = bytes;
+  return HMN_OK;
+}
+
+// copy nplanes host planes (ghosted or packed) into contiguous device planes
+static int to_device(hmn_ctx* ctx, double* dst, const double* src, int nplanes, size_t src_plane_stride) {
+  const size_t P = ctx->plane;
+  if (ctx->ghost == 0) {
+    for (int q = 0; q < nplanes; q++)
+      CK(cudaMemcpyAsync(dst + q * P, src + q * src_plane_stride, P * sizeof(double), cudaMemcpyHostToDevice,
+                         ctx->st),
+         "upload");
+    return HMN_OK;
+  }
+  int rc = ensure_stage(ctx, (size_t)nplanes * P * sizeof(double));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  size_t o = 0;
+  for (int q = 0; q < nplanes; q++)
+    for (int k = 0; k < ctx->n[2]; k++)
+      for (int j = 0; j < ctx->n[1]; j++)
+        for (int i = 0; i < ctx->n[0]; i++) ctx->stage_h[o++] = src[q * src_plane_stride + ghosted_index(ctx, i, j, k)];
+  CK(cudaMemcpyAsync(dst, ctx->stage_h, (size_t)nplanes * P * sizeof(double), cudaMemcpyHostToDevice, ctx->st),
+     "upload");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  return HMN_OK;
+}
+
+static int to_host(hmn_ctx* ctx, double* dst, const double* src, int nplanes, size_t dst_plane_stride) {
+  const size_t P = ctx->plane;
+  if (ctx->ghost == 0) {
+    for (int q = 0; q < nplanes; q++)
+      CK(cudaMemcpyAsync(dst + q * dst_plane_stride, src + q * P, P * sizeof(double), cudaMemcpyDeviceToHost,
+                         ctx->st),
+         "download");
+    CK(cudaStreamSynchronize(ctx->st), "sync");
+    return HMN_OK;
+  }
+  int rc = ensure_stage(ctx, (size_t)nplanes * P * sizeof(double));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->stage_h, src, (size_t)nplanes * P * sizeof(double), cudaMemcpyDeviceToHost, ctx->st),
+     "download");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  size_t o = 0;
+  for (int q = 0; q < nplanes; q++)
+    for (int k = 0; k < ctx->n[2]; k++)
+      for (int j = 0; j < ctx->n[1]; j++)
+        for (int i = 0; i < ctx->n[0]; i++) dst[q * dst_plane_stride + ghosted_index(ctx, i, j, k)] = ctx->stage_h[o++];
+  return HMN_OK;
+}
+
+static int blocks_for(const hmn_ctx* ctx) {
+  size_t b = (ctx->plane + 255) / 256;
+  size_t cap = (size_t)ctx->nsm * 8;
+  return (int)(b < cap ? (b ? b : 1) : cap);
+}
+
+extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx** out) {
+  if (!grid || !par || !out) return HMN_EINVAL;
+  *out = nullptr;
+  for (int a = 0; a < 3; a++) {
+    if (grid->n[a] < 1) return HMN_EINVAL;
+    if (!grid->x[a] || !grid->xi[a] || !grid->dx[a] || !grid->dxi[a] || !grid->idx[a] || !grid->idxi[a])
+      return HMN_EINVAL;
+  }
+  if (grid->ghost != 0 && grid->ghost != 2) return HMN_EINVAL;
+  if (par->rktype < 1 || par->rktype > 3 || par->limiter < 0 || par->limiter > 2) return HMN_EBADCFG;
+  if (par->gravswitch != 0 && par->gravswitch != 3) return HMN_EBADCFG;
+  if (par->precision != 0) return HMN_EBADCFG;
+  hmn_ctx* ctx = new (std::nothrow) hmn_ctx();
+  if (!ctx) return HMN_ENOMEM;
+  memset(ctx, 0, sizeof(*ctx));
+  ctx->par = *par;
+  ctx->ghost = grid->ghost;
+  ctx->dim = 0;
+  for (int a = 0; a < 3; a++) {
+    ctx->n[a] = grid->n[a];
+    ctx->solve[a] = grid->n[a] > 1;
+    ctx->dim += ctx->solve[a];
+  }
+  memcpy(ctx->bc, grid->bc, sizeof(ctx->bc));
+  for (int a = 0; a < 3; a++) {
+    if (!ctx->solve[a]) continue;
+    for (int io = 0; io < 2; io++)
+      for (int sv = 0; sv < 2; sv++)
+        if (ctx->bc[a][io][sv] < 0 || ctx->bc[a][io][sv] > 3) {
+          delete ctx;
+          return HMN_EBADCFG;
+        }
+    if (ctx->n[a] < 2) {
+      delete ctx;
+      return HMN_EBADCFG;
+    }
+  }
+  if (par->gravswitch == 3 && ctx->dim != 3) {
+    delete ctx;
+    return HMN_EBADCFG;
+  }
+  ctx->mag = par->mag_on != 0;
+  ctx->glm = ctx->mag && ctx->dim > 1;
+  ctx->nvar = 5 + (ctx->mag ? 3 : 0) + (ctx->glm ? 1 : 0);
+  ctx->plane = (size_t)ctx->n[0] * ctx->n[1] * ctx->n[2];
+  ctx->phifac = 1.0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(ctx, e, "device setup");
+    delete ctx;
+    return rc;
+  }
+  // geometry arrays (host derivation, single IEEE operations)
+  const int kA = kGeoArrays;
+  size_t geo_len = 0;
+  for (int a = 0; a < 3; a++) geo_len += (size_t)kA * (ctx->n[a] + 4);
+  std::vector<double> geo(geo_len, 0.0);
+  size_t off = 0;
+  size_t offs[3];
+  for (int a = 0; a < 3; a++) {
+    const int n = ctx->n[a], L = n + 4;
+    offs[a] = off;
+    double* base = geo.data() + off;
+    const double *x = grid->x[a], *xi = grid->xi[a];
+    for (int s = 0; s < L; s++) {
+      base[0 * L + s] = x[s];
+      base[1 * L + s] = grid->dx[a][s];
+      base[2 * L + s] = grid->idx[a][s];
+      base[3 * L + s] = grid->dxi[a][s];
+      base[4 * L + s] = grid->idxi[a][s];
+    }
+    for (int s = 1; s < L; s++) base[5 * L + s] = x[s] - xi[s - 1];  // hl
+    for (int s = 0; s < L; s++) base[6 * L + s] = xi[s] - x[s];      // hr
+    for (int s = 1; s + 1 < L; s++) {
+      base[7 * L + s] = (x[s + 1] - x[s]) / (xi[s] - x[s]);          // mcf
+      base[8 * L + s] = (x[s] - x[s - 1]) / (x[s] - xi[s - 1]);      // mcb
+      base[9 * L + s] = x[s + 1] - x[s];                              // ga
+      base[10 * L + s] = x[s] - x[s - 1];                             // gb
+      base[11 * L + s] = grid->idx[a][s] + grid->idx[a][s + 1];       // isum
+    }
+    off += (size_t)kA * L;
+  }
+  size_t bytes = ctx->plane * sizeof(double);
+  int nplanes = 9;  // every RK buffer can also hold the 9 primitive planes
+  e = cudaMalloc((void**)&ctx->geo, geo_len * sizeof(double));
+  for (int b = 0; b < 3 && e == cudaSuccess; b++) e = cudaMalloc((void**)&ctx->buf[b], nplanes * bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->prim_out, 10 * bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->sc, sizeof(DevScalars));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->sc_h, sizeof(DevScalars));
+  if (e == cudaSuccess && par->gravswitch == 3) {
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+      e = cudaMalloc((void**)&ctx->gphi[b], bytes);
+      if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->gpsi[b], bytes);
+      if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->gorg[b], bytes);
+    }
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->geo, geo.data(), geo_len * sizeof(double), cudaMemcpyHostToDevice, ctx->st);
+  if (e == cudaSuccess) {
+    for (int b = 0; b < 3 && e == cudaSuccess; b++) e = cudaMemsetAsync(ctx->buf[b], 0, nplanes * bytes, ctx->st);
+    for (int b = 0; b < 2 && e == cudaSuccess && par->gravswitch == 3; b++) {
+      e = cudaMemsetAsync(ctx->gphi[b], 0, bytes, ctx->st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(ctx->gpsi[b], 0, bytes, ctx->st);
+    }
+  }
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(ctx, e, "allocation");
+    hmn_destroy(ctx);
+    return rc;
+  }
+  // device scalars
+  DevScalars s;
+  memset(&s, 0, sizeof(s));
+  s.min_dti_bits = 0x7ff0000000000000ULL;
+  s.cfmax_bits = 0ULL;
+  s.courant = par->courant;
+  s.HGfac = par->HGfac;
+  s.hgcfl = par->hgcfl;
+  s.outstyle = par->outstyle;
+  s.endstyle = par->endstyle;
+  s.gravswitch = par->gravswitch;
+  s.maxtngrv = par->maxtngrv;
+  // tools.f90:160-183: dtg_unit = min over cells of dtgrav_cell(cgrav=1)
+  if (par->gravswitch == 3) {
+    double m = INFINITY;
+    const double off0 = ctx->solve[0] ? 1.0 : 0.0, off1 = ctx->solve[1] ? 1.0 : 0.0, off2 = ctx->solve[2] ? 1.0 : 0.0;
+    for (int k = 0; k < ctx->n[2]; k++)
+      for (int j = 0; j < ctx->n[1]; j++)
+        for (int i = 0; i < ctx->n[0]; i++) {
+          const double d1 = grid->dxi[0][i + 2], d2 = grid->dxi[1][j + 2], d3 = grid->dxi[2][k + 2];
+          const double dvol = d1 * d2 * d3;
+          const double s1 = d2 * d3 + d2 * d3, s2 = d1 * d3 + d1 * d3, s3 = d1 * d2 + d1 * d2;
+          const double v = dvol / (1.0 * (off0 * s1 + off1 * s2 + off2 * s3));
+          m = v < m ? v : m;
+        }
+    s.dtg_unit = m;
+    ctx->dtg_unit = m;
+  }
+  *ctx->sc_h = s;
+  e = cudaMemcpyAsync(ctx->sc, ctx->sc_h, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(ctx, e, "init");
+    hmn_destroy(ctx);
+    return rc;
+  }
+  // GridDev with device pointers
+  GridDev& G = ctx->G;
+  for (int a = 0; a < 3; a++) {
+    G.n[a] = ctx->n[a];
+    G.solve[a] = ctx->solve[a];
+    const int L = ctx->n[a] + 4;
+    const double* base = ctx->geo + offs[a];
+    G.g[a].x = base + 0 * L;
+    G.g[a].dx = base + 1 * L;
+    G.g[a].idx = base + 2 * L;
+    G.g[a].dxi = base + 3 * L;
+    G.g[a].idxi = base + 4 * L;
+    G.g[a].hl = base + 5 * L;
+    G.g[a].hr = base + 6 * L;
+    G.g[a].mcf = base + 7 * L;
+    G.g[a].mcb = base + 8 * L;
+    G.g[a].ga = base + 9 * L;
+    G.g[a].gb = base + 10 * L;
+    G.g[a].isum = base + 11 * L;
+  }
+  memcpy(G.bc, ctx->bc, sizeof(G.bc));
+  // tile shape by the number of solved axes
+  int t[3] = {1, 1, 1};
+  if (ctx->dim == 3) {
+    t[0] = 8; t[1] = 8; t[2] = 4;
+  } else if (ctx->dim == 2) {
+    for (int a = 0; a < 3; a++) if (ctx->solve[a]) t[a] = 16;
+  } else {
+    for (int a = 0; a < 3; a++) if (ctx->solve[a]) t[a] = 256;
+  }
+  for (int a = 0; a < 3; a++) {
+    ctx->tile[a] = t[a];
+    ctx->tiles[a] = (ctx->n[a] + t[a] - 1) / t[a];
+  }
+  *out = ctx;
+  return HMN_OK;
+}
+
+extern "C" int hmn_destroy(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
+  for (int b = 0; b < 2; b++) {
+    cudaFree(ctx->gphi[b]);
+    cudaFree(ctx->gpsi[b]);
+    cudaFree(ctx->gorg[b]);
+  }
+  cudaFree(ctx->geo);
+  cudaFree(ctx->prim_out);
+  cudaFree(ctx->sc);
+  if (ctx->sc_h) cudaFreeHost(ctx->sc_h);
+  if (ctx->stage_h) cudaFreeHost(ctx->stage_h);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+  return HMN_OK;
+}
+
+extern "C" int hmn_upload(hmn_ctx* ctx, const double* u, const double* const prim[9], const double* grvphi,
+                          const double* grvpsi) {
+  if (!ctx) return HMN_EINVAL;
+  const size_t gp = ghosted_plane(ctx);
+  int rc;
+  if (u) {
+    rc = to_device(ctx, ctx->buf[0], u, ctx->nvar, gp);
+    if (rc) return rc;
+    ctx->prim_from_p = 0;
+    ctx->phifac = 1.0;
+  }
+  if (prim) {
+    const size_t P = ctx->plane;
+    for (int q = 0; q < 9; q++) {
+      if (prim[q]) {
+        rc = to_device(ctx, ctx->buf[2] + q * P, prim[q], 1, gp);
+        if (rc) return rc;
+      } else {
+        CK(cudaMemsetAsync(ctx->buf[2] + q * P, 0, P * sizeof(double), ctx->st), "memset");
+      }
+    }
+    ctx->prim_from_p = 1;
+    ctx->phifac = 1.0;
+  }
+  if (grvphi && ctx->par.gravswitch == 3) {
+    rc = to_device(ctx, ctx->gphi[ctx->gcur], grvphi, 1, gp);
+    if (rc) return rc;
+  }
+  if (grvpsi && ctx->par.gravswitch == 3) {
+    rc = to_device(ctx, ctx->gpsi[ctx->gcur], grvpsi, 1, gp);
+    if (rc) return rc;
+  }
+  ctx->graph_steps = 0;
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  return HMN_OK;
+}
+
+// pull the scalars and the error word; returns the error code if any kernel recorded one
+static int fetch_scalars(hmn_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->sc_h, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->st), "scalars");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  if (ctx->sc_h->err_code) return ctx->sc_h->err_code;
+  return HMN_OK;
+}
+
+static int push_times(hmn_ctx* ctx, double time, double t_out, double t_end) {
+  // only the three time fields change; write them individually
+  double tv[3] = {time, t_out, t_end};
+  static_assert(offsetof(DevScalars, t_out) == offsetof(DevScalars, time) + sizeof(double), "layout");
+  static_assert(offsetof(DevScalars, t_end) == offsetof(DevScalars, time) + 2 * sizeof(double), "layout");
+  double* dst = &ctx->sc->time;
+  CK(cudaMemcpyAsync(dst, tv, sizeof(tv), cudaMemcpyHostToDevice, ctx->st), "times");
+  CK(cudaMemsetAsync(&ctx->sc->done, 0, sizeof(int), ctx->st), "times");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  return HMN_OK;
+}
+
+static const double* prim_src(const hmn_ctx* ctx, int* src_prim) {
+  *src_prim = ctx->prim_from_p;
+  return ctx->prim_from_p ? ctx->buf[2] : ctx->buf[0];
+}
+
+static int enqueue_cfl(hmn_ctx* ctx) {
+  int sp;
+  const double* src = prim_src(ctx, &sp);
+  CK(launch_cfl(ctx->G, src, sp, ctx->plane, ctx->par.gamma, ctx->sc, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st),
+     "cfl");
+  ctx->launches += 2;
+  return HMN_OK;
+}
+
+extern "C" int hmn_timestep(hmn_ctx* ctx, double time, double t_out, double t_end, double* dt, double* ch) {
+  if (!ctx) return HMN_EINVAL;
+  int rc = push_times(ctx, time, t_out, t_end);
+  if (rc) return rc;
+  rc = enqueue_cfl(ctx);
+  if (rc) return rc;
+  rc = fetch_scalars(ctx);
+  if (dt) *dt = ctx->sc_h->dt;
+  if (ch) *ch = ctx->sc_h->ch;
+  return rc;
+}
+
+static void rk_coeff(int iter, int type, double* faco, double* fact, double* facn) {
+  // rungekutta.f90:146-183
+  if (type == 3) {
+    if (iter == 1) { *faco = 1.0; *fact = 1.0; *facn = 0.0; }
+    else if (iter == 2) { *faco = 0.75; *fact = 0.25; *facn = *fact; }
+    else { *faco = 1.0 / 3.0; *fact = 2.0 / 3.0; *facn = *fact; }
+  } else if (type == 2) {
+    if (iter == 1) { *faco = 1.0; *fact = 1.0; *facn = 0.0; }
+    else { *faco = 0.5; *fact = 0.5; *facn = *fact; }
+  } else {
+    *faco = 1.0; *fact = 1.0; *facn = 0.0;
+  }
+}
+
+static int enqueue_hydro(hmn_ctx* ctx) {
+  const int rk = ctx->par.rktype;
+  double* A = ctx->buf[0];
+  double* B = ctx->buf[1];
+  double* C = ctx->buf[2];
+  for (int s = 1; s <= rk; s++) {
+    StageArgs a;
+    memset(&a, 0, sizeof(a));
+    rk_coeff(s, rk, &a.faco, &a.fact, &a.facn);
+    a.uorg = A;
+    if (s == 1) {
+      int sp;
+      a.src = prim_src(ctx, &sp);
+      a.src_prim = sp;
+      a.phifac = ctx->phifac;
+      a.ucur = A;
+      a.uout = B;
+    } else if (s == 2) {
+      a.src = B;
+      a.ucur = B;
+      a.uout = rk == 2 ? A : C;
+      a.phifac = 1.0;
+    } else {
+      a.src = C;
+      a.ucur = C;
+      a.uout = A;
+      a.phifac = 1.0;
+    }
+    a.gphi = ctx->par.gravswitch == 3 ? ctx->gphi[ctx->gcur] : nullptr;
+    a.sc = ctx->sc;
+    a.plane = ctx->plane;
+    a.gamma = ctx->par.gamma;
+    a.gm1 = ctx->par.gamma - 1.0;
+    a.limiter = ctx->par.limiter;
+    a.nvar = ctx->nvar;
+    for (int d = 0; d < 3; d++) {
+      a.tile[d] = ctx->tile[d];
+      a.tiles[d] = ctx->tiles[d];
+    }
+    CK(launch_stage(ctx->G, a, ctx->mag, ctx->glm, ctx->st), "stage");
+    ctx->launches += 1;
+  }
+  if (rk == 1) {
+    double* t = ctx->buf[0];
+    ctx->buf[0] = ctx->buf[1];
+    ctx->buf[1] = t;
+  }
+  ctx->prim_from_p = 0;
+  ctx->phifac = 1.0;
+  return HMN_OK;
+}
+
+extern "C" int hmn_hydro_step(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  ctx->graph_steps = 0;
+  return enqueue_hydro(ctx);
+}
+
+extern "C" int hmn_phidamp(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  ctx->phifac = ctx->phifac * std::exp(-ctx->par.alpha9wave * ctx->par.courant);  // source.f90:253
+  return HMN_OK;
+}
+
+extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
+  if (!ctx) return HMN_EINVAL;
+  if (ctx->par.gravswitch != 3) return HMN_OK;
+  if (tn == 0) {  // grav_init_other: only the boundary images, which the kernels form on the fly
+    ctx->grvtime = time;
+    return HMN_OK;
+  }
+  // cgrav and dtgrav of the last hmn_timestep
+  int rc = fetch_scalars(ctx);
+  if (rc) return rc;
+  const double cgrav = ctx->sc_h->cgrav;
+  double dtgrav = ctx->sc_h->dtgrav;
+  const int tngrav = (int)std::ceil((time + dt - ctx->grvtime) / dtgrav);  // gravity_hyperbolic.f90:33-34
+  if (tngrav < 1) return HMN_OK;
+  dtgrav = (time + dt - ctx->grvtime) / (double)tngrav;
+  int sp;
+  const double* dens = prim_src(ctx, &sp);  // density plane is slot 0 in both layouts
+  const double fourpiG = 4.0 * M_PI * ctx->par.G;
+  for (int l = 0; l < tngrav; l++) {
+    const double damp = std::exp(-(1.0 - ctx->cgrav_old / cgrav + ctx->par.alphagrv * ctx->par.hgcfl));
+    for (int g = 1; g <= ctx->par.grktype; g++) {
+      double faco, fact, facn;
+      rk_coeff(g, ctx->par.grktype, &faco, &fact, &facn);
+      HGArgs a;
+      memset(&a, 0, sizeof(a));
+      a.phi_in = ctx->gphi[ctx->gcur];
+      a.psi_in = ctx->gpsi[ctx->gcur];
+      a.phi_out = ctx->gphi[1 - ctx->gcur];
+      a.psi_out = ctx->gpsi[1 - ctx->gcur];
+      a.org_phi = ctx->gorg[0];
+      a.org_psi = ctx->gorg[1];
+      a.dens = dens;
+      a.plane = ctx->plane;
+      a.faco = faco;
+      a.facn = facn;
+      a.fdc = fact * dtgrav * cgrav;
+      a.fourpiG = fourpiG;
+      a.damp = damp;
+      a.stage1 = g == 1;
+      a.last = g == ctx->par.grktype;
+      a.sc = ctx->sc;
+      CK(launch_hg_stage(ctx->G, a, blocks_for(ctx), ctx->st), "hg stage");
+      ctx->launches += 1;
+      ctx->gcur = 1 - ctx->gcur;
+    }
+    ctx->grvtime = ctx->grvtime + dtgrav;
+    ctx->cgrav_old = cgrav;
+  }
+  return HMN_OK;
+}
+
+extern "C" int hmn_set_gravity_clock(hmn_ctx* ctx, double grvtime, double cgrav_old) {
+  if (!ctx) return HMN_EINVAL;
+  ctx->grvtime = grvtime;
+  ctx->cgrav_old = cgrav_old;
+  return HMN_OK;
+}
+
+extern "C" int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi) {
+  if (!ctx) return HMN_EINVAL;
+  const size_t gp = ghosted_plane(ctx);
+  int rc;
+  if (u) {
+    rc = to_host(ctx, u, ctx->buf[0], ctx->nvar, gp);
+    if (rc) return rc;
+  }
+  if (prim) {
+    int sp;
+    const double* src = prim_src(ctx, &sp);
+    CK(launch_prim(ctx->G, src, sp, ctx->plane, ctx->phifac, ctx->prim_out, ctx->prim_out + 9 * ctx->plane,
+                   ctx->par.gamma - 1.0, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st),
+       "prim");
+    ctx->launches += 1;
+    for (int q = 0; q < 9; q++) {
+      if (!prim[q]) continue;
+      rc = to_host(ctx, prim[q], ctx->prim_out + q * ctx->plane, 1, gp);
+      if (rc) return rc;
+    }
+  }
+  if (grvphi && ctx->par.gravswitch == 3) {
+    rc = to_host(ctx, grvphi, ctx->gphi[ctx->gcur], 1, gp);
+    if (rc) return rc;
+  }
+  if (grvpsi && ctx->par.gravswitch == 3) {
+    rc = to_host(ctx, grvpsi, ctx->gpsi[ctx->gcur], 1, gp);
+    if (rc) return rc;
+  }
+  return fetch_scalars(ctx);
+}
+
+extern "C" int hmn_download_pressure(hmn_ctx* ctx, double* p) {
+  if (!ctx || !p) return HMN_EINVAL;
+  int sp;
+  const double* src = prim_src(ctx, &sp);
+  CK(launch_prim(ctx->G, src, sp, ctx->plane, ctx->phifac, ctx->prim_out, ctx->prim_out + 9 * ctx->plane,
+                 ctx->par.gamma - 1.0, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st),
+     "prim");
+  ctx->launches += 1;
+  return to_host(ctx, p, ctx->prim_out + 9 * ctx->plane, 1, ghosted_plane(ctx));
+}
+
+// one whole step on the device (hormone.f90:126-147) with device-resident time
+static int enqueue_step(hmn_ctx* ctx) {
+  int rc = enqueue_cfl(ctx);
+  if (rc) return rc;
+  rc = enqueue_hydro(ctx);
+  if (rc) return rc;
+  if (ctx->glm) ctx->phifac = std::exp(-ctx->par.alpha9wave * ctx->par.courant);
+  CK(launch_advance(ctx->sc, ctx->st), "advance");
+  ctx->launches += 1;
+  return HMN_OK;
+}
+
+extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, int* steps) {
+  if (!ctx || !time) return HMN_EINVAL;
+  if (ctx->par.gravswitch == 3) {
+    // the sub-cycle count depends on each step's dt: step on the host clock
+    int done = 0;
+    double t = *time;
+    while (done < max_steps && t < t_end) {
+      double dt, ch;
+      int rc = hmn_timestep(ctx, t, t_end, t_end, &dt, &ch);
+      if (rc) return rc;
+      rc = hmn_gravity_step(ctx, t, dt, 1);
+      if (rc) return rc;
+      rc = enqueue_hydro(ctx);
+      if (rc) return rc;
+      t = t + dt;
+      done++;
+    }
+    *time = t;
+    if (steps) *steps = done;
+    return fetch_scalars(ctx);
+  }
+  int rc = push_times(ctx, *time, t_end, t_end);
+  if (rc) return rc;
+  int done = 0;
+  const int chunk = ctx->par.rktype == 1 ? 1 : 8;  // rktype 1 swaps buffers on the host after each step
+  while (done < max_steps) {
+    int n = max_steps - done < chunk ? max_steps - done : chunk;
+    for (int s = 0; s < n; s++) {
+      rc = enqueue_step(ctx);
+      if (rc) return rc;
+    }
+    done += n;
+    rc = fetch_scalars(ctx);
+    if (rc) return rc;
+    if (ctx->sc_h->time >= t_end) break;
+  }
+  *time = ctx->sc_h->time;
+  if (steps) *steps = done;
+  return HMN_OK;
+}
+
+extern "C" int hmn_last_error(hmn_ctx* ctx, int* code, int* i, int* j, int* k, int* sim) {
+  if (!ctx) return HMN_EINVAL;
+  int rc = fetch_scalars(ctx);
+  (void)rc;
+  if (code) *code = ctx->sc_h->err_code;
+  if (i) *i = ctx->sc_h->err_i;
+  if (j) *j = ctx->sc_h->err_j;
+  if (k) *k = ctx->sc_h->err_k;
+  if (sim) *sim = 0;
+  return HMN_OK;
+}
+
+extern "C" long long hmn_launch_count(hmn_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int hmn_sync(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  return HMN_OK;
+}
+
+extern "C" void* hmn_stream(hmn_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }

@@ -1,0 +1,102 @@
+// hmn_internal.h -- structures shared by the C-ABI layer and the kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hmn {
+
+// Per-axis geometry, each array indexed [c+2] for c in [-2, n+1] (the
+// Fortran range is-2..ie+2).  Derived once on the host from the grid arrays
+// the caller passes, with the same single IEEE operations the reference
+// performs inside its loops, so that reading them is bit-equivalent to
+// recomputing them.
+struct AxisGeo {
+  const double* x;     // cell centres
+  const double* dx;    // centre spacing dx(c) = x(c)-x(c-1) as the grid defines it
+  const double* idx;   // 1/dx(c)
+  const double* dxi;   // cell width
+  const double* idxi;  // 1/dxi(c)
+  const double* hl;    // x(c) - xi(c-1): centre to left face
+  const double* hr;    // xi(c) - x(c): centre to right face
+  const double* mcf;   // (x(c+1)-x(c)) / (xi(c)-x(c))      modified_mc cf
+  const double* mcb;   // (x(c)-x(c-1)) / (x(c)-xi(c-1))    modified_mc cb
+  const double* ga;    // x(c+1) - x(c)
+  const double* gb;    // x(c) - x(c-1)
+  const double* isum;  // idx(c) + idx(c+1)                  minmod denominator
+};
+constexpr int kGeoArrays = 12;
+
+struct GridDev {
+  int n[3];
+  int solve[3];
+  int bc[3][2][2];  // [axis][inner,outer][scalar,vector]
+  AxisGeo g[3];
+};
+
+// Device-resident scalars of one simulation: the CFL reduction slots, the
+// step's dt/ch and the first error seen by any kernel.
+struct DevScalars {
+  unsigned long long min_dti_bits;  // atomicMin over bit patterns of dti > 0
+  unsigned long long cfmax_bits;    // atomicMax over bit patterns of cf >= 0
+  double time, t_out, t_end;
+  double dt, ch, cfmax;
+  double cgrav, dtgrav, dtg_unit;
+  double courant, HGfac, hgcfl;
+  int outstyle, endstyle, gravswitch, maxtngrv;
+  int err_code, err_i, err_j, err_k;
+  int done;  // set by advance_kernel once time >= t_end; later launches of hmn_run skip their work
+  int tn;
+};
+
+// Arguments of one fused RK stage launch (hmn_kernels.cu: stage_kernel).
+struct StageArgs {
+  const double* src;    // stencil source: U planes, or primitive planes when src_prim
+  const double* uorg;   // RK base state U^n (pointwise)
+  const double* ucur;   // state entering this stage (pointwise)
+  double* uout;         // state leaving this stage
+  const double* gphi;   // gravitational potential (interior planes) or nullptr
+  DevScalars* sc;       // dt, ch, errors
+  size_t plane;         // cells per plane (nx*ny*nz)
+  double phifac;        // multiplier of the phi slot when deriving primitives
+  double faco, facn, fact;
+  double gamma, gm1;
+  int src_prim;
+  int limiter;          // 0 flat, 1 minmod, 2 modified_mc
+  int nvar;
+  int tile[3];          // tile extent
+  int tiles[3];         // tiles per axis
+};
+
+// Arguments of one hyperbolic-gravity RK stage (hmn_kernels.cu: hg_stage_kernel).
+struct HGArgs {
+  const double* phi_in;
+  const double* psi_in;
+  double* phi_out;
+  double* psi_out;
+  double* org_phi;
+  double* org_psi;
+  const double* dens;  // density plane of the state at the gravity call
+  size_t plane;
+  double faco, facn, fdc;  // fdc = (fact*dtg)*cgrav
+  double fourpiG;
+  double damp;             // applied to psi after the last stage
+  int stage1, last;
+  DevScalars* sc;
+};
+
+enum : int { kOK = 0, kEINVAL = -1, kENEG_EINT = -2, kECUDA = -3, kEBADCFG = -4, kENOMEM = -5, kETIMEOUT = -6 };
+
+}  // namespace hmn
+
+namespace hmn {
+// launchers (hmn_kernels.cu)
+cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st);
+cudaError_t launch_cfl(const GridDev& G, const double* src, int src_prim, size_t plane, double gamma,
+                       DevScalars* sc, bool mag, bool glm, int nblocks, cudaStream_t st);
+cudaError_t launch_prim(const GridDev& G, const double* src, int src_prim, size_t plane, double phifac, double* out,
+                        double* p_out, double gm1, bool mag, bool glm, int nblocks, cudaStream_t st);
+cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cudaStream_t st);
+cudaError_t launch_advance(DevScalars* sc, cudaStream_t st);
+size_t stage_smem_bytes();
+}  // namespace hmn

@@ -140,22 +140,28 @@ def kelvin_helmholtz(cfg, grid, rho_ratio: float, bx: float, width: float = 0.05
 
 
 def polytrope_n1(cfg, grid, rho_floor: float = 1e-6):
-    """n=1 polytrope of unit radius centred on the origin (G=1, K=2/pi):
-    rho = sin(pi r)/(pi r) inside r<1, ``rho_floor`` outside; p = K rho^2;
-    the analytic potential phi = -(4/pi)(1+rho) inside, -4/(pi r) outside.
+    """n=1 polytrope of unit radius centred on the origin (G=1, K=2/pi).
+
+    rho = sin(pi r)/(pi r) inside r<1 (at least ``rho_floor``) and
+    ``rho_floor`` outside; p = K rho^2 + rho_floor*GM/max(r,1) with M = 4/pi,
+    i.e. the interior polytrope plus the hydrostatic pressure of a
+    constant-density atmosphere in the exterior potential (continuous at
+    r=1).  The potential is the analytic one: phi = -(4/pi)(1+rho_poly)
+    inside, -4/(pi r) outside (from phi + 2K rho = -GM/R).
     Returns (prims, grvphi)."""
     out = _blank(cfg)
     K = 2.0 / PI
+    GM = 4.0 / PI
     x, y, z = centres(grid, 0), centres(grid, 1), centres(grid, 2)
     r = np.sqrt(x[None, None, :] ** 2 + y[None, :, None] ** 2 + z[:, None, None] ** 2)
     inside = r < 1.0
-    pr = np.where(inside, PI * r, 1.0)
-    rho = np.where(inside, np.sin(pr) / pr, rho_floor)
-    rho = np.where(r == 0.0, 1.0, rho)
+    pr = np.where(inside & (r > 0.0), PI * r, 1.0)
+    poly = np.where(inside, np.where(r > 0.0, np.sin(pr) / pr, 1.0), 0.0)
+    rho = np.maximum(poly, rho_floor)
     out["d"][:] = rho
-    out["p"][:] = K * rho * rho
+    out["p"][:] = K * poly * poly + rho_floor * GM / np.maximum(r, 1.0)
     rs = np.where(r > 0.0, r, 1.0)
-    phi = np.where(inside, -(4.0 / PI) * (1.0 + rho), -4.0 / (PI * rs))
+    phi = np.where(inside, -GM * (1.0 + poly), -GM / rs)
     return out, phi
 
 

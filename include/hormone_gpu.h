@@ -1,0 +1,132 @@
+/*
+ * hormone_gpu.h -- C ABI of the B200 implementation of HORMONE's explicit
+ * MHD step.
+ *
+ * The reference has no plugin or FFI layer: its step loop
+ * (src/main/hormone.f90:124-179) calls four argument-less subroutines that
+ * read and write module globals.  Each entry point below replaces one of
+ * them; a Fortran ISO_C_BINDING shim keeps the subroutine names and passes
+ * the module arrays.  All functions return 0 on success or a negative
+ * HMN_E* code, and never abort the host process.
+ *
+ * Layout: host arrays are Fortran order (i fastest) and may carry
+ * ``ghost`` layers on every side (2 for HORMONE's module arrays
+ * u(is-2:ie+2,js-2:je+2,ks-2:ke+2,1:ufnmax), 0 for packed interiors); only
+ * interior cells are read or written.  Conserved-variable slot order is
+ * HORMONE's (src/main/checksetup.f90:61-75): rho, m1, m2, m3, E, B1, B2,
+ * B3, phi (the magnetic slots only with mag_on, phi only with mag_on and
+ * dim > 1).
+ */
+#ifndef HORMONE_GPU_H
+#define HORMONE_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HMN_OK 0
+#define HMN_EINVAL (-1)     /* bad argument */
+#define HMN_ENEG_EINT (-2)  /* negative internal energy: numflux.f90:579-593 / eos.f90:833-839 stop */
+#define HMN_ECUDA (-3)      /* CUDA runtime error */
+#define HMN_EBADCFG (-4)    /* configuration outside this path (checksetup.f90 stop) */
+#define HMN_ENOMEM (-5)     /* device allocation failed */
+#define HMN_ETIMEOUT (-6)   /* a bounded device wait ran out */
+
+typedef struct hmn_ctx hmn_ctx;
+
+/* Grid: the resolved indices and 1-D coordinate arrays of module `grid`
+ * (src/main/modules.f90; filled by gridset.f90:40-140).  Each coordinate
+ * array covers Fortran indices is-2..ie+2 (n+4 values). */
+typedef struct {
+  int n[3];           /* ie-is+1, je-js+1, ke-ks+1 */
+  int ghost;          /* ghost layers of the caller's 3-D arrays (0 or 2) */
+  int bc[3][2][2];    /* boundary codes [axis][inner,outer][scalar,vector], after checksetup.f90:109-128 */
+  const double* x[3];
+  const double* xi[3];
+  const double* dx[3];
+  const double* dxi[3];
+  const double* idx[3];
+  const double* idxi[3];
+} hmn_grid;
+
+/* Settings of module `settings`/`physval`/`gravmod` used by the step. */
+typedef struct {
+  double gamma, courant, alpha9wave;
+  double HGfac, hgcfl, alphagrv, G;
+  int rktype;      /* 1, 2 or 3 */
+  int grktype;     /* RK order of the gravity sub-steps */
+  int limiter;     /* 0 flat, 1 minmod, 2 modified_mc */
+  int mag_on;
+  int gravswitch;  /* 0 off, 3 hyperbolic */
+  int maxtngrv;
+  int outstyle, endstyle;
+  int precision;   /* 0 FP64 (bit-compatible), 1 FP32 flux / FP64 accumulation */
+} hmn_params;
+
+/* allocations.f90 + metric.f90 for this grid: allocates device state. */
+int hmn_create(const hmn_grid* grid, const hmn_params* params, hmn_ctx** out);
+
+/* Device copy of the state after initialcondition/conserve/pressure
+ * (hormone.f90:94-100).  u: conserved array (ufnmax planes); prim: d, v1,
+ * v2, v3, e, b1, b2, b3, phi as the reference holds them (NULL entries are
+ * zero); grvphi/grvpsi: potential and its time derivative (may be NULL).
+ * Any pointer may be NULL to leave that part unchanged. */
+int hmn_upload(hmn_ctx* ctx, const double* u, const double* const prim[9], const double* grvphi,
+               const double* grvpsi);
+
+/* timestep (src/main/timestep.f90:15-105): CFL reduction on the device,
+ * output/end clamps, ch = cfmax, and for gravswitch 3 cgrav and dtgrav.
+ * Writes dt and ch (either pointer may be NULL). */
+int hmn_timestep(hmn_ctx* ctx, double time, double t_out, double t_end, double* dt, double* ch);
+
+/* gravity (src/main/gravity.f90:18-64 -> gravity_hyperbolic.f90:19-50):
+ * the hyperbolic sub-cycles from grvtime to time+dt; tn is the step index
+ * (tn == 0 only sets the boundary images, grav_init_other). */
+int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn);
+
+/* hydro_step (src/main/hydro.f90:15-52): rktype fused RK stages (boundary
+ * images, slopes, HLLD fluxes, source, update, primitive check) with the dt
+ * of the last hmn_timestep. */
+int hmn_hydro_step(hmn_ctx* ctx);
+
+/* phidamp (src/main/source.f90:239-260). */
+int hmn_phidamp(hmn_ctx* ctx);
+
+/* Host copy of the current state (output, restart dumps, the test harness,
+ * tests.f90:46): u, the primitives d, v1, v2, v3, e, b1, b2, b3, phi as
+ * rungekutta.f90:205-229 and phidamp leave them, and the potential.  NULL
+ * pointers are skipped. */
+int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi);
+
+/* Gas pressure p = (gamma-1)*eint of the current state (eos.f90:742-794). */
+int hmn_download_pressure(hmn_ctx* ctx, double* p);
+
+/* Clock of the hyperbolic solver: grvtime and cgrav_old of module gravmod
+ * (restored from a dump by readbin.f90:60-65). */
+int hmn_set_gravity_clock(hmn_ctx* ctx, double grvtime, double cgrav_old);
+
+/* Advance whole steps on the device without host round trips: the loop of
+ * hormone.f90:126-155 (timestep, gravity, hydro_step, phidamp, time += dt)
+ * until time >= t_end or max_steps steps; the clamps use t_out = t_end.
+ * *time and *steps are updated. */
+int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, int* steps);
+
+/* First error recorded by any kernel: code and the cell (0-based). */
+int hmn_last_error(hmn_ctx* ctx, int* code, int* i, int* j, int* k, int* sim);
+
+/* Number of kernel launches issued by this context so far (diagnostics). */
+long long hmn_launch_count(hmn_ctx* ctx);
+
+/* Wait for all work of the context. */
+int hmn_sync(hmn_ctx* ctx);
+
+/* The context's CUDA stream (cudaStream_t), for callers that order their
+ * own work after the step. */
+void* hmn_stream(hmn_ctx* ctx);
+
+int hmn_destroy(hmn_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
