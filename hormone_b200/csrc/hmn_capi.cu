@@ -629,6 +629,7 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
       if (rc) return rc;
       rc = enqueue_hydro(ctx);
       if (rc) return rc;
+      if (ctx->glm) ctx->phifac = std::exp(-ctx->par.alpha9wave * ctx->par.courant);
       t = t + dt;
       done++;
     }
@@ -638,6 +639,9 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
   }
   int rc = push_times(ctx, *time, t_end, t_end);
   if (rc) return rc;
+  rc = fetch_scalars(ctx);
+  if (rc) return rc;
+  const int tn0 = ctx->sc_h->tn;
   int done = 0;
   const int chunk = ctx->par.rktype == 1 ? 1 : 8;  // rktype 1 swaps buffers on the host after each step
   while (done < max_steps) {
@@ -652,7 +656,7 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
     if (ctx->sc_h->time >= t_end) break;
   }
   *time = ctx->sc_h->time;
-  if (steps) *steps = done;
+  if (steps) *steps = ctx->sc_h->tn - tn0;  // steps that ran before the end time was reached
   return HMN_OK;
 }
 
