@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhormone_b200.so")
-SOURCES = ["hmn_kernels.cu", "hmn_capi.cu"]
+SOURCES = ["hmn_kernels.cu", "hmn_capi.cu", "hmn_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

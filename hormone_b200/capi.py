@@ -81,6 +81,8 @@ def lib():
         L.hmn_set_gravity_clock.argtypes = [_P, _D, _D]
         L.hmn_stream.argtypes = [_P]
         L.hmn_stream.restype = _P
+        L.hmn_timestep_noalloc.argtypes = [ctypes.POINTER(HmnGrid), ctypes.POINTER(HmnParams), _P, _D, _D, _D, _P, _P]
+        L.hmn_timestep_noalloc.restype = _I
         for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
                      "hmn_set_gravity_clock"):
@@ -91,6 +93,33 @@ def lib():
 
 def _dp(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(_DP)
+
+
+def grid_struct(cfg: dict, grid):
+    """hmn_grid for a resolved configuration; returns (struct, arrays to keep alive)."""
+    keep = []
+    g = HmnGrid()
+    for a in range(3):
+        g.n[a] = cfg["n"][a]
+    g.ghost = 0
+    bc = np.asarray(cfg["bc"], dtype=np.int32).reshape(-1)
+    for q in range(12):
+        g.bc[q] = int(bc[q])
+    for key in ("x", "xi", "dx", "dxi", "idx", "idxi"):
+        arr = getattr(g, key)
+        for a in range(3):
+            v = np.ascontiguousarray(grid[a][key], dtype=np.float64)
+            keep.append(v)
+            arr[a] = _dp(v)
+    return g, keep
+
+
+def params_struct(cfg: dict, precision: int = 0) -> HmnParams:
+    return HmnParams(gamma=cfg["gamma"], courant=cfg["courant"], alpha9wave=cfg["alpha9wave"], HGfac=cfg["HGfac"],
+                     hgcfl=cfg["hgcfl"], alphagrv=cfg["alphagrv"], G=cfg["G"], rktype=cfg["rktype"],
+                     grktype=cfg["grktype"], limiter=cfg["limiter_code"], mag_on=int(cfg["mag_on"]),
+                     gravswitch=cfg["gravswitch"], maxtngrv=cfg["maxtngrv"], outstyle=cfg["outstyle"],
+                     endstyle=cfg["endstyle"], precision=precision)
 
 
 class Context:

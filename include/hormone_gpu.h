@@ -126,6 +126,22 @@ void* hmn_stream(hmn_ctx* ctx);
 
 int hmn_destroy(hmn_ctx* ctx);
 
+/* The CFL timestep of hmn_timestep for callers that cannot allocate device
+ * memory (no counterpart in the reference: HORMONE has no device code).
+ * It needs no hmn_ctx: u_dev holds the conserved planes on the device
+ * (packed interior, x fastest, ufnmax planes), and on completion out_dev
+ * (3 doubles of caller-owned device memory) holds dt, ch and a status
+ * (0, or HMN_ENEG_EINT if a cell has eint <= 0).  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL for the default stream); nothing is
+ * synchronised.  The scratch is a static device array of 114,784 bytes
+ * per GPU that loads the library: at most 4096 cells per axis (larger
+ * grids return HMN_EINVAL), gravswitch must be 0.  The first call on a
+ * device looks up the array's device address; make it before any stream
+ * capture.  Calls that overlap on the GPU share the array and race: the
+ * caller must order them. */
+int hmn_timestep_noalloc(const hmn_grid* grid, const hmn_params* params, const double* u_dev, double time,
+                         double t_out, double t_end, double* out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
