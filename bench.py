@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     return ap.parse_args()
 
 
@@ -193,6 +194,51 @@ def run_reference(args, rank):
 
 
 # ---------------------------------------------------------------------------
+def mixed_leg(args, cfg, prims, sim64, rank, world, dist):
+    """The FP32-flux / FP64-accumulate form on the same workload: throughput,
+    and the one-step L1 error per variable against the FP64 form started
+    from the same state (sum |q_mixed - q_fp64| / sum |q_fp64|)."""
+    import numpy as np
+    import torch
+
+    from hormone_b200.sim import Simulation
+
+    n = args.size
+    sim = Simulation(cfg, prims, precision=1)
+    stream = torch.cuda.ExternalStream(sim.ctx.stream_ptr())
+    sim.run_device(max_steps=args.warmup)
+    torch.cuda.synchronize()
+    sim.ctx.sync()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t, nrun = sim.ctx.run(sim.time, cfg["t_end"], args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * n ** 3 * nrun / (ms * 1e-3)
+    # one step from an identical state
+    st = sim64.state()
+    prim = [st[k] for k in ("d", "v1", "v2", "v3", "e", "b1", "b2", "b3", "phi")]
+    for s_ in (sim64, sim):
+        s_.ctx.upload(u=st["u"], prim=prim)
+        s_.time, s_.tn = 0.1, 1
+    sim64.step()
+    sim.step()
+    a, b = sim64.state(), sim.state()
+    l1 = {k: float(np.sum(np.abs(b[k] - a[k])) / max(np.sum(np.abs(a[k])), 1e-300))
+          for k in ("d", "e", "v1", "v2", "v3", "b1", "b2", "b3")}
+    sim.close()
+    return {"value": value, "unit": METRIC, "ms_per_step": ms / max(nrun, 1), "steps": nrun,
+            "dtype": "f32 Riemann solver / f64 reconstruction, pressure recovery and compensated accumulation",
+            "l1_one_step_vs_fp64": l1}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -300,6 +346,10 @@ def run_ours(args, rank, world, local_rank):
                "d2h_bytes_per_step": db / args.steps, "steps": args.steps,
                "path": "hmn_upload + per step hmn_timestep/hmn_hydro_step/hmn_phidamp + hmn_download"}
 
+    mixed = None
+    if not args.no_mixed:
+        mixed = mixed_leg(args, cfg, prims, sim, rank, world, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, el = cpu_leg(args.cpu_size, args.cpu_steps)
@@ -315,7 +365,7 @@ def run_ours(args, rank, world, local_rank):
                            "rktype": 3, "courant": 0.9, "precision": "fp64 bit-compatible (no FMA)",
                            "l2": "inputs larger than L2 (9 x 8 B x 256^3 = 1.2 GB per RK buffer)",
                            "parallelism": f"replicas{world}"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "mixed": mixed,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
 

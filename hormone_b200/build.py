@@ -14,7 +14,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhormone_b200.so")
-SOURCES = ["hmn_kernels.cu", "hmn_capi.cu", "hmn_noalloc.cu"]
+SOURCES = ["hmn_kernels.cu", "hmn_capi.cu", "hmn_noalloc.cu", "hmn_mixed.cu"]
+# per-source precision flags: the FP64 path is bit-compatible (no fused
+# multiply-add); the mixed-precision stage uses fast single-precision math
+FLAGS = {"hmn_mixed.cu": ["-use_fast_math"]}
+DEFAULT_FLAGS = ["--fmad=false"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -34,7 +38,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(bdir, exist_ok=True)
     for src in SOURCES:
         obj = os.path.join(bdir, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler",
+        cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", *FLAGS.get(src, DEFAULT_FLAGS), "-lineinfo", "-Xcompiler",
                "-fPIC,-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

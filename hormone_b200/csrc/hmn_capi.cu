@@ -24,7 +24,9 @@ struct hmn_ctx {
   int bc[3][2][2];
   hmn_params par;
   size_t plane;
-  double* buf[3];            // RK state ping-pong: [0] = U^n (A), [1] = B, [2] = C
+  double* buf[3];            // conserved-state RK buffers: [0] = U^n (A), [1] = B, [2] = C
+  double* pbuf[2];           // primitive planes (10 each), ping-pong across stages
+  int pcur;                  // primitive buffer of the current state
   double* geo;               // 3 axes x kGeoArrays x (n+4)
   double* gphi[2];           // gravitational potential ping-pong
   double* gpsi[2];
@@ -37,7 +39,6 @@ struct hmn_ctx {
   DevScalars* sc_h;          // pinned mirror
   GridDev G;
   cudaStream_t st;
-  int prim_from_p;           // primitives of the next stage come from the uploaded arrays (in buf[2])
   double phifac;             // pending phidamp factor of the phi slot
   int tile[3], tiles[3];
   long long launches;
@@ -146,7 +147,7 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   if (grid->ghost != 0 && grid->ghost != 2) return HMN_EINVAL;
   if (par->rktype < 1 || par->rktype > 3 || par->limiter < 0 || par->limiter > 2) return HMN_EBADCFG;
   if (par->gravswitch != 0 && par->gravswitch != 3) return HMN_EBADCFG;
-  if (par->precision != 0) return HMN_EBADCFG;
+  if (par->precision != 0 && par->precision != 1) return HMN_EBADCFG;
   hmn_ctx* ctx = new (std::nothrow) hmn_ctx();
   if (!ctx) return HMN_ENOMEM;
   memset(ctx, 0, sizeof(*ctx));
@@ -217,6 +218,9 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
       base[9 * L + s] = x[s + 1] - x[s];                              // ga
       base[10 * L + s] = x[s] - x[s - 1];                             // gb
       base[11 * L + s] = grid->idx[a][s] + grid->idx[a][s + 1];       // isum
+      base[12 * L + s] = 1.0 / base[9 * L + s];                       // rga
+      base[13 * L + s] = base[9 * L + s] / base[10 * L + s];          // gab
+      base[14 * L + s] = 1.0 / base[11 * L + s];                      // risum
     }
     off += (size_t)kA * L;
   }
@@ -224,6 +228,7 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   int nplanes = 9;  // every RK buffer can also hold the 9 primitive planes
   e = cudaMalloc((void**)&ctx->geo, geo_len * sizeof(double));
   for (int b = 0; b < 3 && e == cudaSuccess; b++) e = cudaMalloc((void**)&ctx->buf[b], nplanes * bytes);
+  for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMalloc((void**)&ctx->pbuf[b], 10 * bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->prim_out, 10 * bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->sc, sizeof(DevScalars));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->sc_h, sizeof(DevScalars));
@@ -237,6 +242,7 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->geo, geo.data(), geo_len * sizeof(double), cudaMemcpyHostToDevice, ctx->st);
   if (e == cudaSuccess) {
     for (int b = 0; b < 3 && e == cudaSuccess; b++) e = cudaMemsetAsync(ctx->buf[b], 0, nplanes * bytes, ctx->st);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMemsetAsync(ctx->pbuf[b], 0, 10 * bytes, ctx->st);
     for (int b = 0; b < 2 && e == cudaSuccess && par->gravswitch == 3; b++) {
       e = cudaMemsetAsync(ctx->gphi[b], 0, bytes, ctx->st);
       if (e == cudaSuccess) e = cudaMemsetAsync(ctx->gpsi[b], 0, bytes, ctx->st);
@@ -302,21 +308,13 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     G.g[a].ga = base + 9 * L;
     G.g[a].gb = base + 10 * L;
     G.g[a].isum = base + 11 * L;
+    G.g[a].rga = base + 12 * L;
+    G.g[a].gab = base + 13 * L;
+    G.g[a].risum = base + 14 * L;
   }
   memcpy(G.bc, ctx->bc, sizeof(G.bc));
-  // tile shape by the number of solved axes
-  int t[3] = {1, 1, 1};
-  if (ctx->dim == 3) {
-    t[0] = 8; t[1] = 8; t[2] = 4;
-  } else if (ctx->dim == 2) {
-    for (int a = 0; a < 3; a++) if (ctx->solve[a]) t[a] = 16;
-  } else {
-    for (int a = 0; a < 3; a++) if (ctx->solve[a]) t[a] = 256;
-  }
-  for (int a = 0; a < 3; a++) {
-    ctx->tile[a] = t[a];
-    ctx->tiles[a] = (ctx->n[a] + t[a] - 1) / t[a];
-  }
+  stage_tile(ctx->solve, ctx->tile);
+  for (int a = 0; a < 3; a++) ctx->tiles[a] = (ctx->n[a] + ctx->tile[a] - 1) / ctx->tile[a];
   *out = ctx;
   return HMN_OK;
 }
@@ -326,6 +324,7 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
+  for (int b = 0; b < 2; b++) cudaFree(ctx->pbuf[b]);
   for (int b = 0; b < 2; b++) {
     cudaFree(ctx->gphi[b]);
     cudaFree(ctx->gpsi[b]);
@@ -349,21 +348,27 @@ extern "C" int hmn_upload(hmn_ctx* ctx, const double* u, const double* const pri
   if (u) {
     rc = to_device(ctx, ctx->buf[0], u, ctx->nvar, gp);
     if (rc) return rc;
-    ctx->prim_from_p = 0;
     ctx->phifac = 1.0;
   }
+  double* Pc = ctx->pbuf[ctx->pcur];
   if (prim) {
+    // the primitives as the reference holds them after initialcondition;
+    // eint as pressure -> internalenergy derives it (eos.f90:805-842)
     const size_t P = ctx->plane;
     for (int q = 0; q < 9; q++) {
       if (prim[q]) {
-        rc = to_device(ctx, ctx->buf[2] + q * P, prim[q], 1, gp);
+        rc = to_device(ctx, Pc + q * P, prim[q], 1, gp);
         if (rc) return rc;
       } else {
-        CK(cudaMemsetAsync(ctx->buf[2] + q * P, 0, P * sizeof(double), ctx->st), "memset");
+        CK(cudaMemsetAsync(Pc + q * P, 0, P * sizeof(double), ctx->st), "memset");
       }
     }
-    ctx->prim_from_p = 1;
+    CK(launch_prim_init(Pc, ctx->plane, ctx->mag, blocks_for(ctx), ctx->st), "prim init");
+    ctx->launches += 1;
     ctx->phifac = 1.0;
+  } else if (u) {
+    CK(launch_prim_from_u(ctx->buf[0], Pc, ctx->plane, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st), "prim");
+    ctx->launches += 1;
   }
   if (grvphi && ctx->par.gravswitch == 3) {
     rc = to_device(ctx, ctx->gphi[ctx->gcur], grvphi, 1, gp);
@@ -398,15 +403,9 @@ static int push_times(hmn_ctx* ctx, double time, double t_out, double t_end) {
   return HMN_OK;
 }
 
-static const double* prim_src(const hmn_ctx* ctx, int* src_prim) {
-  *src_prim = ctx->prim_from_p;
-  return ctx->prim_from_p ? ctx->buf[2] : ctx->buf[0];
-}
-
 static int enqueue_cfl(hmn_ctx* ctx) {
-  int sp;
-  const double* src = prim_src(ctx, &sp);
-  CK(launch_cfl(ctx->G, src, sp, ctx->plane, ctx->par.gamma, ctx->sc, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st),
+  CK(launch_cfl(ctx->G, ctx->pbuf[ctx->pcur], ctx->plane, ctx->par.gamma, ctx->sc, ctx->mag, blocks_for(ctx),
+                ctx->st),
      "cfl");
   ctx->launches += 2;
   return HMN_OK;
@@ -448,20 +447,17 @@ static int enqueue_hydro(hmn_ctx* ctx) {
     memset(&a, 0, sizeof(a));
     rk_coeff(s, rk, &a.faco, &a.fact, &a.facn);
     a.uorg = A;
+    a.pin = ctx->pbuf[ctx->pcur];
+    a.pout = ctx->pbuf[1 - ctx->pcur];
     if (s == 1) {
-      int sp;
-      a.src = prim_src(ctx, &sp);
-      a.src_prim = sp;
       a.phifac = ctx->phifac;
       a.ucur = A;
       a.uout = B;
     } else if (s == 2) {
-      a.src = B;
       a.ucur = B;
       a.uout = rk == 2 ? A : C;
       a.phifac = 1.0;
     } else {
-      a.src = C;
       a.ucur = C;
       a.uout = A;
       a.phifac = 1.0;
@@ -477,15 +473,18 @@ static int enqueue_hydro(hmn_ctx* ctx) {
       a.tile[d] = ctx->tile[d];
       a.tiles[d] = ctx->tiles[d];
     }
-    CK(launch_stage(ctx->G, a, ctx->mag, ctx->glm, ctx->st), "stage");
+    if (ctx->par.precision == 1)
+      CK(launch_stage_mixed(ctx->G, a, ctx->mag, ctx->glm, ctx->st), "stage");
+    else
+      CK(launch_stage(ctx->G, a, ctx->mag, ctx->glm, ctx->st), "stage");
     ctx->launches += 1;
+    ctx->pcur = 1 - ctx->pcur;
   }
   if (rk == 1) {
     double* t = ctx->buf[0];
     ctx->buf[0] = ctx->buf[1];
     ctx->buf[1] = t;
   }
-  ctx->prim_from_p = 0;
   ctx->phifac = 1.0;
   return HMN_OK;
 }
@@ -517,8 +516,7 @@ extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
   const int tngrav = (int)std::ceil((time + dt - ctx->grvtime) / dtgrav);  // gravity_hyperbolic.f90:33-34
   if (tngrav < 1) return HMN_OK;
   dtgrav = (time + dt - ctx->grvtime) / (double)tngrav;
-  int sp;
-  const double* dens = prim_src(ctx, &sp);  // density plane is slot 0 in both layouts
+  const double* dens = ctx->pbuf[ctx->pcur];  // density plane of the state at the gravity call
   const double fourpiG = 4.0 * M_PI * ctx->par.G;
   for (int l = 0; l < tngrav; l++) {
     const double damp = std::exp(-(1.0 - ctx->cgrav_old / cgrav + ctx->par.alphagrv * ctx->par.hgcfl));
@@ -569,10 +567,8 @@ extern "C" int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], doub
     if (rc) return rc;
   }
   if (prim) {
-    int sp;
-    const double* src = prim_src(ctx, &sp);
-    CK(launch_prim(ctx->G, src, sp, ctx->plane, ctx->phifac, ctx->prim_out, ctx->prim_out + 9 * ctx->plane,
-                   ctx->par.gamma - 1.0, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st),
+    CK(launch_prim_out(ctx->pbuf[ctx->pcur], ctx->plane, ctx->phifac, ctx->par.gamma - 1.0, ctx->prim_out,
+                       ctx->prim_out + 9 * ctx->plane, blocks_for(ctx), ctx->st),
        "prim");
     ctx->launches += 1;
     for (int q = 0; q < 9; q++) {
@@ -594,10 +590,8 @@ extern "C" int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], doub
 
 extern "C" int hmn_download_pressure(hmn_ctx* ctx, double* p) {
   if (!ctx || !p) return HMN_EINVAL;
-  int sp;
-  const double* src = prim_src(ctx, &sp);
-  CK(launch_prim(ctx->G, src, sp, ctx->plane, ctx->phifac, ctx->prim_out, ctx->prim_out + 9 * ctx->plane,
-                 ctx->par.gamma - 1.0, ctx->mag, ctx->glm, blocks_for(ctx), ctx->st),
+  CK(launch_prim_out(ctx->pbuf[ctx->pcur], ctx->plane, ctx->phifac, ctx->par.gamma - 1.0, ctx->prim_out,
+                     ctx->prim_out + 9 * ctx->plane, blocks_for(ctx), ctx->st),
      "prim");
   ctx->launches += 1;
   return to_host(ctx, p, ctx->prim_out + 9 * ctx->plane, 1, ghosted_plane(ctx));

@@ -24,8 +24,12 @@ struct AxisGeo {
   const double* ga;    // x(c+1) - x(c)
   const double* gb;    // x(c) - x(c-1)
   const double* isum;  // idx(c) + idx(c+1)                  minmod denominator
+  // reciprocal forms used only by the mixed-precision stage (division-free limiters)
+  const double* rga;   // 1 / ga
+  const double* gab;   // ga / gb
+  const double* risum; // 1 / isum
 };
-constexpr int kGeoArrays = 12;
+constexpr int kGeoArrays = 15;
 
 struct GridDev {
   int n[3];
@@ -51,17 +55,17 @@ struct DevScalars {
 
 // Arguments of one fused RK stage launch (hmn_kernels.cu: stage_kernel).
 struct StageArgs {
-  const double* src;    // stencil source: U planes, or primitive planes when src_prim
+  const double* pin;    // primitive planes of the state entering the stage (stencil source)
+  double* pout;         // primitive planes of the state leaving the stage
   const double* uorg;   // RK base state U^n (pointwise)
   const double* ucur;   // state entering this stage (pointwise)
   double* uout;         // state leaving this stage
   const double* gphi;   // gravitational potential (interior planes) or nullptr
   DevScalars* sc;       // dt, ch, errors
   size_t plane;         // cells per plane (nx*ny*nz)
-  double phifac;        // multiplier of the phi slot when deriving primitives
+  double phifac;        // pending phidamp factor applied to the phi plane
   double faco, facn, fact;
   double gamma, gm1;
-  int src_prim;
   int limiter;          // 0 flat, 1 minmod, 2 modified_mc
   int nvar;
   int tile[3];          // tile extent
@@ -91,12 +95,17 @@ enum : int { kOK = 0, kEINVAL = -1, kENEG_EINT = -2, kECUDA = -3, kEBADCFG = -4,
 
 namespace hmn {
 // launchers (hmn_kernels.cu)
+void stage_tile(const int solve[3], int tile[3]);
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st);
-cudaError_t launch_cfl(const GridDev& G, const double* src, int src_prim, size_t plane, double gamma,
-                       DevScalars* sc, bool mag, bool glm, int nblocks, cudaStream_t st);
-cudaError_t launch_prim(const GridDev& G, const double* src, int src_prim, size_t plane, double phifac, double* out,
-                        double* p_out, double gm1, bool mag, bool glm, int nblocks, cudaStream_t st);
+// mixed precision (hmn_mixed.cu): FP32 Riemann solver, FP64 reconstruction and accumulation
+cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st);
+cudaError_t launch_cfl(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc, bool mag,
+                       int nblocks, cudaStream_t st);
+cudaError_t launch_prim_init(double* P, size_t plane, bool mag, int nblocks, cudaStream_t st);
+cudaError_t launch_prim_from_u(const double* U, double* P, size_t plane, bool mag, bool glm, int nblocks,
+                               cudaStream_t st);
+cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double gm1, double* out, double* p_out,
+                            int nblocks, cudaStream_t st);
 cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cudaStream_t st);
 cudaError_t launch_advance(DevScalars* sc, cudaStream_t st);
-size_t stage_smem_bytes();
 }  // namespace hmn

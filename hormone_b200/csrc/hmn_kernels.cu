@@ -4,418 +4,365 @@
 // operation in the reference's order, so results are bit-identical to the
 // Fortran path (and to the CPU oracle that restates it).
 //
-// One RK stage (src/main/hydro.f90:35-41: boundarycondition -> numflux ->
-// source -> rungekutta) is ONE launch of stage_kernel.  A CTA owns a tile of
-// cells; for every solved axis it
-//   1. stages the primitives of the tile plus two cells either side along
-//      the axis into shared memory, generating ghost cells from the boundary
-//      codes on the fly (boundarycondition.f90, codes 0-3),
-//   2. computes the limited slopes of those cells (interpolation.f90),
-//   3. computes the HLLD face fluxes (numflux.f90 + hlldflux.f90),
-//   4. accumulates the flux divergence of its cells in shared memory,
-// and finally applies the RK combination (rungekutta.f90:35-59) with the
-// gravity source (source.f90:70-85) and writes the new conserved state.
-// Fluxes and slopes never leave the SM.
+// State in HBM (per simulation, interior cells only, x fastest):
+//   U planes  (nvar):  rho, m1, m2, m3, E, B1, B2, B3, phi   (conserved)
+//   P planes  (10):    rho, v1, v2, v3, e, B1, B2, B3, phi, eint
+// P is what HORMONE keeps in module physval after `primitive`/`pressure`
+// (rungekutta.f90:193-232, eos.f90:742-842); every stage writes the P of
+// its output so the next stage reads primitives without dividing again.
+//
+// One RK stage (hydro.f90:35-41: boundarycondition -> numflux -> source ->
+// rungekutta) is ONE launch of stage_kernel.  A CTA owns a tile of 256 cells:
+//   1. it stages the primitives of the tile and of two cells beyond each face
+//      of the tile (a cross-shaped region, no corners) into shared memory,
+//      forming ghost cells from the boundary codes on the fly
+//      (boundarycondition.f90, codes 0-3 and the ghost energy of :222-243);
+//   2. per solved axis it computes the limited slopes (interpolation.f90),
+//      the HLLD face fluxes (numflux.f90 + hlldflux.f90) and adds the flux
+//      divergence of its cell to registers;
+//   3. it applies the RK combination (rungekutta.f90:35-59) with the gravity
+//      source (source.f90:70-85) and writes U and P of the new state.
+// Slopes and fluxes never leave the SM.
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
+#include "hmn_tile.cuh"
 
 namespace hmn {
 
-// conserved slots (checksetup.f90:61-75)
-enum { ICNT = 0, IMO1 = 1, IENE = 4, IMG1 = 5, I9WV = 8 };
-// staged primitive quantities per cell: d, m1..3 (= d*v), e, b1..3, phi, eint
-enum { Q_D = 0, Q_M = 1, Q_E = 4, Q_B = 5, Q_PHI = 8, Q_EINT = 9, NQ = 10 };
-// slopes: d, e, m1..3, b1..3
-enum { S_D = 0, S_E = 1, S_M = 2, S_B = 5, NS = 8 };
-
-constexpr int kThreads = 256;
-constexpr int kMaxCells = 256;   // interior cells of a tile
-constexpr int kMaxRegion = 512;  // tile + 2 cells either side along one axis
-constexpr int kMaxSlope = 384;   // tile + 1 cell either side
-constexpr int kMaxFace = 320;    // tile + 1 face
-
-__device__ __forceinline__ void record_error(DevScalars* sc, int code, int i, int j, int k) {
-  if (atomicCAS(&sc->err_code, 0, code) == 0) {
-    sc->err_i = i;
-    sc->err_j = j;
-    sc->err_k = k;
-  }
-}
-
-__device__ __forceinline__ size_t cidx(const GridDev& G, int i, int j, int k) {
-  return (size_t)i + (size_t)G.n[0] * ((size_t)j + (size_t)G.n[1] * (size_t)k);
-}
-
-// Primitives of an interior cell, derived from the state exactly as
-// rungekutta.f90:205-229 (primitive) and eos.f90:805-842 (internalenergy).
-template <bool MAG, bool GLM>
-__device__ __forceinline__ void interior_prim(const double* src, int src_prim, size_t plane, size_t c,
-                                              double phifac, double& d, double v[3], double& e, double b[3],
-                                              double& phi, double& eint) {
-  d = src[c];
-  if (src_prim) {
-    v[0] = src[plane + c];
-    v[1] = src[2 * plane + c];
-    v[2] = src[3 * plane + c];
-  } else {
-    v[0] = src[plane + c] / d;
-    v[1] = src[2 * plane + c] / d;
-    v[2] = src[3 * plane + c] / d;
-  }
-  e = src[4 * plane + c];
-  if (MAG) {
-    b[0] = src[5 * plane + c];
-    b[1] = src[6 * plane + c];
-    b[2] = src[7 * plane + c];
-  } else {
-    b[0] = b[1] = b[2] = 0.0;
-  }
-  phi = GLM ? src[8 * plane + c] * phifac : 0.0;
-  eint = get_eint<MAG>(e, d, v[0], v[1], v[2], b[0], b[1], b[2]);
-}
-
-// Staged quantities of any cell of a tile's region: interior cells directly,
-// ghost cells (at most one axis out of range) through the boundary codes
-// (boundarycondition.f90, codes 0 periodic, 1 reflective, 2 outgoing,
-// 3 free) followed by the ghost energy of boundarycondition.f90:222-243.
-template <bool MAG, bool GLM>
-__device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A, int i, int j, int k,
-                                           double q[NQ]) {
-  int c3[3] = {i, j, k};
-  int ax = -1;
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-    if (c3[a] < 0 || c3[a] >= G.n[a]) ax = a;
-  double d, v[3], e, b[3], phi, eint;
-  if (ax < 0) {
-    interior_prim<MAG, GLM>(A.src, A.src_prim, A.plane, cidx(G, i, j, k), A.phifac, d, v, e, b, phi, eint);
-    q[Q_D] = d;
-    q[Q_M + 0] = d * v[0];
-    q[Q_M + 1] = d * v[1];
-    q[Q_M + 2] = d * v[2];
-    q[Q_E] = e;
-    q[Q_B + 0] = b[0];
-    q[Q_B + 1] = b[1];
-    q[Q_B + 2] = b[2];
-    q[Q_PHI] = phi;
-    q[Q_EINT] = eint;
-    return;
-  }
-  const int n = G.n[ax];
-  const int s = c3[ax];
-  const int io = s < 0 ? 0 : 1;
-  const int gl = io == 0 ? s + 2 : s - n;  // ghost layer 0 or 1
-  const int per = io == 0 ? n - 2 + gl : gl;
-  const int refl = io == 0 ? 1 - gl : n - 1 - gl;
-  const int edge = io == 0 ? 0 : n - 1;
-  const int bs = G.bc[ax][io][0], bv = G.bc[ax][io][1];
-  const int ss = bs == 0 ? per : (bs == 1 ? refl : edge);
-  const int sv = bv == 0 ? per : (bv == 1 ? refl : edge);
-  // scalar quantities (d, p, phi) from the scalar image cell
-  c3[ax] = ss;
-  interior_prim<MAG, GLM>(A.src, A.src_prim, A.plane, cidx(G, c3[0], c3[1], c3[2]), A.phifac, d, v, e, b, phi,
-                          eint);
-  const double dg = d;
-  const double pg = A.gm1 * eint;  // eos.f90:256 (pressure of the image cell)
-  const double phig = phi;
-  // vector quantities (v, B) from the vector image cell
-  if (sv != ss) {
-    c3[ax] = sv;
-    interior_prim<MAG, GLM>(A.src, A.src_prim, A.plane, cidx(G, c3[0], c3[1], c3[2]), A.phifac, d, v, e, b, phi,
-                            eint);
-  }
-  double vn = v[ax];
-  if (bv == 1) {
-    vn = -vn;
-    b[ax] = -b[ax];
-  } else if (bv == 2) {
-    if (io == 0) {
-      vn = ax == 0 ? fmin2(0.0, vn) : vn * (0.5 - fsign(0.5, vn));  // :165 and the y/z plug form
-    } else {
-      vn = vn * (0.5 + fsign(0.5, vn));
-    }
-  }
-  v[ax] = vn;
-  const double eg = pg / A.gm1;  // eos.f90:287-289
-  const double b1 = b[0], b2 = b[1], b3 = b[2];
-  q[Q_D] = dg;
-  q[Q_M + 0] = dg * v[0];
-  q[Q_M + 1] = dg * v[1];
-  q[Q_M + 2] = dg * v[2];
-  q[Q_E] = eg + 0.5 * (dg * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + b1 * b1 + b2 * b2 + b3 * b3);
-  q[Q_B + 0] = b1;
-  q[Q_B + 1] = b2;
-  q[Q_B + 2] = b3;
-  q[Q_PHI] = phig;
-  q[Q_EINT] = eg;
-}
-
-struct Smem {
-  double P[NQ][kMaxRegion];
-  double S[NS][kMaxSlope];
-  double F[9][kMaxFace];
-  double acc[9][kMaxCells];
+template <class TL>
+struct SmemT {
+  double P[NQ][TL::NR];
+  double S[NS][TL::NSB];
+  double F[9][TL::NFB];
 };
 
-template <bool MAG, bool GLM>
-__global__ void __launch_bounds__(kThreads, 2) stage_kernel(const GridDev G, const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+// One axis of the fused stage: slopes, face fluxes, flux divergence of the
+// thread's own cell added to acc[].
+template <int AX, bool MAG, bool GLM, class TL>
+__device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, const int t0[3],
+                                          const int T[3], double acc[9], double ch) {
+  constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ;
+  constexpr int SBX = TX + (AX == 0 ? 2 : 0), SBY = TY + (AX == 1 ? 2 : 0), SBZ = TZ + (AX == 2 ? 2 : 0);
+  constexpr int FBX = TX + (AX == 0 ? 1 : 0), FBY = TY + (AX == 1 ? 1 : 0), FBZ = TZ + (AX == 2 ? 1 : 0);
+  constexpr int NSB = SBX * SBY * SBZ, NFB = FBX * FBY * FBZ;
+  constexpr int SSTR = AX == 0 ? 1 : (AX == 1 ? SBX : SBX * SBY);
+  constexpr int FSTR = AX == 0 ? 1 : (AX == 1 ? FBX : FBX * FBY);
+  constexpr int cn = AX, c1 = (AX + 1) % 3, c2 = (AX + 2) % 3;
+  const AxisGeo& g = G.g[AX];
   const int tid = threadIdx.x;
-  if (A.sc->done) return;
+  constexpr int nsl = MAG ? NS : S_B;
 
-  // tile origin and effective extent
-  int bid = blockIdx.x;
-  int t0[3], T[3];
+  // ---- limited slopes of the tile +-1 along AX -------------------------------
+  for (int w = tid; w < NSB; w += TL::NT) {
+    const int sx = w % SBX, sy = (w / SBX) % SBY, sz = w / (SBX * SBY);
+    int lc[3] = {sx, sy, sz};
+    lc[AX] -= 1;
+    if (lc[AX] > T[AX] || lc[0] >= T[0] + (AX == 0) || lc[1] >= T[1] + (AX == 1) || lc[2] >= T[2] + (AX == 2))
+      continue;  // outside a ragged tile
+    int lm[3] = {lc[0], lc[1], lc[2]}, lp[3] = {lc[0], lc[1], lc[2]};
+    lm[AX] -= 1;
+    lp[AX] += 1;
+    const int r = TL::pidx(lc[0], lc[1], lc[2]);
+    const int rm = TL::pidx(lm[0], lm[1], lm[2]);
+    const int rp = TL::pidx(lp[0], lp[1], lp[2]);
+    const int cg = lc[AX] + t0[AX];  // global coordinate along AX
+    double sl[NS];
+    if (A.limiter == 0) {
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
-    int ti = bid % A.tiles[a];
-    bid /= A.tiles[a];
-    t0[a] = ti * A.tile[a];
-    T[a] = min(A.tile[a], G.n[a] - t0[a]);
+      for (int q = 0; q < NS; q++) sl[q] = 0.0;
+    } else {
+      constexpr int qmap[NS] = {Q_D, Q_E, Q_M + 0, Q_M + 1, Q_M + 2, Q_B + 0, Q_B + 1, Q_B + 2};
+      const double hl = g.hl[cg + 2], hr = g.hr[cg + 2];
+      double L[NS], R[NS];
+      if (A.limiter == 1) {
+        const double i0 = g.idx[cg + 2], i1 = g.idx[cg + 3], is = g.isum[cg + 2];
+#pragma unroll
+        for (int q = 0; q < nsl; q++) {
+          const double u0 = sm.P[qmap[q]][rm], u1 = sm.P[qmap[q]][r], u2 = sm.P[qmap[q]][rp];
+          const double du = lim_minmod(u0, u1, u2, i0, i1, is);
+          sl[q] = du;
+          L[q] = u1 - hl * du;
+          R[q] = u1 + hr * du;
+        }
+      } else {
+        const double cf = g.mcf[cg + 2], cb = g.mcb[cg + 2], ga = g.ga[cg + 2], gb = g.gb[cg + 2];
+#pragma unroll
+        for (int q = 0; q < nsl; q++) {
+          const double u0 = sm.P[qmap[q]][rm], u1 = sm.P[qmap[q]][r], u2 = sm.P[qmap[q]][rp];
+          const double du = lim_mmc(u0, u1, u2, cf, cb, ga, gb);
+          sl[q] = du;
+          L[q] = u1 - hl * du;
+          R[q] = u1 + hr * du;
+        }
+      }
+#pragma unroll
+      for (int q = nsl; q < NS; q++) sl[q] = 0.0;
+      // admissibility of the face internal energies (interpolation.f90:147-163)
+      double eintl = L[S_E] - 0.5 * (L[S_M] * L[S_M] + L[S_M + 1] * L[S_M + 1] + L[S_M + 2] * L[S_M + 2]) / L[S_D];
+      double eintr = R[S_E] - 0.5 * (R[S_M] * R[S_M] + R[S_M + 1] * R[S_M + 1] + R[S_M + 2] * R[S_M + 2]) / R[S_D];
+      if (MAG) {
+        eintl = eintl - 0.5 * (L[S_B] * L[S_B] + L[S_B + 1] * L[S_B + 1] + L[S_B + 2] * L[S_B + 2]);
+        eintr = eintr - 0.5 * (R[S_B] * R[S_B] + R[S_B + 1] * R[S_B + 1] + R[S_B + 2] * R[S_B + 2]);
+      }
+      const double em = sm.P[Q_EINT][rm], e0 = sm.P[Q_EINT][r], ep = sm.P[Q_EINT][rp];
+      if (eintl >= fmax2(em, e0) || eintl <= fmin2(em, e0) || eintr >= fmax2(e0, ep) || eintr <= fmin2(e0, ep)) {
+#pragma unroll
+        for (int q = 0; q < NS; q++) sl[q] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < nsl; q++) sm.S[q][w] = sl[q];
   }
-  const int ncell = T[0] * T[1] * T[2];
-  const int nvar = A.nvar;
-  for (int w = tid; w < ncell; w += kThreads)
-    for (int q = 0; q < 9; q++) sm.acc[q][w] = 0.0;
+  __syncthreads();
 
-  const double ch = A.sc->ch;
-  const int nsl = MAG ? NS : S_B;
-
-  for (int a = 0; a < 3; a++) {
-    if (!G.solve[a]) continue;
-    const AxisGeo& g = G.g[a];
-    // ---- 1. stage the region (tile +-2 along a) ---------------------------
-    int R[3] = {T[0], T[1], T[2]};
-    R[a] += 4;
-    int r0[3] = {t0[0], t0[1], t0[2]};
-    r0[a] -= 2;
-    const int nreg = R[0] * R[1] * R[2];
-    __syncthreads();  // previous axis finished with P/S/F
-    for (int w = tid; w < nreg; w += kThreads) {
-      int rx = w % R[0], ry = (w / R[0]) % R[1], rz = w / (R[0] * R[1]);
-      double q[NQ];
-      stage_cell<MAG, GLM>(G, A, r0[0] + rx, r0[1] + ry, r0[2] + rz, q);
-#pragma unroll
-      for (int k = 0; k < NQ; k++) sm.P[k][w] = q[k];
+  // ---- HLLD fluxes on the T+1 faces along AX --------------------------------
+  for (int w = tid; w < NFB; w += TL::NT) {
+    const int fx = w % FBX, fy = (w / FBX) % FBY, fz = w / (FBX * FBY);
+    int fc[3] = {fx, fy, fz};
+    const int f = fc[AX];  // face between local cells f-1 and f
+    if (f > T[AX] || fx >= T[0] + (AX == 0) || fy >= T[1] + (AX == 1) || fz >= T[2] + (AX == 2)) continue;
+    int lL[3] = {fx, fy, fz};
+    lL[AX] = f - 1;
+    int lR[3] = {lL[0], lL[1], lL[2]};
+    lR[AX] = f;
+    const int rL = TL::pidx(lL[0], lL[1], lL[2]), rR = TL::pidx(lR[0], lR[1], lR[2]);
+    const int sL = fx + SBX * (fy + SBY * fz);  // slope-box index of the left cell (coordinate f along AX)
+    const int sR = sL + SSTR;
+    const int gL = t0[AX] + f - 1;
+    const double dx1 = g.hr[gL + 2];  // xi(i)-x(i)
+    const double dx2 = g.hl[gL + 3];  // x(i+1)-xi(i)
+    const double dl = sm.P[Q_D][rL] + dx1 * sm.S[S_D][sL];
+    const double dr = sm.P[Q_D][rR] - dx2 * sm.S[S_D][sR];
+    const double el = sm.P[Q_E][rL] + dx1 * sm.S[S_E][sL];
+    const double er = sm.P[Q_E][rR] - dx2 * sm.S[S_E][sR];
+    const double v1l = (sm.P[Q_M + cn][rL] + dx1 * sm.S[S_M + cn][sL]) / dl;
+    const double v1r = (sm.P[Q_M + cn][rR] - dx2 * sm.S[S_M + cn][sR]) / dr;
+    const double v2l = (sm.P[Q_M + c1][rL] + dx1 * sm.S[S_M + c1][sL]) / dl;
+    const double v2r = (sm.P[Q_M + c1][rR] - dx2 * sm.S[S_M + c1][sR]) / dr;
+    const double v3l = (sm.P[Q_M + c2][rL] + dx1 * sm.S[S_M + c2][sL]) / dl;
+    const double v3r = (sm.P[Q_M + c2][rR] - dx2 * sm.S[S_M + c2][sR]) / dr;
+    double b1l = 0.0, b1r = 0.0, b2l = 0.0, b2r = 0.0, b3l = 0.0, b3r = 0.0, phil = 0.0, phir = 0.0;
+    if (MAG) {
+      b1l = sm.P[Q_B + cn][rL] + dx1 * sm.S[S_B + cn][sL];
+      b1r = sm.P[Q_B + cn][rR] - dx2 * sm.S[S_B + cn][sR];
+      b2l = sm.P[Q_B + c1][rL] + dx1 * sm.S[S_B + c1][sL];
+      b2r = sm.P[Q_B + c1][rR] - dx2 * sm.S[S_B + c1][sR];
+      b3l = sm.P[Q_B + c2][rL] + dx1 * sm.S[S_B + c2][sL];
+      b3r = sm.P[Q_B + c2][rR] - dx2 * sm.S[S_B + c2][sR];
+      // phi is never reconstructed: its slope is identically zero (allocations.f90)
+      phil = sm.P[Q_PHI][rL] + dx1 * 0.0;
+      phir = sm.P[Q_PHI][rR] - dx2 * 0.0;
     }
-    const int rstride = a == 0 ? 1 : (a == 1 ? R[0] : R[0] * R[1]);
-    __syncthreads();
-
-    // ---- 2. limited slopes for the tile +-1 along a -----------------------
-    int SB[3] = {T[0], T[1], T[2]};
-    SB[a] += 2;
-    const int nsb = SB[0] * SB[1] * SB[2];
-    const int sstride = a == 0 ? 1 : (a == 1 ? SB[0] : SB[0] * SB[1]);
-    for (int w = tid; w < nsb; w += kThreads) {
-      int sx = w % SB[0], sy = (w / SB[0]) % SB[1], sz = w / (SB[0] * SB[1]);
-      int rc[3] = {sx, sy, sz};
-      rc[a] += 1;
-      const int r = rc[0] + R[0] * (rc[1] + R[1] * rc[2]);
-      const int cg = (a == 0 ? sx : (a == 1 ? sy : sz)) + t0[a] - 1;  // global coordinate along a
-      double sl[NS];
-      if (A.limiter == 0) {
+    const double eil = get_eint<MAG>(el, dl, v1l, v2l, v3l, b1l, b2l, b3l);
+    const double eir = get_eint<MAG>(er, dr, v1r, v2r, v3r, b1r, b2r, b3r);
+    double fl[9];
+    if (eil <= 0.0 || dl <= 0.0 || eir <= 0.0 || dr <= 0.0) {
+      int gi[3] = {t0[0] + fx, t0[1] + fy, t0[2] + fz};
+      gi[AX] = gL;
+      record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);  // numflux.f90:117 -> error_flux
 #pragma unroll
-        for (int k = 0; k < NS; k++) sl[k] = 0.0;
-      } else {
-        const double hl = g.hl[cg + 2], hr = g.hr[cg + 2];
-        double L[NS], Rv[NS];
-        // slope inputs in the order d, e, m1, m2, m3, b1, b2, b3
-        const int qmap[NS] = {Q_D, Q_E, Q_M + 0, Q_M + 1, Q_M + 2, Q_B + 0, Q_B + 1, Q_B + 2};
-        if (A.limiter == 1) {
-          const double i0 = g.idx[cg + 2], i1 = g.idx[cg + 3], is = g.isum[cg + 2];
-#pragma unroll
-          for (int k = 0; k < NS; k++) {
-            if (k >= nsl) { sl[k] = 0.0; continue; }
-            const double u0 = sm.P[qmap[k]][r - rstride], u1 = sm.P[qmap[k]][r], u2 = sm.P[qmap[k]][r + rstride];
-            const double du = lim_minmod(u0, u1, u2, i0, i1, is);
-            sl[k] = du;
-            L[k] = u1 - hl * du;
-            Rv[k] = u1 + hr * du;
-          }
-        } else {
-          const double cf = g.mcf[cg + 2], cb = g.mcb[cg + 2], ga = g.ga[cg + 2], gb = g.gb[cg + 2];
-#pragma unroll
-          for (int k = 0; k < NS; k++) {
-            if (k >= nsl) { sl[k] = 0.0; continue; }
-            const double u0 = sm.P[qmap[k]][r - rstride], u1 = sm.P[qmap[k]][r], u2 = sm.P[qmap[k]][r + rstride];
-            const double du = lim_mmc(u0, u1, u2, cf, cb, ga, gb);
-            sl[k] = du;
-            L[k] = u1 - hl * du;
-            Rv[k] = u1 + hr * du;
-          }
-        }
-        // admissibility of the face internal energies (interpolation.f90:147-163)
-        double eintl = L[S_E] - 0.5 * (L[S_M] * L[S_M] + L[S_M + 1] * L[S_M + 1] + L[S_M + 2] * L[S_M + 2]) / L[S_D];
-        double eintr =
-            Rv[S_E] - 0.5 * (Rv[S_M] * Rv[S_M] + Rv[S_M + 1] * Rv[S_M + 1] + Rv[S_M + 2] * Rv[S_M + 2]) / Rv[S_D];
-        if (MAG) {
-          eintl = eintl - 0.5 * (L[S_B] * L[S_B] + L[S_B + 1] * L[S_B + 1] + L[S_B + 2] * L[S_B + 2]);
-          eintr = eintr - 0.5 * (Rv[S_B] * Rv[S_B] + Rv[S_B + 1] * Rv[S_B + 1] + Rv[S_B + 2] * Rv[S_B + 2]);
-        }
-        const double em = sm.P[Q_EINT][r - rstride], e0 = sm.P[Q_EINT][r], ep = sm.P[Q_EINT][r + rstride];
-        if (eintl >= fmax2(em, e0) || eintl <= fmin2(em, e0) || eintr >= fmax2(e0, ep) || eintr <= fmin2(e0, ep)) {
-#pragma unroll
-          for (int k = 0; k < NS; k++) sl[k] = 0.0;
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < NS; k++) sm.S[k][w] = sl[k];
+      for (int q = 0; q < 9; q++) fl[q] = 0.0;
+    } else {
+      // eos_p_cs (eos.f90:209-219) with erad = 0
+      const double ptl0 = A.gm1 * eil, ptr0 = A.gm1 * eir;
+      const double csl = sqrt(A.gamma * ptl0 / dl), csr = sqrt(A.gamma * ptr0 / dr);
+      const double ptl = ptl0 + 0.5 * (b1l * b1l + b2l * b2l + b3l * b3l);
+      const double ptr = ptr0 + 0.5 * (b1r * b1r + b2r * b2r + b3r * b3r);
+      const double cfl = get_cf(dl, csl, b1l, b2l, b3l);
+      const double cfr = get_cf(dr, csr, b1r, b2r, b3r);
+      hlld(fl, cfl, cfr, v1l, v1r, v2l, v2r, v3l, v3r, dl, dr, el, er, ptl, ptr, b1l, b1r, b2l, b2r, b3l, b3r, phil,
+           phir, ch);
     }
-    __syncthreads();
-
-    // ---- 3. HLLD fluxes on the T+1 faces along a ---------------------------
-    int FB[3] = {T[0], T[1], T[2]};
-    FB[a] += 1;
-    const int nfb = FB[0] * FB[1] * FB[2];
-    const int cn = a, c1 = (a + 1) % 3, c2 = (a + 2) % 3;  // normal and tangential components
-    for (int w = tid; w < nfb; w += kThreads) {
-      int fx = w % FB[0], fy = (w / FB[0]) % FB[1], fz = w / (FB[0] * FB[1]);
-      int fc[3] = {fx, fy, fz};
-      const int f = fc[a];
-      // left cell: slope-box coordinate f along a, region coordinate f+1
-      int sc3[3] = {fx, fy, fz};
-      const int sL = sc3[0] + SB[0] * (sc3[1] + SB[1] * sc3[2]);
-      const int sR = sL + sstride;
-      int rc[3] = {fx, fy, fz};
-      rc[a] += 1;
-      const int rL = rc[0] + R[0] * (rc[1] + R[1] * rc[2]);
-      const int rR = rL + rstride;
-      const int gLc = t0[a] - 1 + f;  // global coordinate of the left cell
-      const double dx1 = g.hr[gLc + 2];      // xi(i)-x(i)
-      const double dx2 = g.hl[gLc + 3];      // x(i+1)-xi(i)
-      const double dl = sm.P[Q_D][rL] + dx1 * sm.S[S_D][sL];
-      const double dr = sm.P[Q_D][rR] - dx2 * sm.S[S_D][sR];
-      const double el = sm.P[Q_E][rL] + dx1 * sm.S[S_E][sL];
-      const double er = sm.P[Q_E][rR] - dx2 * sm.S[S_E][sR];
-      const double v1l = (sm.P[Q_M + cn][rL] + dx1 * sm.S[S_M + cn][sL]) / dl;
-      const double v1r = (sm.P[Q_M + cn][rR] - dx2 * sm.S[S_M + cn][sR]) / dr;
-      const double v2l = (sm.P[Q_M + c1][rL] + dx1 * sm.S[S_M + c1][sL]) / dl;
-      const double v2r = (sm.P[Q_M + c1][rR] - dx2 * sm.S[S_M + c1][sR]) / dr;
-      const double v3l = (sm.P[Q_M + c2][rL] + dx1 * sm.S[S_M + c2][sL]) / dl;
-      const double v3r = (sm.P[Q_M + c2][rR] - dx2 * sm.S[S_M + c2][sR]) / dr;
-      double b1l = 0.0, b1r = 0.0, b2l = 0.0, b2r = 0.0, b3l = 0.0, b3r = 0.0, phil = 0.0, phir = 0.0;
-      if (MAG) {
-        b1l = sm.P[Q_B + cn][rL] + dx1 * sm.S[S_B + cn][sL];
-        b1r = sm.P[Q_B + cn][rR] - dx2 * sm.S[S_B + cn][sR];
-        b2l = sm.P[Q_B + c1][rL] + dx1 * sm.S[S_B + c1][sL];
-        b2r = sm.P[Q_B + c1][rR] - dx2 * sm.S[S_B + c1][sR];
-        b3l = sm.P[Q_B + c2][rL] + dx1 * sm.S[S_B + c2][sL];
-        b3r = sm.P[Q_B + c2][rR] - dx2 * sm.S[S_B + c2][sR];
-        // phi is never reconstructed: its slope is identically zero (allocations.f90)
-        phil = sm.P[Q_PHI][rL] + dx1 * 0.0;
-        phir = sm.P[Q_PHI][rR] - dx2 * 0.0;
-      }
-      const double eil = get_eint<MAG>(el, dl, v1l, v2l, v3l, b1l, b2l, b3l);
-      const double eir = get_eint<MAG>(er, dr, v1r, v2r, v3r, b1r, b2r, b3r);
-      double fl[9];
-      if (eil <= 0.0 || dl <= 0.0 || eir <= 0.0 || dr <= 0.0) {
-        int gi[3] = {t0[0] + fx, t0[1] + fy, t0[2] + fz};
-        gi[a] = gLc;
-        record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);  // numflux.f90:117 -> error_flux
-#pragma unroll
-        for (int k = 0; k < 9; k++) fl[k] = 0.0;
-      } else {
-        // eos_p_cs (eos.f90:209-219) with erad = 0
-        const double ptl0 = A.gm1 * eil, ptr0 = A.gm1 * eir;
-        const double csl = sqrt(A.gamma * ptl0 / dl), csr = sqrt(A.gamma * ptr0 / dr);
-        const double ptl = ptl0 + 0.5 * (b1l * b1l + b2l * b2l + b3l * b3l);
-        const double ptr = ptr0 + 0.5 * (b1r * b1r + b2r * b2r + b3r * b3r);
-        const double cfl = get_cf(dl, csl, b1l, b2l, b3l);
-        const double cfr = get_cf(dr, csr, b1r, b2r, b3r);
-        hlld(fl, cfl, cfr, v1l, v1r, v2l, v2r, v3l, v3r, dl, dr, el, er, ptl, ptr, b1l, b1r, b2l, b2r, b3l, b3r,
-             phil, phir, ch);
-      }
-      // rotate back into the conserved slots (numflux.f90:186-198, 359-371, 531-543)
-      sm.F[ICNT][w] = fl[0];
-      sm.F[IMO1 + cn][w] = fl[1];
-      sm.F[IMO1 + c1][w] = fl[2];
-      sm.F[IMO1 + c2][w] = fl[3];
-      sm.F[IENE][w] = fl[4];
-      if (MAG) {
-        sm.F[IMG1 + cn][w] = fl[5];
-        sm.F[IMG1 + c1][w] = fl[6];
-        sm.F[IMG1 + c2][w] = fl[7];
-        if (GLM) sm.F[I9WV][w] = fl[8];
-      }
-    }
-    __syncthreads();
-
-    // ---- 4. flux divergence along a ---------------------------------------
-    const int fstride = a == 0 ? 1 : (a == 1 ? FB[0] : FB[0] * FB[1]);
-    for (int w = tid; w < ncell; w += kThreads) {
-      int cx = w % T[0], cy = (w / T[0]) % T[1], cz = w / (T[0] * T[1]);
-      const int wm = cx + FB[0] * (cy + FB[1] * cz);  // face on the low side
-      const int wp = wm + fstride;
-      const int cga = (a == 0 ? cx : (a == 1 ? cy : cz)) + t0[a];
-      const double idxi = g.idxi[cga + 2];
-      for (int q = 0; q < nvar; q++) sm.acc[q][w] = sm.acc[q][w] + idxi * (sm.F[q][wm] - sm.F[q][wp]);
+    // rotate back into the conserved slots (numflux.f90:186-198, 359-371, 531-543)
+    sm.F[ICNT][w] = fl[0];
+    sm.F[IMO1 + cn][w] = fl[1];
+    sm.F[IMO1 + c1][w] = fl[2];
+    sm.F[IMO1 + c2][w] = fl[3];
+    sm.F[IENE][w] = fl[4];
+    if (MAG) {
+      sm.F[IMG1 + cn][w] = fl[5];
+      sm.F[IMG1 + c1][w] = fl[6];
+      sm.F[IMG1 + c2][w] = fl[7];
+      if (GLM) sm.F[I9WV][w] = fl[8];
     }
   }
   __syncthreads();
 
-  // ---- RK combination (rungekutta.f90:35-59) + source (source.f90:70-85) ---
-  const double dtf = A.fact * A.sc->dt;
-  for (int w = tid; w < ncell; w += kThreads) {
-    int cx = w % T[0], cy = (w / T[0]) % T[1], cz = w / (T[0] * T[1]);
-    const int i = t0[0] + cx, j = t0[1] + cy, k = t0[2] + cz;
-    const size_t c = cidx(G, i, j, k);
-    double src[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const bool grav = A.gphi != nullptr;
-    if (grav) {
-      double d, v[3], e, b[3], phi, eint;
-      interior_prim<MAG, GLM>(A.src, A.src_prim, A.plane, c, A.phifac, d, v, e, b, phi, eint);
-      double frc[3];
-      int ijk[3] = {i, j, k};
-      for (int a = 0; a < 3; a++) {
-        const AxisGeo& g = G.g[a];
-        const int s = ijk[a];
-        // neighbours of the potential with the ghost images of the
-        // boundary (periodic copy, or phi ~ 1/r elsewhere)
-        double ph[3];
-        for (int o = -1; o <= 1; o++) {
-          int nb[3] = {i, j, k};
-          nb[a] = s + o;
-          if (nb[a] >= 0 && nb[a] < G.n[a]) {
-            ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
-          } else if (G.bc[a][0][0] == 0) {
-            nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
-            ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
-          } else {
-            // Robin image phi_g = phi_edge * r_edge / r_g
-            int ed[3] = {i, j, k};
-            const double xe = G.g[0].x[ed[0] + 2], ye = G.g[1].x[ed[1] + 2], ze = G.g[2].x[ed[2] + 2];
-            const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
-            const double re = sqrt(xe * xe + ye * ye + ze * ze), rg = sqrt(xg * xg + yg * yg + zg * zg);
-            ph[o + 1] = A.gphi[c] * re / rg;
-          }
-        }
-        const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
-        frc[a] = -((dxm * ip * ph[2] - dxp * im * ph[0]) / (dxm + dxp) + (dxp - dxm) * im * ip * ph[1]) * d;
+  // ---- flux divergence of the thread's own cell -------------------------------
+  if (tid < TL::NC) {
+    const int cx = tid % TX, cy = (tid / TX) % TY, cz = tid / (TX * TY);
+    const int cc[3] = {cx, cy, cz};
+    if (cx < T[0] && cy < T[1] && cz < T[2]) {
+      const int wm = cx + FBX * (cy + FBY * cz);  // face on the low side
+      const int wp = wm + FSTR;
+      const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
+      constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
+#pragma unroll
+      for (int q = 0; q < nv; q++) acc[q] = acc[q] + idxi * (sm.F[q][wm] - sm.F[q][wp]);
+    }
+  }
+  __syncthreads();  // S and F are reused by the next axis
+}
+
+template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G, const StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
+  const int tid = threadIdx.x;
+  if (A.sc->done) return;
+
+  int bid = blockIdx.x;
+  int t0[3], T[3];
+  constexpr int TT[3] = {TL::TX, TL::TY, TL::TZ};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int ti = bid % A.tiles[a];
+    bid /= A.tiles[a];
+    t0[a] = ti * TT[a];
+    T[a] = min(TT[a], G.n[a] - t0[a]);
+  }
+
+  // ---- 1. stage the cross-shaped region --------------------------------------
+  // Every slot of the full-tile layout is one local cell (pidx and
+  // region_cell are inverse); a ragged tile needs the cells within two of
+  // its real extent, so its high halo occupies interior-layout slots.
+  for (int w = tid; w < TL::NR; w += TL::NT) {
+    int lc[3];
+    TL::region_cell(w, lc[0], lc[1], lc[2]);
+    int out = 0;
+    bool need = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (lc[a] < 0 || lc[a] >= T[a]) {
+        out++;
+        if (TT[a] == 1 || lc[a] < -2 || lc[a] > T[a] + 1) need = false;
       }
-      src[1] = frc[0];
-      src[2] = frc[1];
-      src[3] = frc[2];
-      src[4] = frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2];
     }
-    double un[9];
-    for (int q = 0; q < nvar; q++) {
-      double s = sm.acc[q][w];
-      if (grav && q >= 1 && q <= 4) s = s + src[q];
-      const double val = A.faco * A.uorg[q * A.plane + c] + A.facn * A.ucur[q * A.plane + c] + dtf * s;
-      un[q] = val;
-      A.uout[q * A.plane + c] = val;
+    if (!need || out > 1) continue;
+    double q[NQ];
+    stage_cell<MAG, GLM>(G, A, t0[0] + lc[0], t0[1] + lc[1], t0[2] + lc[2], q);
+#pragma unroll
+    for (int s = 0; s < NQ; s++) sm.P[s][w] = q[s];
+  }
+  __syncthreads();
+
+  double acc[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) acc[q] = 0.0;
+  const double ch = A.sc->ch;
+  if (TL::TX > 1 && G.solve[0]) axis_pass<0, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
+  if (TL::TY > 1 && G.solve[1]) axis_pass<1, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
+  if (TL::TZ > 1 && G.solve[2]) axis_pass<2, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
+
+  // ---- RK combination (rungekutta.f90:35-59) + source (source.f90:70-85) -------
+  if (tid >= TL::NC) return;
+  const int cx = tid % TL::TX, cy = (tid / TL::TX) % TL::TY, cz = tid / (TL::TX * TL::TY);
+  if (cx >= T[0] || cy >= T[1] || cz >= T[2]) return;
+  const int i = t0[0] + cx, j = t0[1] + cy, k = t0[2] + cz;
+  const size_t c = cidx(G, i, j, k);
+  const size_t pl = A.plane;
+  constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
+  if (A.gphi != nullptr) {
+    const double d = A.pin[c];
+    const double v[3] = {A.pin[PV * pl + c], A.pin[(PV + 1) * pl + c], A.pin[(PV + 2) * pl + c]};
+    double frc[3];
+    const int ijk[3] = {i, j, k};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const AxisGeo& g = G.g[a];
+      const int s = ijk[a];
+      // neighbours of the potential with the ghost images of the boundary
+      // (periodic copy, or the Robin image phi ~ 1/r)
+      double ph[3];
+#pragma unroll
+      for (int o = -1; o <= 1; o++) {
+        int nb[3] = {i, j, k};
+        nb[a] = s + o;
+        if (nb[a] >= 0 && nb[a] < G.n[a]) {
+          ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+        } else if (G.bc[a][0][0] == 0) {
+          nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
+          ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+        } else {
+          const double xe = G.g[0].x[i + 2], ye = G.g[1].x[j + 2], ze = G.g[2].x[k + 2];
+          const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
+          const double re = sqrt(xe * xe + ye * ye + ze * ze), rg = sqrt(xg * xg + yg * yg + zg * zg);
+          ph[o + 1] = A.gphi[c] * re / rg;
+        }
+      }
+      const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
+      frc[a] = -((dxm * ip * ph[2] - dxp * im * ph[0]) / (dxm + dxp) + (dxp - dxm) * im * ip * ph[1]) * d;
     }
-    // primitive + internalenergy check of the new state (eos.f90:833-839)
-    const double d = un[0];
-    const double v1 = un[1] / d, v2 = un[2] / d, v3 = un[3] / d;
-    const double eint =
-        get_eint<MAG>(un[4], d, v1, v2, v3, MAG ? un[5] : 0.0, MAG ? un[6] : 0.0, MAG ? un[7] : 0.0);
-    if (eint <= 0.0) record_error(A.sc, kENEG_EINT, i, j, k);
+    acc[1] = acc[1] + frc[0];
+    acc[2] = acc[2] + frc[1];
+    acc[3] = acc[3] + frc[2];
+    acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
+  }
+  const double dtf = A.fact * A.sc->dt;
+  double un[9];
+#pragma unroll
+  for (int q = 0; q < nv; q++) {
+    const double val = A.faco * A.uorg[q * pl + c] + A.facn * A.ucur[q * pl + c] + dtf * acc[q];
+    un[q] = val;
+    A.uout[q * pl + c] = val;
+  }
+  // primitive + pressure of the new state (rungekutta.f90:205-229, eos.f90:805-842)
+  const double d = un[0];
+  const double v1 = un[1] / d, v2 = un[2] / d, v3 = un[3] / d;
+  const double b1 = MAG ? un[5] : 0.0, b2 = MAG ? un[6] : 0.0, b3 = MAG ? un[7] : 0.0;
+  const double eint = get_eint<MAG>(un[4], d, v1, v2, v3, b1, b2, b3);
+  double* Po = A.pout;
+  Po[c] = d;
+  Po[PV * pl + c] = v1;
+  Po[(PV + 1) * pl + c] = v2;
+  Po[(PV + 2) * pl + c] = v3;
+  Po[PE * pl + c] = un[4];
+  Po[PB * pl + c] = b1;
+  Po[(PB + 1) * pl + c] = b2;
+  Po[(PB + 2) * pl + c] = b3;
+  Po[PPHI * pl + c] = GLM ? un[8] : 0.0;
+  Po[PEINT * pl + c] = eint;
+  if (eint <= 0.0) record_error(A.sc, kENEG_EINT, i, j, k);
+}
+
+// ---------------------------------------------------------------------------
+// P planes from the uploaded primitives (pressure at start-up, eos.f90:805-842)
+
+template <bool MAG>
+__global__ void prim_init_kernel(double* P, size_t plane) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
+    const double d = P[c], v1 = P[plane + c], v2 = P[2 * plane + c], v3 = P[3 * plane + c];
+    const double e = P[4 * plane + c];
+    const double b1 = MAG ? P[5 * plane + c] : 0.0, b2 = MAG ? P[6 * plane + c] : 0.0;
+    const double b3 = MAG ? P[7 * plane + c] : 0.0;
+    P[PEINT * plane + c] = get_eint<MAG>(e, d, v1, v2, v3, b1, b2, b3);
+  }
+}
+
+// P planes from conserved variables (rungekutta.f90:205-229 + eos.f90:805-842)
+template <bool MAG, bool GLM>
+__global__ void prim_from_u_kernel(const double* U, double* P, size_t plane) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
+    const double d = U[c];
+    const double v1 = U[plane + c] / d, v2 = U[2 * plane + c] / d, v3 = U[3 * plane + c] / d;
+    const double e = U[4 * plane + c];
+    const double b1 = MAG ? U[5 * plane + c] : 0.0, b2 = MAG ? U[6 * plane + c] : 0.0;
+    const double b3 = MAG ? U[7 * plane + c] : 0.0;
+    P[c] = d;
+    P[plane + c] = v1;
+    P[2 * plane + c] = v2;
+    P[3 * plane + c] = v3;
+    P[4 * plane + c] = e;
+    P[5 * plane + c] = b1;
+    P[6 * plane + c] = b2;
+    P[7 * plane + c] = b3;
+    P[8 * plane + c] = GLM ? U[8 * plane + c] : 0.0;
+    P[PEINT * plane + c] = get_eint<MAG>(e, d, v1, v2, v3, b1, b2, b3);
   }
 }
 
@@ -424,21 +371,20 @@ __global__ void __launch_bounds__(kThreads, 2) stage_kernel(const GridDev G, con
 
 __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
 
-template <bool MAG, bool GLM>
-__global__ void __launch_bounds__(256) cfl_kernel(const GridDev G, const double* src, int src_prim, size_t plane,
-                                                  double gamma, DevScalars* sc) {
+template <bool MAG>
+__global__ void __launch_bounds__(256) cfl_kernel(const GridDev G, const double* P, size_t plane, double gamma,
+                                                  DevScalars* sc) {
   if (sc->done) return;
   const double gm1 = gamma - 1.0;
-  const size_t ncell = plane;
   double my_dti = __longlong_as_double(0x7ff0000000000000LL);  // +inf
   double my_cf = 0.0;
   const double off0 = G.solve[0] ? 1.0 : 0.0, off1 = G.solve[1] ? 1.0 : 0.0, off2 = G.solve[2] ? 1.0 : 0.0;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (size_t)gridDim.x * blockDim.x) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(c % G.n[0]);
     const int j = (int)((c / G.n[0]) % G.n[1]);
     const int k = (int)(c / ((size_t)G.n[0] * G.n[1]));
-    double d, v[3], e, b[3], phi, eint;
-    interior_prim<MAG, GLM>(src, src_prim, plane, c, 1.0, d, v, e, b, phi, eint);
+    const double d = P[c], eint = P[PEINT * plane + c];
+    const double v1 = P[plane + c], v2 = P[2 * plane + c], v3 = P[3 * plane + c];
     if (eint <= 0.0 || d <= 0.0) {
       record_error(sc, kENEG_EINT, i, j, k);
       continue;
@@ -447,20 +393,20 @@ __global__ void __launch_bounds__(256) cfl_kernel(const GridDev G, const double*
     const double cs = sqrt(gamma * p / d);
     double cf1, cf2, cf3;
     if (MAG) {
-      cf1 = get_cf(d, cs, b[0], b[1], b[2]) + fabs(v[0]);
-      cf2 = get_cf(d, cs, b[1], b[0], b[2]) + fabs(v[1]);
-      cf3 = get_cf(d, cs, b[2], b[0], b[1]) + fabs(v[2]);
+      const double b1 = P[5 * plane + c], b2 = P[6 * plane + c], b3 = P[7 * plane + c];
+      cf1 = get_cf(d, cs, b1, b2, b3) + fabs(v1);
+      cf2 = get_cf(d, cs, b2, b1, b3) + fabs(v2);
+      cf3 = get_cf(d, cs, b3, b1, b2) + fabs(v3);
     } else {
-      cf1 = cs + fabs(v[0]);
-      cf2 = cs + fabs(v[1]);
-      cf3 = cs + fabs(v[2]);
+      cf1 = cs + fabs(v1);
+      cf2 = cs + fabs(v2);
+      cf3 = cs + fabs(v3);
     }
     const double dxi1 = G.g[0].dxi[i + 2], dxi2 = G.g[1].dxi[j + 2], dxi3 = G.g[2].dxi[k + 2];
     const double dvol = dxi1 * dxi2 * dxi3;  // metric.f90:45-48
     const double sa1 = dxi2 * dxi3, sa2 = dxi1 * dxi3, sa3 = dxi1 * dxi2;
     const double dti = dvol / (cf1 * off0 * (sa1 + sa1) + cf2 * off1 * (sa2 + sa2) + cf3 * off2 * (sa3 + sa3));
-    const double cm = fmax2(fmax2(cf1, cf2), cf3);
-    my_cf = fmax2(my_cf, cm);
+    my_cf = fmax2(my_cf, fmax2(fmax2(cf1, cf2), cf3));
     my_dti = fmin2(my_dti, dti);
   }
   // warp then block reduction; min/max are exact so the order is irrelevant
@@ -520,32 +466,17 @@ __global__ void cfl_finalize_kernel(DevScalars* sc) {
   sc->cfmax_bits = 0ULL;
 }
 
-// ---------------------------------------------------------------------------
-// layout kernels: primitives of the current state for download
-
-template <bool MAG, bool GLM>
-__global__ void prim_kernel(const GridDev G, const double* src, int src_prim, size_t plane, double phifac,
-                            double* out /* 9 planes d,v1,v2,v3,e,b1,b2,b3,phi */, double* p_out, double gm1) {
+// primitives of the current state for download: 9 planes (phi with the
+// pending phidamp factor) and the gas pressure
+__global__ void prim_out_kernel(const double* P, size_t plane, double phifac, double gm1, double* out,
+                                double* p_out) {
   for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
-    double d, v[3], e, b[3], phi, eint;
-    interior_prim<MAG, GLM>(src, src_prim, plane, c, phifac, d, v, e, b, phi, eint);
-    out[c] = d;
-    out[plane + c] = v[0];
-    out[2 * plane + c] = v[1];
-    out[3 * plane + c] = v[2];
-    out[4 * plane + c] = e;
-    out[5 * plane + c] = b[0];
-    out[6 * plane + c] = b[1];
-    out[7 * plane + c] = b[2];
-    out[8 * plane + c] = phi;
-    if (p_out) p_out[c] = gm1 * eint;
+#pragma unroll
+    for (int q = 0; q < 8; q++) out[q * plane + c] = P[q * plane + c];
+    out[8 * plane + c] = P[8 * plane + c] * phifac;
+    if (p_out) p_out[c] = gm1 * P[PEINT * plane + c];
   }
 }
-
-// ---------------------------------------------------------------------------
-// host-side launchers (called from hmn_capi.cu)
-
-size_t stage_smem_bytes() { return sizeof(Smem); }
 
 // time += dt; tn += 1; end check (hormone.f90:147-155) on the device clock
 __global__ void advance_kernel(DevScalars* sc) {
@@ -555,57 +486,101 @@ __global__ void advance_kernel(DevScalars* sc) {
   if (sc->endstyle == 1 && sc->time >= sc->t_end) sc->done = 1;
 }
 
-cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
-  advance_kernel<<<1, 32, 0, st>>>(sc);
-  return cudaGetLastError();
-}
+// ---------------------------------------------------------------------------
+// host-side launchers (called from hmn_capi.cu)
 
-template <bool MAG, bool GLM>
+template <bool MAG, bool GLM, class TL>
 static cudaError_t launch_stage_t(const GridDev& G, const StageArgs& A, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MAG, GLM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(Smem));
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MAG, GLM, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(SmemT<TL>));
     if (e != cudaSuccess) return e;
     attr = true;
   }
   const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
-  stage_kernel<MAG, GLM><<<blocks, kThreads, sizeof(Smem), st>>>(G, A);
+  stage_kernel<MAG, GLM, TL><<<blocks, TL::NT, sizeof(SmemT<TL>), st>>>(G, A);
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
-  if (mag && glm) return launch_stage_t<true, true>(G, A, st);
-  if (mag) return launch_stage_t<true, false>(G, A, st);
-  return launch_stage_t<false, false>(G, A, st);
+template <class TL>
+static cudaError_t launch_stage_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  if (mag && glm) return launch_stage_t<true, true, TL>(G, A, st);
+  if (mag) return launch_stage_t<true, false, TL>(G, A, st);
+  return launch_stage_t<false, false, TL>(G, A, st);
 }
 
-cudaError_t launch_cfl(const GridDev& G, const double* src, int src_prim, size_t plane, double gamma,
-                       DevScalars* sc, bool mag, bool glm, int nblocks, cudaStream_t st) {
-  if (mag && glm)
-    cfl_kernel<true, true><<<nblocks, 256, 0, st>>>(G, src, src_prim, plane, gamma, sc);
-  else if (mag)
-    cfl_kernel<true, false><<<nblocks, 256, 0, st>>>(G, src, src_prim, plane, gamma, sc);
+// tile shapes by solved axes: 3-D 8x8x8 (or 8x8x4 when HMN_TILE3D=884),
+// 2-D 16x16, 1-D 256
+void stage_tile(const int solve[3], int tile[3]) {
+  const int dim = solve[0] + solve[1] + solve[2];
+  for (int a = 0; a < 3; a++) tile[a] = 1;
+  if (dim == 3) {
+    const char* env = getenv("HMN_TILE3D");
+    const bool t884 = env && env[0] == '8' && env[1] == '8' && env[2] == '4';
+    tile[0] = 8;
+    tile[1] = 8;
+    tile[2] = t884 ? 4 : 8;
+  } else {
+    for (int a = 0; a < 3; a++)
+      if (solve[a]) tile[a] = dim == 2 ? 16 : 256;
+  }
+}
+
+cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  const int* t = A.tile;
+  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4>>(G, A, mag, glm, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1>>(G, A, mag, glm, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16>>(G, A, mag, glm, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16>>(G, A, mag, glm, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1>>(G, A, mag, glm, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1>>(G, A, mag, glm, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256>>(G, A, mag, glm, st);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_cfl(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc, bool mag,
+                       int nblocks, cudaStream_t st) {
+  if (mag)
+    cfl_kernel<true><<<nblocks, 256, 0, st>>>(G, P, plane, gamma, sc);
   else
-    cfl_kernel<false, false><<<nblocks, 256, 0, st>>>(G, src, src_prim, plane, gamma, sc);
+    cfl_kernel<false><<<nblocks, 256, 0, st>>>(G, P, plane, gamma, sc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   cfl_finalize_kernel<<<1, 32, 0, st>>>(sc);
   return cudaGetLastError();
 }
 
-cudaError_t launch_prim(const GridDev& G, const double* src, int src_prim, size_t plane, double phifac, double* out,
-                        double* p_out, double gm1, bool mag, bool glm, int nblocks, cudaStream_t st) {
-  if (mag && glm)
-    prim_kernel<true, true><<<nblocks, 256, 0, st>>>(G, src, src_prim, plane, phifac, out, p_out, gm1);
-  else if (mag)
-    prim_kernel<true, false><<<nblocks, 256, 0, st>>>(G, src, src_prim, plane, phifac, out, p_out, gm1);
+cudaError_t launch_prim_init(double* P, size_t plane, bool mag, int nblocks, cudaStream_t st) {
+  if (mag)
+    prim_init_kernel<true><<<nblocks, 256, 0, st>>>(P, plane);
   else
-    prim_kernel<false, false><<<nblocks, 256, 0, st>>>(G, src, src_prim, plane, phifac, out, p_out, gm1);
+    prim_init_kernel<false><<<nblocks, 256, 0, st>>>(P, plane);
   return cudaGetLastError();
 }
 
-}  // namespace hmn
+cudaError_t launch_prim_from_u(const double* U, double* P, size_t plane, bool mag, bool glm, int nblocks,
+                               cudaStream_t st) {
+  if (mag && glm)
+    prim_from_u_kernel<true, true><<<nblocks, 256, 0, st>>>(U, P, plane);
+  else if (mag)
+    prim_from_u_kernel<true, false><<<nblocks, 256, 0, st>>>(U, P, plane);
+  else
+    prim_from_u_kernel<false, false><<<nblocks, 256, 0, st>>>(U, P, plane);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double gm1, double* out, double* p_out,
+                            int nblocks, cudaStream_t st) {
+  prim_out_kernel<<<nblocks, 256, 0, st>>>(P, plane, phifac, gm1, out, p_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
+  advance_kernel<<<1, 32, 0, st>>>(sc);
+  return cudaGetLastError();
+}
 
 // ---------------------------------------------------------------------------
 // Hyperbolic self-gravity (gravity_hyperbolic.f90:61-125, 230-280) with a
@@ -613,8 +588,6 @@ cudaError_t launch_prim(const GridDev& G, const double* src, int src_prim, size_
 // coefficients of gravity_hyperbolic.f90:385-406 with unit radial weights;
 // each non-periodic face carries the Robin condition phi ~ 1/r folded into
 // the centre coefficient as gravity_hyperbolic.f90:400-404 does.
-
-namespace hmn {
 
 __device__ __forceinline__ double rdist(const GridDev& G, int i, int j, int k) {
   const double x = G.g[0].x[i + 2], y = G.g[1].x[j + 2], z = G.g[2].x[k + 2];
@@ -641,6 +614,7 @@ __global__ void __launch_bounds__(256) hg_stage_kernel(const GridDev G, const HG
     const int ijk[3] = {i, j, k};
     bool use_m[3] = {true, true, true}, use_p[3] = {true, true, true};
     size_t nbm[3], nbp[3];
+#pragma unroll
     for (int a = 0; a < 3; a++) {
       const int n = G.n[a];
       const bool per = G.bc[a][0][0] == 0;
@@ -666,6 +640,7 @@ __global__ void __launch_bounds__(256) hg_stage_kernel(const GridDev G, const HG
     const double cn = gx.dxi[i + 2] * gy.dxi[j + 2] * gz.dxi[k + 2];
     const double* ph = A.phi_in;
     double lap = c0 * ph[c];
+#pragma unroll
     for (int a = 0; a < 3; a++) {
       if (use_m[a]) lap = lap + cm[a] * ph[nbm[a]];
       if (use_p[a]) lap = lap + cp[a] * ph[nbp[a]];

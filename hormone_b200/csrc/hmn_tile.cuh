@@ -1,0 +1,169 @@
+// hmn_tile.cuh -- tile geometry and ghost-cell staging shared by the FP64
+// and the mixed-precision stage kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hmn_internal.h"
+#include "hmn_math.cuh"
+
+namespace hmn {
+
+// conserved slots (checksetup.f90:61-75)
+enum { ICNT = 0, IMO1 = 1, IENE = 4, IMG1 = 5, I9WV = 8 };
+// primitive planes in HBM
+enum { PD = 0, PV = 1, PE = 4, PB = 5, PPHI = 8, PEINT = 9, NP = 10 };
+// staged quantities per cell in shared memory: d, m1..3 (= d*v), e, b1..3, phi, eint
+enum { Q_D = 0, Q_M = 1, Q_E = 4, Q_B = 5, Q_PHI = 8, Q_EINT = 9, NQ = 10 };
+// slopes: d, e, m1..3, b1..3
+enum { S_D = 0, S_E = 1, S_M = 2, S_B = 5, NS = 8 };
+
+
+__device__ __forceinline__ void record_error(DevScalars* sc, int code, int i, int j, int k) {
+  if (atomicCAS(&sc->err_code, 0, code) == 0) {
+    sc->err_i = i;
+    sc->err_j = j;
+    sc->err_k = k;
+  }
+}
+
+__device__ __forceinline__ size_t cidx(const GridDev& G, int i, int j, int k) {
+  return (size_t)i + (size_t)G.n[0] * ((size_t)j + (size_t)G.n[1] * (size_t)k);
+}
+
+// Compile-time description of a tile: TX x TY x TZ cells (256 in all) and a
+// halo of two cells beyond each face of every axis with extent > 1.
+template <int TX_, int TY_, int TZ_, int NT_ = 256, int MINB_ = 2>
+struct Tile {
+  static constexpr int TX = TX_, TY = TY_, TZ = TZ_;
+  static constexpr int NT = NT_;      // threads per CTA (at least the tile's cell count)
+  static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget is sized for
+  static constexpr int NC = TX * TY * TZ;
+  static constexpr int HX = TX > 1 ? 2 : 0, HY = TY > 1 ? 2 : 0, HZ = TZ > 1 ? 2 : 0;
+  // region part 0: x-extended rows of every interior (j,k); part 1: y halos; part 2: z halos
+  static constexpr int N0 = (TX + 2 * HX) * TY * TZ;
+  static constexpr int N1 = TX * (2 * HY) * TZ;
+  static constexpr int N2 = TX * TY * (2 * HZ);
+  static constexpr int NR = N0 + N1 + N2;
+  static constexpr int maxi(int a, int b) { return a > b ? a : b; }
+  // slope and face boxes of the largest solved axis (axes of extent 1 are never swept)
+  static constexpr int NSB = maxi(maxi(HX ? (TX + 2) * TY * TZ : 1, HY ? TX * (TY + 2) * TZ : 1),
+                                  HZ ? TX * TY * (TZ + 2) : 1);
+  static constexpr int NFB = maxi(maxi(HX ? (TX + 1) * TY * TZ : 1, HY ? TX * (TY + 1) * TZ : 1),
+                                  HZ ? TX * TY * (TZ + 1) : 1);
+  // shared-memory slot of local cell (i,j,k); at most one coordinate lies outside the tile
+  __device__ static __forceinline__ int pidx(int i, int j, int k) {
+    if (HY && (j < 0 || j >= TY)) {
+      const int jj = j < 0 ? j + 2 : j - TY + 2;
+      return N0 + i + TX * (jj + 4 * k);
+    }
+    if (HZ && (k < 0 || k >= TZ)) {
+      const int kk = k < 0 ? k + 2 : k - TZ + 2;
+      return N0 + N1 + i + TX * (j + TY * kk);
+    }
+    return (i + HX) + (TX + 2 * HX) * (j + TY * k);
+  }
+  // local cell of region slot w
+  __device__ static __forceinline__ void region_cell(int w, int& i, int& j, int& k) {
+    if (w < N0) {
+      constexpr int RX = TX + 2 * HX;
+      i = w % RX - HX;
+      j = (w / RX) % TY;
+      k = w / (RX * TY);
+    } else if (w < N0 + N1) {
+      const int v = w - N0;
+      i = v % TX;
+      const int jj = (v / TX) % 4;
+      k = v / (TX * 4);
+      j = jj < 2 ? jj - 2 : TY + jj - 2;
+    } else {
+      const int v = w - N0 - N1;
+      i = v % TX;
+      j = (v / TX) % TY;
+      const int kk = v / (TX * TY);
+      k = kk < 2 ? kk - 2 : TZ + kk - 2;
+    }
+  }
+};
+
+// Staged quantities of a global cell (i,j,k): interior cells from P, ghost
+// cells (one axis out of range) through the boundary codes.
+template <bool MAG, bool GLM>
+__device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A, int i, int j, int k,
+                                           double* q /* NQ values */) {
+  const double* P = A.pin;
+  const size_t pl = A.plane;
+  int c3[3] = {i, j, k};
+  int ax = -1;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    if (c3[a] < 0 || c3[a] >= G.n[a]) ax = a;
+  if (ax < 0) {
+    const size_t c = cidx(G, i, j, k);
+    const double d = P[c];
+    q[Q_D] = d;
+    q[Q_M + 0] = d * P[PV * pl + c];
+    q[Q_M + 1] = d * P[(PV + 1) * pl + c];
+    q[Q_M + 2] = d * P[(PV + 2) * pl + c];
+    q[Q_E] = P[PE * pl + c];
+    if (MAG) {
+      q[Q_B + 0] = P[PB * pl + c];
+      q[Q_B + 1] = P[(PB + 1) * pl + c];
+      q[Q_B + 2] = P[(PB + 2) * pl + c];
+    } else {
+      q[Q_B + 0] = q[Q_B + 1] = q[Q_B + 2] = 0.0;
+    }
+    q[Q_PHI] = GLM ? P[PPHI * pl + c] * A.phifac : 0.0;
+    q[Q_EINT] = P[PEINT * pl + c];
+    return;
+  }
+  const int n = G.n[ax];
+  const int s = c3[ax];
+  const int io = s < 0 ? 0 : 1;
+  const int gl = io == 0 ? s + 2 : s - n;  // ghost layer 0 or 1
+  const int per = io == 0 ? n - 2 + gl : gl;
+  const int refl = io == 0 ? 1 - gl : n - 1 - gl;
+  const int edge = io == 0 ? 0 : n - 1;
+  const int bs = G.bc[ax][io][0], bv = G.bc[ax][io][1];
+  c3[ax] = bs == 0 ? per : (bs == 1 ? refl : edge);
+  const size_t cs = cidx(G, c3[0], c3[1], c3[2]);  // scalar image (d, p, phi)
+  c3[ax] = bv == 0 ? per : (bv == 1 ? refl : edge);
+  const size_t cv = cidx(G, c3[0], c3[1], c3[2]);  // vector image (v, B)
+  const double dg = P[cs];
+  const double pg = A.gm1 * P[PEINT * pl + cs];  // pressure of the image cell (eos.f90:256)
+  const double phig = GLM ? P[PPHI * pl + cs] * A.phifac : 0.0;
+  double v[3] = {P[PV * pl + cv], P[(PV + 1) * pl + cv], P[(PV + 2) * pl + cv]};
+  double b[3] = {0.0, 0.0, 0.0};
+  if (MAG) {
+    b[0] = P[PB * pl + cv];
+    b[1] = P[(PB + 1) * pl + cv];
+    b[2] = P[(PB + 2) * pl + cv];
+  }
+  double vn = v[ax];
+  if (bv == 1) {
+    vn = -vn;
+    b[ax] = -b[ax];
+  } else if (bv == 2) {
+    if (io == 0)
+      vn = ax == 0 ? fmin2(0.0, vn) : vn * (0.5 - fsign(0.5, vn));  // :165 and the y/z plug form
+    else
+      vn = vn * (0.5 + fsign(0.5, vn));
+  }
+  v[ax] = vn;
+  const double eg = pg / A.gm1;  // eos.f90:287-289
+  const double b1 = b[0], b2 = b[1], b3 = b[2];
+  q[Q_D] = dg;
+  q[Q_M + 0] = dg * v[0];
+  q[Q_M + 1] = dg * v[1];
+  q[Q_M + 2] = dg * v[2];
+  q[Q_E] = eg + 0.5 * (dg * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + b1 * b1 + b2 * b2 + b3 * b3);
+  q[Q_B + 0] = b1;
+  q[Q_B + 1] = b2;
+  q[Q_B + 2] = b3;
+  q[Q_PHI] = phig;
+  q[Q_EINT] = eg;
+}
+
+
+}  // namespace hmn
