@@ -47,6 +47,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope"], default="ot3d",
+                    help="ot3d: the headline (3-D Orszag-Tang 256^3); kh-batch: 512 uneven 2-D KH boxes batched vs "
+                         "one at a time; serve: a Poisson request stream through the continuous-batching server; "
+                         "polytrope: 192^3 self-gravitating polytrope with hyperbolic gravity")
+    ap.add_argument("--boxes", type=int, default=512)
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--precision", type=int, default=0)
     return ap.parse_args()
 
 
@@ -370,8 +378,100 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_kh_batch(args):
+    """512 periodic KH boxes, edges round(128*4^u) with u ~ U[0,1] (seeded):
+    K steps of every box in one batch (persistent launches, autotuned
+    schedule, CUDA graph) against the same K steps box by box."""
+    import math
+
+    import numpy as np
+    import torch
+
+    from hormone_b200 import autotune, config, grid as G, ic
+    from hormone_b200.batch import Batch, footprint
+    from hormone_b200.sim import Simulation
+
+    rng = np.random.Generator(np.random.PCG64(20261203))
+    boxes = []
+    for b in range(args.boxes):
+        n = int(round(128 * 4 ** rng.uniform()))
+        ratio, bx = float(rng.uniform(1, 4)), float(rng.uniform(0, 0.1))
+        ov = dict(ie=n, je=n, ke=1, mag_on=True, gamma=1.6666666666666667, t_end=2.0, dt_out=2.0,
+                  xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5)
+        cfg = config.resolve("kh_batch", overrides=ov)
+        boxes.append((cfg, ic.kelvin_helmholtz(cfg, G.make_grid(cfg), ratio, bx)))
+    cells = sum(int(np.prod(c["n"])) for c, _ in boxes)
+    K = args.steps
+    sched = autotune.tune(boxes[:32], precision=args.precision, steps=2, cache=None)
+    b = Batch(sum(footprint(c) for c, _ in boxes) + (1 << 26), max_sims=args.boxes + 1, precision=args.precision)
+    for c, p in boxes:
+        assert b.add(c, p) is not None
+    autotune.apply(b, sched)
+    stream = torch.cuda.ExternalStream(b.stream_ptr())
+    b.step(args.warmup)
+    b.sync()
+    l0 = b.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(K)
+    e1.record(stream)
+    e1.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    launches_b = b.launches() - l0
+    b.close()
+    # one at a time: every box's K steps through its own context, box after box
+    sims = [Simulation(c, p, precision=args.precision) for c, p in boxes]
+    for s_ in sims:
+        s_.run_device(max_steps=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    l1 = sum(s_.ctx.launches() for s_ in sims)
+    for s_ in sims:
+        s_.ctx.run(s_.time, s_.t_end, K)
+    for s_ in sims:
+        s_.ctx.sync()
+    ms_1 = (time.perf_counter() - t0) * 1e3
+    launches_1 = sum(s_.ctx.launches() for s_ in sims) - l1
+    for s_ in sims:
+        s_.close()
+    line = {"metric": METRIC, "value": cells * K / (ms_b * 1e-3), "unit": METRIC, "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_b / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "mixed", "data": "synthetic",
+            "config": {"workload": f"kh-batch-{args.boxes}-boxes-128^2..512^2", "cells": cells,
+                       "schedule": {str(k): v for k, v in sched.items()}},
+            "one_at_a_time": {"value": cells * K / (ms_1 * 1e-3), "ms_per_step": ms_1 / K,
+                              "gpu_launches": launches_1},
+            "gpu_launches": launches_b, "speedup_vs_one_at_a_time": ms_1 / ms_b}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    from hormone_b200 import serve
+    from hormone_b200.batch import Batch
+
+    import torch
+
+    reqs = serve.make_requests(args.requests, rate=args.rate, seed=20261203)
+    free, total = torch.cuda.mem_get_info()
+    b = Batch(int(free * 0.6), max_sims=1024, precision=args.precision)
+    stats = serve.serve(reqs, b, chunk=8, keep_results=False)
+    b.close()
+    summ = stats.summary()
+    line = {"metric": METRIC, "value": summ["zone_updates_per_s"], "unit": METRIC, "n_gpus": 1,
+            "steps": summ["batch_steps"], "warmup": 0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "mixed", "data": "synthetic",
+            "config": {"workload": f"serve-{args.requests}-requests-poisson-{args.rate}/s",
+                       "pool_bytes": int(free * 0.6)},
+            "serve": summ}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "kh-batch":
+        return run_kh_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

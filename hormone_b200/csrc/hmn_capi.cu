@@ -636,6 +636,7 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
   rc = fetch_scalars(ctx);
   if (rc) return rc;
   const int tn0 = ctx->sc_h->tn;
+  const int pcur0 = ctx->pcur;
   int done = 0;
   const int chunk = ctx->par.rktype == 1 ? 1 : 8;  // rktype 1 swaps buffers on the host after each step
   while (done < max_steps) {
@@ -646,6 +647,10 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
     }
     done += n;
     rc = fetch_scalars(ctx);
+    // steps enqueued after the end time was reached did nothing on the device (every kernel
+    // returns once `done` is set), but enqueue_hydro flipped the primitive buffer for them:
+    // take the buffer parity from the steps that actually ran (each stage writes the other one)
+    ctx->pcur = (pcur0 + ctx->par.rktype * (ctx->sc_h->tn - tn0)) & 1;
     if (rc) return rc;
     if (ctx->sc_h->time >= t_end) break;
   }

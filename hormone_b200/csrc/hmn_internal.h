@@ -89,6 +89,23 @@ struct HGArgs {
   DevScalars* sc;
 };
 
+// One simulation of a batch, resident in device memory.  Every field the
+// batched kernels need to run a step of this grid on its own clock.
+struct SimDesc {
+  GridDev G;
+  double* U[3];       // conserved-state RK buffers (U^n in U[0])
+  double* P[2];       // primitive planes, ping-pong
+  size_t plane;
+  int tiles[3];
+  int pcur;           // P buffer of the current state
+  int nvar, limiter, rktype, glm;
+  int active;         // 0 for a free slot
+  double gamma, gm1;
+  double damp;        // phidamp factor exp(-alpha9wave*courant)
+  double phifac;      // pending phidamp factor for the next stage 1
+  DevScalars sc;      // this simulation's time, dt, ch, CFL reduction, errors
+};
+
 enum : int { kOK = 0, kEINVAL = -1, kENEG_EINT = -2, kECUDA = -3, kEBADCFG = -4, kENOMEM = -5, kETIMEOUT = -6 };
 
 }  // namespace hmn
@@ -108,4 +125,19 @@ cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double
                             int nblocks, cudaStream_t st);
 cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cudaStream_t st);
 cudaError_t launch_advance(DevScalars* sc, cudaStream_t st);
+// batched launchers over a work list of (sim, tile) items; tile_kind selects
+// the compile-time tile (see batch_tile_kind), grid = persistent CTAs
+int batch_tile_kind(const int solve[3]);
+int batch_tile_variants(int kind, int* tile_ids);
+void batch_tile_shape(int tile_id, int tile[3]);
+cudaError_t launch_batch_cfl(SimDesc* sims, const int2* items, int nitems, int kind, bool mag, int grid,
+                             cudaStream_t st);
+cudaError_t launch_batch_finalize(SimDesc* sims, int nsims, cudaStream_t st);
+cudaError_t launch_batch_stage(SimDesc* sims, const int2* items, int nitems, int kind, bool mag, bool glm,
+                               int stage, int rk, int precision, int grid, cudaStream_t st);
+cudaError_t launch_batch_advance(SimDesc* sims, int nsims, cudaStream_t st);
+int batch_stage_blocks_per_sm(int kind, bool mag, bool glm, int precision);
+cudaError_t launch_batch_stage_mixed(SimDesc* sims, const int2* items, int nitems, int kind, bool mag, bool glm,
+                                     int stage, int rk, int grid, cudaStream_t st);
+int batch_stage_mixed_blocks_per_sm(int kind, bool mag, bool glm);
 }  // namespace hmn

@@ -209,14 +209,13 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
   __syncthreads();  // S and F are reused by the next axis
 }
 
+// One tile of one RK stage; `tile_id` enumerates the tiles of the grid
+// (x fastest).  Shared by the single-grid and the batched kernels.
 template <bool MAG, bool GLM, class TL>
-__global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G, const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
+__device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, int tile_id) {
   const int tid = threadIdx.x;
-  if (A.sc->done) return;
 
-  int bid = blockIdx.x;
+  int bid = tile_id;
   int t0[3], T[3];
   constexpr int TT[3] = {TL::TX, TL::TY, TL::TZ};
 #pragma unroll
@@ -330,6 +329,14 @@ __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G
   if (eint <= 0.0) record_error(A.sc, kENEG_EINT, i, j, k);
 }
 
+template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G, const StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
+  if (A.sc->done) return;
+  stage_tile_exact<MAG, GLM, TL>(G, A, sm, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // P planes from the uploaded primitives (pressure at start-up, eos.f90:805-842)
 
@@ -371,45 +378,42 @@ __global__ void prim_from_u_kernel(const double* U, double* P, size_t plane) {
 
 __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
 
+// dti and the largest signal speed of one cell (dti_cell, timestep.f90:125-183,
+// eostype 0); false (and the error recorded) if eint <= 0 or d <= 0
 template <bool MAG>
-__global__ void __launch_bounds__(256) cfl_kernel(const GridDev G, const double* P, size_t plane, double gamma,
-                                                  DevScalars* sc) {
-  if (sc->done) return;
+__device__ __forceinline__ bool cfl_cell(const GridDev& G, const double* P, size_t plane, double gamma, size_t c,
+                                         int i, int j, int k, DevScalars* sc, double& dti, double& cfm) {
   const double gm1 = gamma - 1.0;
-  double my_dti = __longlong_as_double(0x7ff0000000000000LL);  // +inf
-  double my_cf = 0.0;
   const double off0 = G.solve[0] ? 1.0 : 0.0, off1 = G.solve[1] ? 1.0 : 0.0, off2 = G.solve[2] ? 1.0 : 0.0;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(c % G.n[0]);
-    const int j = (int)((c / G.n[0]) % G.n[1]);
-    const int k = (int)(c / ((size_t)G.n[0] * G.n[1]));
-    const double d = P[c], eint = P[PEINT * plane + c];
-    const double v1 = P[plane + c], v2 = P[2 * plane + c], v3 = P[3 * plane + c];
-    if (eint <= 0.0 || d <= 0.0) {
-      record_error(sc, kENEG_EINT, i, j, k);
-      continue;
-    }
-    const double p = gm1 * eint;
-    const double cs = sqrt(gamma * p / d);
-    double cf1, cf2, cf3;
-    if (MAG) {
-      const double b1 = P[5 * plane + c], b2 = P[6 * plane + c], b3 = P[7 * plane + c];
-      cf1 = get_cf(d, cs, b1, b2, b3) + fabs(v1);
-      cf2 = get_cf(d, cs, b2, b1, b3) + fabs(v2);
-      cf3 = get_cf(d, cs, b3, b1, b2) + fabs(v3);
-    } else {
-      cf1 = cs + fabs(v1);
-      cf2 = cs + fabs(v2);
-      cf3 = cs + fabs(v3);
-    }
-    const double dxi1 = G.g[0].dxi[i + 2], dxi2 = G.g[1].dxi[j + 2], dxi3 = G.g[2].dxi[k + 2];
-    const double dvol = dxi1 * dxi2 * dxi3;  // metric.f90:45-48
-    const double sa1 = dxi2 * dxi3, sa2 = dxi1 * dxi3, sa3 = dxi1 * dxi2;
-    const double dti = dvol / (cf1 * off0 * (sa1 + sa1) + cf2 * off1 * (sa2 + sa2) + cf3 * off2 * (sa3 + sa3));
-    my_cf = fmax2(my_cf, fmax2(fmax2(cf1, cf2), cf3));
-    my_dti = fmin2(my_dti, dti);
+  const double d = P[c], eint = P[PEINT * plane + c];
+  const double v1 = P[plane + c], v2 = P[2 * plane + c], v3 = P[3 * plane + c];
+  if (eint <= 0.0 || d <= 0.0) {
+    record_error(sc, kENEG_EINT, i, j, k);
+    return false;
   }
-  // warp then block reduction; min/max are exact so the order is irrelevant
+  const double p = gm1 * eint;
+  const double cs = sqrt(gamma * p / d);
+  double cf1, cf2, cf3;
+  if (MAG) {
+    const double b1 = P[5 * plane + c], b2 = P[6 * plane + c], b3 = P[7 * plane + c];
+    cf1 = get_cf(d, cs, b1, b2, b3) + fabs(v1);
+    cf2 = get_cf(d, cs, b2, b1, b3) + fabs(v2);
+    cf3 = get_cf(d, cs, b3, b1, b2) + fabs(v3);
+  } else {
+    cf1 = cs + fabs(v1);
+    cf2 = cs + fabs(v2);
+    cf3 = cs + fabs(v3);
+  }
+  const double dxi1 = G.g[0].dxi[i + 2], dxi2 = G.g[1].dxi[j + 2], dxi3 = G.g[2].dxi[k + 2];
+  const double dvol = dxi1 * dxi2 * dxi3;  // metric.f90:45-48
+  const double sa1 = dxi2 * dxi3, sa2 = dxi1 * dxi3, sa3 = dxi1 * dxi2;
+  dti = dvol / (cf1 * off0 * (sa1 + sa1) + cf2 * off1 * (sa2 + sa2) + cf3 * off2 * (sa3 + sa3));
+  cfm = fmax2(fmax2(cf1, cf2), cf3);
+  return true;
+}
+
+// block-wide min(dti), max(cf) folded into the simulation's reduction slots
+__device__ __forceinline__ void cfl_block_reduce(double my_dti, double my_cf, DevScalars* sc) {
   for (int o = 16; o > 0; o >>= 1) {
     my_dti = fmin2(my_dti, __shfl_xor_sync(0xffffffffu, my_dti, o));
     my_cf = fmax2(my_cf, __shfl_xor_sync(0xffffffffu, my_cf, o));
@@ -430,16 +434,35 @@ __global__ void __launch_bounds__(256) cfl_kernel(const GridDev G, const double*
       my_cf = fmax2(my_cf, __shfl_xor_sync(0xffffffffu, my_cf, o));
     }
     if (lane == 0) {
-      atomicMin(&sc->min_dti_bits, dbits(my_dti));
-      atomicMax(&sc->cfmax_bits, dbits(my_cf));
+      atomicMin(&sc->min_dti_bits, (unsigned long long)__double_as_longlong(my_dti));
+      atomicMax(&sc->cfmax_bits, (unsigned long long)__double_as_longlong(my_cf));
     }
   }
+  __syncthreads();
 }
+
+template <bool MAG>
+__global__ void __launch_bounds__(256) cfl_kernel(const GridDev G, const double* P, size_t plane, double gamma,
+                                                  DevScalars* sc) {
+  if (sc->done) return;
+  double my_dti = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  double my_cf = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % G.n[0]);
+    const int j = (int)((c / G.n[0]) % G.n[1]);
+    const int k = (int)(c / ((size_t)G.n[0] * G.n[1]));
+    double dti, cfm;
+    if (!cfl_cell<MAG>(G, P, plane, gamma, c, i, j, k, sc, dti, cfm)) continue;
+    my_cf = fmax2(my_cf, cfm);
+    my_dti = fmin2(my_dti, dti);
+  }
+  cfl_block_reduce(my_dti, my_cf, sc);
+}
+
 
 // dt from the reduced values, with the output/end-time clamps
 // (timestep.f90:74-98).  One thread; also re-arms the reduction slots.
-__global__ void cfl_finalize_kernel(DevScalars* sc) {
-  if (threadIdx.x != 0 || blockIdx.x != 0 || sc->done) return;
+__device__ __forceinline__ void finalize_dt(DevScalars* sc) {
   const double mind = __longlong_as_double((long long)sc->min_dti_bits);
   const double cfmax = __longlong_as_double((long long)sc->cfmax_bits);
   double dt = sc->courant * mind;
@@ -464,6 +487,11 @@ __global__ void cfl_finalize_kernel(DevScalars* sc) {
   }
   sc->min_dti_bits = 0x7ff0000000000000ULL;
   sc->cfmax_bits = 0ULL;
+}
+
+__global__ void cfl_finalize_kernel(DevScalars* sc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || sc->done) return;
+  finalize_dt(sc);
 }
 
 // primitives of the current state for download: 9 planes (phi with the
@@ -579,6 +607,221 @@ cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double
 
 cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
   advance_kernel<<<1, 32, 0, st>>>(sc);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Batched step: many independent simulations of uneven sizes advance in one
+// launch per phase.  Each CTA walks a persistent loop over a work list of
+// (simulation, tile) items; every simulation keeps its own dt, ch and clock
+// in its descriptor, so a batch step equals one hormone.f90 step per grid.
+
+using T3D = Tile<8, 8, 8, 640, 1>;
+using T3D4 = Tile<8, 8, 4>;
+using T2D = Tile<16, 16, 1>;
+using T2D8 = Tile<32, 8, 1>;
+using T1D = Tile<256, 1, 1>;
+
+// tile ids: 0 3-D 8x8x8 (640 threads), 1 3-D 8x8x4 (256 threads, 2 CTAs/SM),
+// 2 2-D 16x16, 3 2-D 32x8, 4 1-D 256.  batch_tile_kind gives the grid's
+// kind (0 3-D, 1 2-D x-y, 2 1-D x); each kind has the tile ids listed in
+// batch_tile_variants.
+int batch_tile_kind(const int solve[3]) {
+  const int dim = solve[0] + solve[1] + solve[2];
+  if (dim == 3) return 0;
+  if (dim == 2 && solve[0] && solve[1]) return 1;
+  if (dim == 1 && solve[0]) return 2;
+  return -1;  // other orientations are run as single grids
+}
+
+int batch_tile_variants(int kind, int* ids) {
+  if (kind == 0) {
+    ids[0] = 0;
+    ids[1] = 1;
+    return 2;
+  }
+  if (kind == 1) {
+    ids[0] = 2;
+    ids[1] = 3;
+    return 2;
+  }
+  ids[0] = 4;
+  return 1;
+}
+
+void batch_tile_shape(int tid, int tile[3]) {
+  const int shapes[5][3] = {{8, 8, 8}, {8, 8, 4}, {16, 16, 1}, {32, 8, 1}, {256, 1, 1}};
+  for (int a = 0; a < 3; a++) tile[a] = shapes[tid][a];
+}
+
+template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel(SimDesc* sims, const int2* items, int nitems,
+                                                                        int stage, int rk) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    SimDesc& S = sims[w.x];
+    if (!S.active || S.sc.done) continue;
+    const StageArgs A = batch_stage_args(S, stage, rk);
+    stage_tile_exact<MAG, GLM, TL>(S.G, A, sm, w.y);
+    __syncthreads();
+  }
+}
+
+template <bool MAG, class TL>
+__global__ void __launch_bounds__(TL::NT) batch_cfl_kernel(SimDesc* sims, const int2* items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    SimDesc& S = sims[w.x];
+    if (!S.active || S.sc.done) continue;
+    const GridDev& G = S.G;
+    int bid = w.y, t0[3], T[3];
+    constexpr int TT[3] = {TL::TX, TL::TY, TL::TZ};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int ti = bid % S.tiles[a];
+      bid /= S.tiles[a];
+      t0[a] = ti * TT[a];
+      T[a] = min(TT[a], G.n[a] - t0[a]);
+    }
+    double my_dti = __longlong_as_double(0x7ff0000000000000LL), my_cf = 0.0;
+    const double* P = S.P[S.pcur];
+    for (int c = threadIdx.x; c < TL::NC; c += TL::NT) {
+      const int cx = c % TL::TX, cy = (c / TL::TX) % TL::TY, cz = c / (TL::TX * TL::TY);
+      if (cx >= T[0] || cy >= T[1] || cz >= T[2]) continue;
+      const int i = t0[0] + cx, j = t0[1] + cy, k = t0[2] + cz;
+      double dti, cfm;
+      if (!cfl_cell<MAG>(G, P, S.plane, S.gamma, cidx(G, i, j, k), i, j, k, &S.sc, dti, cfm)) continue;
+      my_cf = fmax2(my_cf, cfm);
+      my_dti = fmin2(my_dti, dti);
+    }
+    cfl_block_reduce(my_dti, my_cf, &S.sc);
+  }
+}
+
+__global__ void batch_finalize_kernel(SimDesc* sims, int nsims) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsims || !sims[s].active || sims[s].sc.done) return;
+  finalize_dt(&sims[s].sc);
+}
+
+// time += dt, tn += 1, end check (hormone.f90:147-155); primitive buffer
+// parity and the phidamp factor (source.f90:239-260) for the next step
+__global__ void batch_advance_kernel(SimDesc* sims, int nsims) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsims) return;
+  SimDesc& S = sims[s];
+  if (!S.active || S.sc.done) return;
+  S.sc.time = S.sc.time + S.sc.dt;
+  S.sc.tn = S.sc.tn + 1;
+  S.pcur = (S.pcur + S.rktype) & 1;
+  if (S.rktype == 1) {
+    double* t = S.U[0];
+    S.U[0] = S.U[1];
+    S.U[1] = t;
+  }
+  S.phifac = S.glm ? S.damp : 1.0;
+  if (S.sc.endstyle == 1 && S.sc.time >= S.sc.t_end) S.sc.done = 1;
+}
+
+// shared-memory opt-in of a batched stage kernel, done once (before any
+// stream capture: rebuilding a batch's work list queries occupancy first)
+template <bool MAG, bool GLM, class TL>
+static cudaError_t batch_attr_t() {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel<MAG, GLM, TL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemT<TL>));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  return cudaSuccess;
+}
+
+template <bool MAG, bool GLM, class TL>
+static cudaError_t launch_batch_stage_t(SimDesc* sims, const int2* items, int nitems, int stage, int rk, int grid,
+                                        cudaStream_t st) {
+  cudaError_t e = batch_attr_t<MAG, GLM, TL>();
+  if (e != cudaSuccess) return e;
+  batch_stage_kernel<MAG, GLM, TL><<<grid, TL::NT, sizeof(SmemT<TL>), st>>>(sims, items, nitems, stage, rk);
+  return cudaGetLastError();
+}
+
+template <class TL>
+static cudaError_t launch_batch_stage_tl(SimDesc* sims, const int2* items, int nitems, bool mag, bool glm, int stage,
+                                         int rk, int grid, cudaStream_t st) {
+  if (mag && glm) return launch_batch_stage_t<true, true, TL>(sims, items, nitems, stage, rk, grid, st);
+  if (mag) return launch_batch_stage_t<true, false, TL>(sims, items, nitems, stage, rk, grid, st);
+  return launch_batch_stage_t<false, false, TL>(sims, items, nitems, stage, rk, grid, st);
+}
+
+cudaError_t launch_batch_stage(SimDesc* sims, const int2* items, int nitems, int tid, bool mag, bool glm, int stage,
+                               int rk, int precision, int grid, cudaStream_t st) {
+  if (precision == 1) return launch_batch_stage_mixed(sims, items, nitems, tid, mag, glm, stage, rk, grid, st);
+  switch (tid) {
+    case 0: return launch_batch_stage_tl<T3D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 1: return launch_batch_stage_tl<T3D4>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 2: return launch_batch_stage_tl<T2D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 3: return launch_batch_stage_tl<T2D8>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 4: return launch_batch_stage_tl<T1D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool MAG, bool GLM, class TL>
+static int occupancy_t() {
+  int n = 0;
+  batch_attr_t<MAG, GLM, TL>();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_stage_kernel<MAG, GLM, TL>, TL::NT, sizeof(SmemT<TL>));
+  return n > 0 ? n : 1;
+}
+
+template <class TL>
+static int occupancy_tl(bool mag, bool glm) {
+  if (mag && glm) return occupancy_t<true, true, TL>();
+  if (mag) return occupancy_t<true, false, TL>();
+  return occupancy_t<false, false, TL>();
+}
+
+int batch_stage_blocks_per_sm(int tid, bool mag, bool glm, int precision) {
+  if (precision == 1) return batch_stage_mixed_blocks_per_sm(tid, mag, glm);
+  switch (tid) {
+    case 0: return occupancy_tl<T3D>(mag, glm);
+    case 1: return occupancy_tl<T3D4>(mag, glm);
+    case 2: return occupancy_tl<T2D>(mag, glm);
+    case 3: return occupancy_tl<T2D8>(mag, glm);
+  }
+  return occupancy_tl<T1D>(mag, glm);
+}
+
+template <class TL>
+static void batch_cfl_tl(SimDesc* sims, const int2* items, int nitems, bool mag, int grid, cudaStream_t st) {
+  if (mag)
+    batch_cfl_kernel<true, TL><<<grid, TL::NT, 0, st>>>(sims, items, nitems);
+  else
+    batch_cfl_kernel<false, TL><<<grid, TL::NT, 0, st>>>(sims, items, nitems);
+}
+
+cudaError_t launch_batch_cfl(SimDesc* sims, const int2* items, int nitems, int tid, bool mag, int grid,
+                             cudaStream_t st) {
+  switch (tid) {
+    case 0: batch_cfl_tl<T3D>(sims, items, nitems, mag, grid, st); break;
+    case 1: batch_cfl_tl<T3D4>(sims, items, nitems, mag, grid, st); break;
+    case 2: batch_cfl_tl<T2D>(sims, items, nitems, mag, grid, st); break;
+    case 3: batch_cfl_tl<T2D8>(sims, items, nitems, mag, grid, st); break;
+    default: batch_cfl_tl<T1D>(sims, items, nitems, mag, grid, st); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_finalize(SimDesc* sims, int nsims, cudaStream_t st) {
+  batch_finalize_kernel<<<(nsims + 127) / 128, 128, 0, st>>>(sims, nsims);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_advance(SimDesc* sims, int nsims, cudaStream_t st) {
+  batch_advance_kernel<<<(nsims + 127) / 128, 128, 0, st>>>(sims, nsims);
   return cudaGetLastError();
 }
 

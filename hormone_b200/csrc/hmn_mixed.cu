@@ -231,13 +231,12 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
   __syncthreads();
 }
 
+// One tile of one RK stage; `tile_id` enumerates the tiles of the grid
+// (x fastest).  Shared by the single-grid and the batched kernels.
 template <bool MAG, bool GLM, class TL>
-__global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel_mixed(const GridDev G, const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
+__device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageArgs& A, SmemMixed<TL>& sm, int tile_id) {
   const int tid = threadIdx.x;
-  if (A.sc->done) return;
-  int bid = blockIdx.x;
+  int bid = tile_id;
   int t0[3], T[3];
   constexpr int TT[3] = {TL::TX, TL::TY, TL::TZ};
 #pragma unroll
@@ -352,6 +351,14 @@ __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel_mixed(const Gri
 }
 
 template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel_mixed(const GridDev G, const StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
+  if (A.sc->done) return;
+  stage_tile_mixed<MAG, GLM, TL>(G, A, sm, blockIdx.x);
+}
+
+template <bool MAG, bool GLM, class TL>
 static cudaError_t launch_mixed_t(const GridDev& G, const StageArgs& A, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
@@ -383,6 +390,95 @@ cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, b
   if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_mixed_tl<Tile<1, 256, 1>>(G, A, mag, glm, st);
   if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_mixed_tl<Tile<1, 1, 256>>(G, A, mag, glm, st);
   return cudaErrorInvalidValue;
+}
+
+// batched form (see batch_stage_kernel in hmn_kernels.cu)
+template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel_mixed(SimDesc* sims, const int2* items,
+                                                                              int nitems, int stage, int rk) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    SimDesc& S = sims[w.x];
+    if (!S.active || S.sc.done) continue;
+    const StageArgs A = batch_stage_args(S, stage, rk);
+    stage_tile_mixed<MAG, GLM, TL>(S.G, A, sm, w.y);
+    __syncthreads();
+  }
+}
+
+using M3D = Tile<8, 8, 8, 640, 1>;
+using M3D4 = Tile<8, 8, 4>;
+using M2D = Tile<16, 16, 1>;
+using M2D8 = Tile<32, 8, 1>;
+using M1D = Tile<256, 1, 1>;
+
+template <bool MAG, bool GLM, class TL>
+static cudaError_t bm_attr_t() {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel_mixed<MAG, GLM, TL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemMixed<TL>));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  return cudaSuccess;
+}
+
+template <bool MAG, bool GLM, class TL>
+static cudaError_t launch_bm_t(SimDesc* sims, const int2* items, int nitems, int stage, int rk, int grid,
+                               cudaStream_t st) {
+  cudaError_t e = bm_attr_t<MAG, GLM, TL>();
+  if (e != cudaSuccess) return e;
+  batch_stage_kernel_mixed<MAG, GLM, TL><<<grid, TL::NT, sizeof(SmemMixed<TL>), st>>>(sims, items, nitems, stage, rk);
+  return cudaGetLastError();
+}
+
+template <class TL>
+static cudaError_t launch_bm_tl(SimDesc* sims, const int2* items, int nitems, bool mag, bool glm, int stage, int rk,
+                                int grid, cudaStream_t st) {
+  if (mag && glm) return launch_bm_t<true, true, TL>(sims, items, nitems, stage, rk, grid, st);
+  if (mag) return launch_bm_t<true, false, TL>(sims, items, nitems, stage, rk, grid, st);
+  return launch_bm_t<false, false, TL>(sims, items, nitems, stage, rk, grid, st);
+}
+
+cudaError_t launch_batch_stage_mixed(SimDesc* sims, const int2* items, int nitems, int tid, bool mag, bool glm,
+                                     int stage, int rk, int grid, cudaStream_t st) {
+  switch (tid) {
+    case 0: return launch_bm_tl<M3D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 1: return launch_bm_tl<M3D4>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 2: return launch_bm_tl<M2D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 3: return launch_bm_tl<M2D8>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 4: return launch_bm_tl<M1D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <bool MAG, bool GLM, class TL>
+static int occ_m() {
+  int n = 0;
+  bm_attr_t<MAG, GLM, TL>();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_stage_kernel_mixed<MAG, GLM, TL>, TL::NT,
+                                                sizeof(SmemMixed<TL>));
+  return n > 0 ? n : 1;
+}
+
+template <class TL>
+static int occ_m_tl(bool mag, bool glm) {
+  if (mag && glm) return occ_m<true, true, TL>();
+  if (mag) return occ_m<true, false, TL>();
+  return occ_m<false, false, TL>();
+}
+
+int batch_stage_mixed_blocks_per_sm(int tid, bool mag, bool glm) {
+  switch (tid) {
+    case 0: return occ_m_tl<M3D>(mag, glm);
+    case 1: return occ_m_tl<M3D4>(mag, glm);
+    case 2: return occ_m_tl<M2D>(mag, glm);
+    case 3: return occ_m_tl<M2D8>(mag, glm);
+  }
+  return occ_m_tl<M1D>(mag, glm);
 }
 
 }  // namespace hmn

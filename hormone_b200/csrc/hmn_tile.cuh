@@ -166,4 +166,68 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
 }
 
 
+// RK coefficients (faco, fact, facn) of stage `iter` of an rktype scheme
+// (rungekutta.f90:146-183)
+__host__ __device__ __forceinline__ void rk_coefficients(int iter, int type, double* faco, double* fact,
+                                                         double* facn) {
+  if (type == 3) {
+    if (iter == 1) {
+      *faco = 1.0; *fact = 1.0; *facn = 0.0;
+    } else if (iter == 2) {
+      *faco = 0.75; *fact = 0.25; *facn = *fact;
+    } else {
+      *faco = 1.0 / 3.0; *fact = 2.0 / 3.0; *facn = *fact;
+    }
+  } else if (type == 2) {
+    if (iter == 1) {
+      *faco = 1.0; *fact = 1.0; *facn = 0.0;
+    } else {
+      *faco = 0.5; *fact = 0.5; *facn = *fact;
+    }
+  } else {
+    *faco = 1.0; *fact = 1.0; *facn = 0.0;
+  }
+}
+
+// Stage arguments of one batched simulation: the same buffer roles as the
+// single-grid driver (stage 1: U[0] -> U[1]; stage 2: U[1] -> U[2] (U[0]
+// for rktype 2); stage 3: U[2] -> U[0]); primitive planes alternate.
+__device__ __forceinline__ StageArgs batch_stage_args(SimDesc& S, int stage, int rk) {
+  StageArgs a;
+  rk_coefficients(stage, rk, &a.faco, &a.fact, &a.facn);
+  const int pin = (S.pcur + stage - 1) & 1;
+  a.pin = S.P[pin];
+  a.pout = S.P[pin ^ 1];
+  a.uorg = S.U[0];
+  if (stage == 1) {
+    a.ucur = S.U[0];
+    a.uout = S.U[1];
+    a.phifac = S.phifac;
+  } else if (stage == 2) {
+    a.ucur = S.U[1];
+    a.uout = rk == 2 ? S.U[0] : S.U[2];
+    a.phifac = 1.0;
+  } else {
+    a.ucur = S.U[2];
+    a.uout = S.U[0];
+    a.phifac = 1.0;
+  }
+  a.gphi = nullptr;
+  a.sc = &S.sc;
+  a.plane = S.plane;
+  a.gamma = S.gamma;
+  a.gm1 = S.gm1;
+  a.limiter = S.limiter;
+  a.nvar = S.nvar;
+  for (int d = 0; d < 3; d++) {
+    a.tile[d] = 0;
+    a.tiles[d] = S.tiles[d];
+  }
+  return a;
+}
+
+// tile kinds of the batched kernels: 0 = 3-D 8x8x8, 1 = 2-D xy 16x16,
+// 2 = 1-D x 256
+constexpr int kBatchKinds = 3;
+
 }  // namespace hmn

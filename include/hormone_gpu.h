@@ -20,6 +20,8 @@
 #ifndef HORMONE_GPU_H
 #define HORMONE_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -125,6 +127,54 @@ int hmn_sync(hmn_ctx* ctx);
 void* hmn_stream(hmn_ctx* ctx);
 
 int hmn_destroy(hmn_ctx* ctx);
+
+/* ---- batches of independent simulations -------------------------------
+ * Not in the reference (it advances one grid per process).  A batch holds
+ * many simulations of uneven sizes in one device pool and advances all of
+ * them, each on its own clock (its own CFL dt, t_end, ch), with one
+ * persistent launch per phase; each simulation's result is bit-identical
+ * to running it alone through hmn_create/hmn_run.  Supported grids: 3-D,
+ * 2-D in the x-y plane and 1-D along x, boundary codes 0-3, no gravity,
+ * one rktype per batch. */
+typedef struct hmn_batch hmn_batch;
+
+/* Device bytes one simulation of this grid occupies in a batch pool. */
+size_t hmn_batch_footprint(const hmn_grid* grid, const hmn_params* params);
+
+int hmn_batch_create(size_t pool_bytes, int max_sims, int precision, int rktype, hmn_batch** out);
+
+/* Admit a simulation (state as for hmn_upload, packed layout, ghost = 0)
+ * that runs from `time` to `t_end`; returns HMN_ENOMEM when the pool or the
+ * slot table is full (the caller keeps it queued).  *sim = slot id. */
+int hmn_batch_add(hmn_batch* b, const hmn_grid* grid, const hmn_params* params, const double* u,
+                  const double* const prim[9], double time, double t_end, int* sim);
+
+/* Release a simulation's slot and pool memory. */
+int hmn_batch_remove(hmn_batch* b, int sim);
+
+/* Advance every admitted, unfinished simulation by up to nsteps steps
+ * (a simulation stops at its t_end).  Asynchronous. */
+int hmn_batch_step(hmn_batch* b, int nsteps);
+
+/* Clock, step count, done flag and error code of every slot (arrays of
+ * max_sims entries; any may be NULL).  Synchronises. */
+int hmn_batch_poll(hmn_batch* b, double* time, int* tn, int* done, int* err);
+
+/* Host copy of one simulation's state (u and the 9 primitive planes);
+ * returns the simulation's error code (0 if none). */
+int hmn_batch_download(hmn_batch* b, int sim, double* u, double* const prim[9]);
+
+/* Schedule of one grid kind (0: 3-D, 1: 2-D x-y, 2: 1-D x): its tile
+ * (tile_id 0 = 8x8x8 or 1 = 8x8x4 for 3-D, 2 = 16x16 or 3 = 32x8 for
+ * 2-D, 4 = 256 for 1-D) and the persistent-grid size of the stage
+ * launches in CTAs per SM (0: the occupancy limit).  The autotuner sets
+ * it; results do not depend on it. */
+int hmn_batch_set_schedule(hmn_batch* b, int kind, int tile_id, int blocks_per_sm);
+
+long long hmn_batch_launch_count(hmn_batch* b);
+int hmn_batch_sync(hmn_batch* b);
+void* hmn_batch_stream(hmn_batch* b);
+int hmn_batch_destroy(hmn_batch* b);
 
 /* The CFL timestep of hmn_timestep for callers that cannot allocate device
  * memory (no counterpart in the reference: HORMONE has no device code).

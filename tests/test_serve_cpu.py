@@ -1,0 +1,80 @@
+"""Host logic of the serving loop, against a fake batch (no GPU): arrivals,
+FIFO admission with back-fill by footprint, retirement and statistics."""
+import numpy as np
+
+from hormone_b200 import serve
+
+
+class FakeBatch:
+    """Each simulation needs `cells` units of a pool and finishes after
+    ceil(cells/100) steps."""
+
+    def __init__(self, pool):
+        self.pool, self.used, self.sims, self.next = pool, 0, {}, 0
+        self.max_sims = 64
+        self.max_live = 0
+
+    def capacity(self, cfg):
+        return int(np.prod(cfg["n"])) <= self.pool
+
+    def add(self, cfg, prims):
+        need = int(np.prod(cfg["n"]))
+        if self.used + need > self.pool:
+            return None
+        s = self.next
+        self.next += 1
+        self.sims[s] = {"need": need, "left": -(-need // 100), "tn": 0}
+        self.used += need
+        self.max_live = max(self.max_live, len(self.sims))
+        return s
+
+    def step(self, n):
+        for v in self.sims.values():
+            k = min(n, v["left"])
+            v["left"] -= k
+            v["tn"] += k
+
+    def poll(self):
+        m = self.next + 1
+        t, tn, done, err = np.zeros(m), np.zeros(m, int), np.zeros(m, int), np.zeros(m, int)
+        for s, v in self.sims.items():
+            tn[s], done[s] = v["tn"], v["left"] == 0
+        return t, tn, done, err
+
+    def download(self, s):
+        return {"tn": self.sims[s]["tn"]}
+
+    def remove(self, s):
+        self.used -= self.sims.pop(s)["need"]
+
+
+def test_request_stream_is_seeded_and_in_range():
+    a = serve.make_requests(50, rate=10.0, seed=3, max_cells=16 ** 3)
+    b = serve.make_requests(50, rate=10.0, seed=3, max_cells=16 ** 3)
+    assert [r.cells for r in a] == [r.cells for r in b]
+    assert all(np.diff([r.arrival for r in a]) >= 0)
+    for r in a:
+        assert 0.05 <= r.cfg["t_end"] <= 0.2
+        assert r.cfg["gamma"] in (1.6666666666666667, 1.4, 2.0)
+        if r.kind.startswith("riemann"):
+            d = r.prims["d"]
+            assert 0.01 <= d.min() and d.max() <= 10.0
+
+
+def test_serving_admits_as_memory_frees_and_reports_latency():
+    reqs = serve.make_requests(20, rate=1e9, seed=1, max_cells=4096, min_cells=256)
+    fake = FakeBatch(pool=6000)
+    stats = serve.serve(reqs, fake, chunk=3, realtime=False)
+    assert stats.completed == 20 and stats.failed == 0
+    assert fake.max_live >= 2
+    assert fake.used == 0 and not fake.sims
+    assert all(r.steps == -(-r.cells // 100) for r in reqs)
+    s = stats.summary()
+    assert s["p99_s"] >= s["p50_s"]
+
+
+def test_request_larger_than_the_pool_fails_instead_of_blocking():
+    reqs = serve.make_requests(3, rate=1e9, seed=2, max_cells=4096, min_cells=2048)
+    fake = FakeBatch(pool=1000)
+    stats = serve.serve(reqs, fake, chunk=1, realtime=False)
+    assert stats.failed == 3 and stats.completed == 0
