@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--poly-steps", type=int, default=2000, help="timed steps of the polytrope workload")
     return ap.parse_args()
 
 
@@ -136,18 +137,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel="stage_kernel"):
-    """dram bytes per cell of one stage launch from the committed ncu summary
-    (profiles/<kernel>*.md, a line 'dram_bytes_per_cell: X'), or None."""
+def profiled_value(key, prefix="stage_kernel_ot3d"):
+    """A figure of a committed ncu summary (profiles/<prefix>*.md, a line
+    '<key>: X'), or None."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
     for fn in sorted(os.listdir(pdir)):
-        if fn.startswith(kernel) and fn.endswith(".md"):
-            m = re.search(r"dram_bytes_per_cell:\s*([0-9.eE+-]+)", open(os.path.join(pdir, fn)).read())
+        if fn.startswith(prefix) and fn.endswith(".md"):
+            m = re.search(re.escape(key) + r":\s*([0-9.eE+-]+)", open(os.path.join(pdir, fn)).read())
             if m:
                 return float(m.group(1))
     return None
+
+
+def profiled_traffic(prefix="stage_kernel_ot3d"):
+    """DRAM bytes per cell of one stage launch (ncu dram__bytes_read.sum +
+    dram__bytes_write.sum over the cells of the launch)."""
+    return profiled_value("dram_bytes_per_cell", prefix)
 
 
 # ---------------------------------------------------------------------------
@@ -315,7 +322,10 @@ def run_ours(args, rank, world, local_rank):
     tpc = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tpc * cells) if tpc else None, "kernel": "stage_kernel",
-                "alg_bytes_per_launch": alg_bytes, "launch_ms": stage_ms, "peak_kind": peak_kind}
+                "alg_bytes_per_launch": alg_bytes, "launch_ms": stage_ms, "peak_kind": peak_kind,
+                "fp64_pipe": profiled_value("fp64_pipe_frac"),
+                "note": "FP64-issue-bound stencil: frac is of measured HBM copy bandwidth; fp64_pipe is ncu's "
+                        "FP64 pipe utilisation of the same kernel (profiles/)"}
 
     # end to end through the drop-in C ABI with pinned host buffers
     e2e = None
@@ -378,18 +388,25 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
-def run_kh_batch(args):
+def run_kh_batch(args, rank=0, world=1, local_rank=0):
     """512 periodic KH boxes, edges round(128*4^u) with u ~ U[0,1] (seeded):
     K steps of every box in one batch (persistent launches, autotuned
-    schedule, CUDA graph) against the same K steps box by box."""
+    schedule, CUDA graph) against the same K steps box by box.  With N ranks
+    the boxes are split by footprint (independent simulations, no
+    collective); the time is the max over ranks."""
     import math
 
     import numpy as np
     import torch
 
-    from hormone_b200 import autotune, config, grid as G, ic
+    from hormone_b200 import autotune, config, grid as G, ic, shard
     from hormone_b200.batch import Batch, footprint
     from hormone_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
 
     rng = np.random.Generator(np.random.PCG64(20261203))
     boxes = []
@@ -399,24 +416,30 @@ def run_kh_batch(args):
         ov = dict(ie=n, je=n, ke=1, mag_on=True, gamma=1.6666666666666667, t_end=2.0, dt_out=2.0,
                   xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5)
         cfg = config.resolve("kh_batch", overrides=ov)
-        boxes.append((cfg, ic.kelvin_helmholtz(cfg, G.make_grid(cfg), ratio, bx)))
+        boxes.append((cfg, ratio, bx))
+    total_cells = sum(int(np.prod(c["n"])) for c, _, _ in boxes)
+    mine = shard.my_share([footprint(c) for c, _, _ in boxes], rank, world)
+    boxes = [(c, ic.kelvin_helmholtz(c, G.make_grid(c), r, b)) for i, (c, r, b) in enumerate(boxes) if i in set(mine)]
     cells = sum(int(np.prod(c["n"])) for c, _ in boxes)
     K = args.steps
     sched = autotune.tune(boxes[:32], precision=args.precision, steps=2, cache=None)
-    b = Batch(sum(footprint(c) for c, _ in boxes) + (1 << 26), max_sims=args.boxes + 1, precision=args.precision)
+    b = Batch(sum(footprint(c) for c, _ in boxes) + (1 << 26), max_sims=len(boxes) + 1, precision=args.precision)
     for c, p in boxes:
         assert b.add(c, p) is not None
     autotune.apply(b, sched)
     stream = torch.cuda.ExternalStream(b.stream_ptr())
     b.step(args.warmup)
     b.sync()
+    if dist:
+        dist.barrier()
     l0 = b.launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    b.step(K)
-    e1.record(stream)
-    e1.synchronize()
-    ms_b = e0.elapsed_time(e1)
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        b.step(K)
+        e1.record(stream)
+        e1.synchronize()
+    ms_b = shard.max_over_ranks(e0.elapsed_time(e1), dist, device="cuda")
     launches_b = b.launches() - l0
     b.close()
     # one at a time: every box's K steps through its own context, box after box
@@ -430,48 +453,170 @@ def run_kh_batch(args):
         s_.ctx.run(s_.time, s_.t_end, K)
     for s_ in sims:
         s_.ctx.sync()
-    ms_1 = (time.perf_counter() - t0) * 1e3
+    ms_1 = shard.max_over_ranks((time.perf_counter() - t0) * 1e3, dist, device="cuda")
     launches_1 = sum(s_.ctx.launches() for s_ in sims) - l1
     for s_ in sims:
         s_.close()
-    line = {"metric": METRIC, "value": cells * K / (ms_b * 1e-3), "unit": METRIC, "n_gpus": 1, "steps": K,
+    if rank != 0:
+        return
+    cells = total_cells
+    line = {"metric": METRIC, "value": cells * K / (ms_b * 1e-3), "unit": METRIC, "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms_b / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "mixed", "data": "synthetic",
             "config": {"workload": f"kh-batch-{args.boxes}-boxes-128^2..512^2", "cells": cells,
-                       "schedule": {str(k): v for k, v in sched.items()}},
+                       "schedule": {str(k): v for k, v in sched.items()},
+                       "l2": "inputs larger than L2 (46 M cells x 9 x 8 B per RK buffer)",
+                       "parallelism": f"boxes sharded over {world} rank(s)"},
+            "clocks": clk.summary(),
             "one_at_a_time": {"value": cells * K / (ms_1 * 1e-3), "ms_per_step": ms_1 / K,
                               "gpu_launches": launches_1},
             "gpu_launches": launches_b, "speedup_vs_one_at_a_time": ms_1 / ms_b}
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
-    from hormone_b200 import serve
+def poly_config(n):
+    from hormone_b200 import config
+
+    ov = dict(ie=n, je=n, ke=n, mag_on=False, gamma=2.0, gravswitch=3, G=1.0, courant=0.9,
+              xi1s=-2.0, xi1e=2.0, xi2s=-2.0, xi2e=2.0, xi3s=-2.0, xi3e=2.0, t_end=1e30, dt_out=1e30)
+    for a in (1, 2, 3):
+        for tag in ("is", "os", "iv", "ov"):
+            ov[f"bc{a}{tag}"] = 3
+    return config.resolve("polytrope_cart", overrides=ov)
+
+
+def run_polytrope(args, rank, world, local_rank):
+    """Self-gravitating n=1 polytrope (G=1, K=2/pi, gamma=2) in a 192^3 box
+    [-2,2]^3 with hyperbolic gravity, FP64: zone-updates/s over the steps
+    (each step = CFL + the gravity sub-cycles + 3 fused RK stages), mass and
+    momentum drift over the run, and the L1 error against the oracle on a
+    48^3 box of the same set-up."""
+    import numpy as np
+    import torch
+
+    from hormone_b200 import grid as G, ic
+    from hormone_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    n = args.size if args.size != 256 else 192
+    cfg = poly_config(n)
+    grid = G.make_grid(cfg)
+    prims, phi = ic.polytrope_n1(cfg, grid)
+    dv = float(grid[0]["dxi"][2] * grid[1]["dxi"][2] * grid[2]["dxi"][2])
+    sim = Simulation(cfg, prims, grvphi=phi)
+    stream = torch.cuda.ExternalStream(sim.ctx.stream_ptr())
+    u0 = sim.state()["u"]
+    mass0 = float(u0[0].sum() * dv)
+    sim.run(max_steps=args.warmup)
+    torch.cuda.synchronize()
+    sim.ctx.sync()
+    steps = args.poly_steps
+    l0 = sim.ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        sim.run(max_steps=steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = sim.ctx.launches() - l0
+    u1 = sim.state()["u"]
+    t_sim = sim.time
+    sim.close()
+    mass1 = float(u1[0].sum() * dv)
+    mom = [float(u1[q].sum() * dv) for q in (1, 2, 3)]
+    vdyn = math.sqrt(4.0 / math.pi)  # sqrt(G M / R) of the star
+    cells = n ** 3
+    value = cells * steps / (ms * 1e-3)
+    # L1 against the oracle on a small box, same set-up, step for step
+    l1 = None
+    cpu = None
+    if not args.no_cpu:
+        from oracle.oracle import Oracle
+
+        m = 48
+        c2 = poly_config(m)
+        p2, f2 = ic.polytrope_n1(c2, G.make_grid(c2))
+        o = Oracle(c2)
+        o.set_prims(p2)
+        o.set_gravity_state(f2, None, 0.0)
+        o.start()
+        s2 = Simulation(c2, p2, grvphi=f2)
+        k = 20
+        t0 = time.perf_counter()
+        for _ in range(k):
+            o.step()
+        el = time.perf_counter() - t0
+        s2.run(max_steps=k)
+        a, b = s2.state()["u"], o.u()
+        s2.close()
+        l1 = {name: float(np.sum(np.abs(a[q] - b[q])) / max(np.sum(np.abs(b[q])), 1e-300))
+              for q, name in enumerate(("rho", "m1", "m2", "m3", "E"))}
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": m ** 3 * k / el, "unit": METRIC, "cores": cores, "kind": "port",
+               "sample": f"{m}^3 box of the same set-up, {k} steps ({el:.1f} s) of the CPU restatement, OpenMP"}
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"polytrope-n1-hyperbolic-gravity-{n}^3", "grid": [n, n, n], "box": [-2, 2],
+                       "G": 1.0, "K": 2 / math.pi, "gamma": 2.0, "HGfac": cfg["HGfac"], "hgcfl": cfg["hgcfl"],
+                       "l2": f"inputs larger than L2 (5 x 8 B x {n}^3 per RK buffer)"},
+            "polytrope": {"t": t_sim, "mass_drift": (mass1 - mass0) / mass0,
+                          "momentum_drift": math.sqrt(sum(x * x for x in mom)) / (mass0 * vdyn),
+                          "l1_vs_oracle_48^3_20_steps": l1},
+            "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_serve(args, rank=0, world=1, local_rank=0):
+    """The serving stream through the continuous-batching server.  With N
+    ranks every request goes to one rank (split by cells, in arrival order
+    within a rank); latencies are pooled over ranks."""
+    from hormone_b200 import serve, shard
     from hormone_b200.batch import Batch
 
     import torch
 
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
     reqs = serve.make_requests(args.requests, rate=args.rate, seed=20261203)
+    mine = set(shard.my_share([r.cells for r in reqs], rank, world))
+    reqs = [r for i, r in enumerate(reqs) if i in mine]
     free, total = torch.cuda.mem_get_info()
     b = Batch(int(free * 0.6), max_sims=1024, precision=args.precision)
-    stats = serve.serve(reqs, b, chunk=8, keep_results=False)
+    if dist:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
+        stats = serve.serve(reqs, b, chunk=8, keep_results=False)
     b.close()
+    if dist:
+        allst = [None] * world
+        dist.all_gather_object(allst, (stats.latencies, stats.zone_updates, stats.wall_s, stats.completed,
+                                       stats.failed, stats.max_live, stats.batch_steps))
+        stats.latencies = [x for a in allst for x in a[0]]
+        stats.zone_updates = sum(a[1] for a in allst)
+        stats.wall_s = max(a[2] for a in allst)
+        stats.completed = sum(a[3] for a in allst)
+        stats.failed = sum(a[4] for a in allst)
+        stats.max_live = max(a[5] for a in allst)
+        stats.batch_steps = max(a[6] for a in allst)
+    if rank != 0:
+        return
     summ = stats.summary()
-    line = {"metric": METRIC, "value": summ["zone_updates_per_s"], "unit": METRIC, "n_gpus": 1,
+    line = {"metric": METRIC, "value": summ["zone_updates_per_s"], "unit": METRIC, "n_gpus": world,
             "steps": summ["batch_steps"], "warmup": 0, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "mixed", "data": "synthetic",
             "config": {"workload": f"serve-{args.requests}-requests-poisson-{args.rate}/s",
-                       "pool_bytes": int(free * 0.6)},
-            "serve": summ}
+                       "pool_bytes": int(free * 0.6), "parallelism": f"requests sharded over {world} rank(s)"},
+            "serve": summ, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
-    if args.workload == "kh-batch":
-        return run_kh_batch(args)
-    if args.workload == "serve":
-        return run_serve(args)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -487,7 +632,14 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "kh-batch":
+            run_kh_batch(args, rank, world, local_rank)
+        elif args.workload == "serve":
+            run_serve(args, rank, world, local_rank)
+        elif args.workload == "polytrope":
+            run_polytrope(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

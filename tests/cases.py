@@ -13,9 +13,10 @@ def golden_case(name):
     return cfg, ic.make(cfg, G.make_grid(cfg))
 
 
-def ot3d(n=16, limiter="modified_mc", courant=0.9, seed=20261203):
+def ot3d(n=16, limiter="modified_mc", courant=0.9, seed=20261203, rktype=3):
     cfg = config.resolve("ot3d", overrides=dict(ie=n, je=n, ke=n, mag_on=True, gamma=1.6666666666666667,
-                                                 courant=courant, flux_limiter=limiter, t_end=0.5, dt_out=0.5))
+                                                 courant=courant, flux_limiter=limiter, t_end=0.5, dt_out=0.5,
+                                                 rktype=rktype))
     return cfg, ic.orszagtang3d(cfg, G.make_grid(cfg), seed=seed)
 
 

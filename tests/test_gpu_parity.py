@@ -102,3 +102,14 @@ def test_random_riemann_mixed_boundaries():
 def test_polytrope_hyperbolic_gravity():
     cfg, prims, phi = cases.polytrope(16)
     run_pair(cfg, prims, 5, grvphi=phi, cgrav_old=0.0)
+
+
+@pytest.mark.parametrize("rktype", [1, 2])
+def test_runge_kutta_orders(rktype):
+    """rungekutta.f90's first- and second-order schemes (buffer roles and
+    coefficients differ from SSP-RK3)."""
+    cfg, prims = cases.ot3d(12, rktype=rktype, courant=0.4)
+    run_pair(cfg, prims, 6)
+    cfg, prims = cases.golden_case("briowushock_x")
+    cfg = dict(cfg, rktype=rktype, courant=0.4)
+    run_pair(cfg, prims, 30)
