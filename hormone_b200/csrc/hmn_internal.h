@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "hmn_tma.cuh"
+
 namespace hmn {
 
 // Per-axis geometry, each array indexed [c+2] for c in [-2, n+1] (the
@@ -112,10 +114,13 @@ enum : int { kOK = 0, kEINVAL = -1, kENEG_EINT = -2, kECUDA = -3, kEBADCFG = -4,
 
 namespace hmn {
 // launchers (hmn_kernels.cu)
-void stage_tile(const int solve[3], int tile[3]);
-cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st);
+void stage_tile(const int solve[3], int precision, int tile[3]);
+// tm: tensor maps of A.pin for TMA staging (3-D tiles; nullptr stages with plain loads)
+cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
+                         cudaStream_t st);
 // mixed precision (hmn_mixed.cu): FP32 Riemann solver, FP64 reconstruction and accumulation
-cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st);
+cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
+                               cudaStream_t st);
 cudaError_t launch_cfl(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc, bool mag,
                        int nblocks, cudaStream_t st);
 cudaError_t launch_prim_init(double* P, size_t plane, bool mag, int nblocks, cudaStream_t st);

@@ -25,6 +25,8 @@
 // Slopes and fluxes never leave the SM.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include <cstdint>
 #include <cstdlib>
 
@@ -36,9 +38,10 @@ namespace hmn {
 
 template <class TL>
 struct SmemT {
-  double P[NQ][TL::NR];
+  double P[NQ][TL::NR];  // first: every TMA box destination in it is 128-byte aligned
   double S[NS][TL::NSB];
   double F[9][TL::NFB];
+  uint64_t bar;          // completion barrier of the region's bulk copies
 };
 
 // One axis of the fused stage: slopes, face fluxes, flux divergence of the
@@ -212,7 +215,8 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
 // (x fastest).  Shared by the single-grid and the batched kernels.
 template <bool MAG, bool GLM, class TL>
-__device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, int tile_id) {
+__device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, int tile_id,
+                                                 const TmaMaps* tm) {
   const int tid = threadIdx.x;
 
   int bid = tile_id;
@@ -230,25 +234,7 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
   // Every slot of the full-tile layout is one local cell (pidx and
   // region_cell are inverse); a ragged tile needs the cells within two of
   // its real extent, so its high halo occupies interior-layout slots.
-  for (int w = tid; w < TL::NR; w += TL::NT) {
-    int lc[3];
-    TL::region_cell(w, lc[0], lc[1], lc[2]);
-    int out = 0;
-    bool need = true;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      if (lc[a] < 0 || lc[a] >= T[a]) {
-        out++;
-        if (TT[a] == 1 || lc[a] < -2 || lc[a] > T[a] + 1) need = false;
-      }
-    }
-    if (!need || out > 1) continue;
-    double q[NQ];
-    stage_cell<MAG, GLM>(G, A, t0[0] + lc[0], t0[1] + lc[1], t0[2] + lc[2], q);
-#pragma unroll
-    for (int s = 0; s < NQ; s++) sm.P[s][w] = q[s];
-  }
-  __syncthreads();
+  stage_region<MAG, GLM, TL>(G, A, sm.P, &sm.bar, tm, t0, T);
 
   double acc[9];
 #pragma unroll
@@ -331,10 +317,22 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
 
 template <bool MAG, bool GLM, class TL>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G, const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
   if (A.sc->done) return;
-  stage_tile_exact<MAG, GLM, TL>(G, A, sm, blockIdx.x);
+  stage_tile_exact<MAG, GLM, TL>(G, A, sm, blockIdx.x, nullptr);
+}
+
+// the same stage with the stencil region staged by TMA (3-D tiles)
+template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB)
+    stage_kernel_tma(const GridDev G, const StageArgs A, const __grid_constant__ TmaMaps tm) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
+  if (A.sc->done) return;
+  // bulk tensor copies need 128-byte aligned destinations (uniform over the CTA)
+  const bool tma = (smem_addr(&sm.P[0][0]) & 127u) == 0;
+  stage_tile_exact<MAG, GLM, TL>(G, A, sm, blockIdx.x, tma ? &tm : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -518,34 +516,50 @@ __global__ void advance_kernel(DevScalars* sc) {
 // host-side launchers (called from hmn_capi.cu)
 
 template <bool MAG, bool GLM, class TL>
-static cudaError_t launch_stage_t(const GridDev& G, const StageArgs& A, cudaStream_t st) {
+static cudaError_t launch_stage_t(const GridDev& G, const StageArgs& A, const TmaMaps* tm, cudaStream_t st) {
+  constexpr int smem = (int)sizeof(SmemT<TL>);
+  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
+  if constexpr (TL::HX && TL::HY && TL::HZ) {  // TMA staging needs halos on all three axes
+    if (tm != nullptr) {
+      static bool attr_tma = false;
+      if (!attr_tma) {
+        cudaError_t e = cudaFuncSetAttribute(stage_kernel_tma<MAG, GLM, TL>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_tma = true;
+      }
+      stage_kernel_tma<MAG, GLM, TL><<<blocks, TL::NT, smem, st>>>(G, A, *tm);
+      return cudaGetLastError();
+    }
+  }
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MAG, GLM, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(SmemT<TL>));
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MAG, GLM, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
-  stage_kernel<MAG, GLM, TL><<<blocks, TL::NT, sizeof(SmemT<TL>), st>>>(G, A);
+  stage_kernel<MAG, GLM, TL><<<blocks, TL::NT, smem, st>>>(G, A);
   return cudaGetLastError();
 }
 
 template <class TL>
-static cudaError_t launch_stage_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
-  if (mag && glm) return launch_stage_t<true, true, TL>(G, A, st);
-  if (mag) return launch_stage_t<true, false, TL>(G, A, st);
-  return launch_stage_t<false, false, TL>(G, A, st);
+static cudaError_t launch_stage_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
+                                   cudaStream_t st) {
+  if (mag && glm) return launch_stage_t<true, true, TL>(G, A, tm, st);
+  if (mag) return launch_stage_t<true, false, TL>(G, A, tm, st);
+  return launch_stage_t<false, false, TL>(G, A, tm, st);
 }
 
-// tile shapes by solved axes: 3-D 8x8x8 (or 8x8x4 when HMN_TILE3D=884),
-// 2-D 16x16, 1-D 256
-void stage_tile(const int solve[3], int tile[3]) {
+// tile shapes by solved axes: 3-D 8x8x8 for FP64 (one CTA of 640 threads per
+// SM) and 8x8x4 for the mixed form (two CTAs per SM), either one forced by
+// HMN_TILE3D=888 or 884; 2-D 16x16, 1-D 256
+void stage_tile(const int solve[3], int precision, int tile[3]) {
   const int dim = solve[0] + solve[1] + solve[2];
   for (int a = 0; a < 3; a++) tile[a] = 1;
   if (dim == 3) {
     const char* env = getenv("HMN_TILE3D");
-    const bool t884 = env && env[0] == '8' && env[1] == '8' && env[2] == '4';
+    bool t884 = precision == 1;
+    if (env && env[0] == '8' && env[1] == '8' && (env[2] == '4' || env[2] == '8')) t884 = env[2] == '4';
     tile[0] = 8;
     tile[1] = 8;
     tile[2] = t884 ? 4 : 8;
@@ -555,16 +569,17 @@ void stage_tile(const int solve[3], int tile[3]) {
   }
 }
 
-cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
+                         cudaStream_t st) {
   const int* t = A.tile;
-  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, st);
-  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4>>(G, A, mag, glm, st);
-  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1>>(G, A, mag, glm, st);
-  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16>>(G, A, mag, glm, st);
-  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16>>(G, A, mag, glm, st);
-  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1>>(G, A, mag, glm, st);
-  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1>>(G, A, mag, glm, st);
-  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4>>(G, A, mag, glm, tm, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256>>(G, A, mag, glm, nullptr, st);
   return cudaErrorInvalidValue;
 }
 
@@ -657,14 +672,14 @@ void batch_tile_shape(int tid, int tile[3]) {
 template <bool MAG, bool GLM, class TL>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel(SimDesc* sims, const int2* items, int nitems,
                                                                         int stage, int rk) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     SimDesc& S = sims[w.x];
     if (!S.active || S.sc.done) continue;
     const StageArgs A = batch_stage_args(S, stage, rk);
-    stage_tile_exact<MAG, GLM, TL>(S.G, A, sm, w.y);
+    stage_tile_exact<MAG, GLM, TL>(S.G, A, sm, w.y, nullptr);
     __syncthreads();
   }
 }

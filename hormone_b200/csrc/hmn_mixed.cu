@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
@@ -28,9 +29,10 @@ namespace hmn {
 
 template <class TL>
 struct SmemMixed {
-  double P[NQ][TL::NR];
+  double P[NQ][TL::NR];  // first: every TMA box destination in it is 128-byte aligned
   float S[NS][TL::NSB];
   float F[9][TL::NFB];
+  uint64_t bar;          // completion barrier of the region's bulk copies
 };
 
 // s + e == a + b exactly (Knuth's TwoSum); intrinsics keep every operation
@@ -234,7 +236,8 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
 // (x fastest).  Shared by the single-grid and the batched kernels.
 template <bool MAG, bool GLM, class TL>
-__device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageArgs& A, SmemMixed<TL>& sm, int tile_id) {
+__device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageArgs& A, SmemMixed<TL>& sm, int tile_id,
+                                                 const TmaMaps* tm) {
   const int tid = threadIdx.x;
   int bid = tile_id;
   int t0[3], T[3];
@@ -246,25 +249,7 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
     t0[a] = ti * TT[a];
     T[a] = min(TT[a], G.n[a] - t0[a]);
   }
-  for (int w = tid; w < TL::NR; w += TL::NT) {
-    int lc[3];
-    TL::region_cell(w, lc[0], lc[1], lc[2]);
-    int out = 0;
-    bool need = true;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      if (lc[a] < 0 || lc[a] >= T[a]) {
-        out++;
-        if (TT[a] == 1 || lc[a] < -2 || lc[a] > T[a] + 1) need = false;
-      }
-    }
-    if (!need || out > 1) continue;
-    double q[NQ];
-    stage_cell<MAG, GLM>(G, A, t0[0] + lc[0], t0[1] + lc[1], t0[2] + lc[2], q);
-#pragma unroll
-    for (int s = 0; s < NQ; s++) sm.P[s][w] = q[s];
-  }
-  __syncthreads();
+  stage_region<MAG, GLM, TL>(G, A, sm.P, &sm.bar, tm, t0, T);
   double acc[9];
 #pragma unroll
   for (int q = 0; q < 9; q++) acc[q] = 0.0;
@@ -352,43 +337,70 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
 
 template <bool MAG, bool GLM, class TL>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel_mixed(const GridDev G, const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
   if (A.sc->done) return;
-  stage_tile_mixed<MAG, GLM, TL>(G, A, sm, blockIdx.x);
+  stage_tile_mixed<MAG, GLM, TL>(G, A, sm, blockIdx.x, nullptr);
+}
+
+// the same stage with the stencil region staged by TMA (3-D tiles)
+template <bool MAG, bool GLM, class TL>
+__global__ void __launch_bounds__(TL::NT, TL::MINB)
+    stage_kernel_mixed_tma(const GridDev G, const StageArgs A, const __grid_constant__ TmaMaps tm) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
+  if (A.sc->done) return;
+  const bool tma = (smem_addr(&sm.P[0][0]) & 127u) == 0;
+  stage_tile_mixed<MAG, GLM, TL>(G, A, sm, blockIdx.x, tma ? &tm : nullptr);
 }
 
 template <bool MAG, bool GLM, class TL>
-static cudaError_t launch_mixed_t(const GridDev& G, const StageArgs& A, cudaStream_t st) {
+static cudaError_t launch_mixed_t(const GridDev& G, const StageArgs& A, const TmaMaps* tm, cudaStream_t st) {
+  constexpr int smem = (int)sizeof(SmemMixed<TL>);
+  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
+  if constexpr (TL::HX && TL::HY && TL::HZ) {  // TMA staging needs halos on all three axes
+    if (tm != nullptr) {
+      static bool attr_tma = false;
+      if (!attr_tma) {
+        cudaError_t e = cudaFuncSetAttribute(stage_kernel_mixed_tma<MAG, GLM, TL>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_tma = true;
+      }
+      stage_kernel_mixed_tma<MAG, GLM, TL><<<blocks, TL::NT, smem, st>>>(G, A, *tm);
+      return cudaGetLastError();
+    }
+  }
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(stage_kernel_mixed<MAG, GLM, TL>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemMixed<TL>));
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
-  stage_kernel_mixed<MAG, GLM, TL><<<blocks, TL::NT, sizeof(SmemMixed<TL>), st>>>(G, A);
+  stage_kernel_mixed<MAG, GLM, TL><<<blocks, TL::NT, smem, st>>>(G, A);
   return cudaGetLastError();
 }
 
 template <class TL>
-static cudaError_t launch_mixed_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
-  if (mag && glm) return launch_mixed_t<true, true, TL>(G, A, st);
-  if (mag) return launch_mixed_t<true, false, TL>(G, A, st);
-  return launch_mixed_t<false, false, TL>(G, A, st);
+static cudaError_t launch_mixed_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
+                                   cudaStream_t st) {
+  if (mag && glm) return launch_mixed_t<true, true, TL>(G, A, tm, st);
+  if (mag) return launch_mixed_t<true, false, TL>(G, A, tm, st);
+  return launch_mixed_t<false, false, TL>(G, A, tm, st);
 }
 
-cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
+                               cudaStream_t st) {
   const int* t = A.tile;
-  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_mixed_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, st);
-  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_mixed_tl<Tile<8, 8, 4>>(G, A, mag, glm, st);
-  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_mixed_tl<Tile<16, 16, 1>>(G, A, mag, glm, st);
-  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_mixed_tl<Tile<16, 1, 16>>(G, A, mag, glm, st);
-  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_mixed_tl<Tile<1, 16, 16>>(G, A, mag, glm, st);
-  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_mixed_tl<Tile<256, 1, 1>>(G, A, mag, glm, st);
-  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_mixed_tl<Tile<1, 256, 1>>(G, A, mag, glm, st);
-  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_mixed_tl<Tile<1, 1, 256>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_mixed_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_mixed_tl<Tile<8, 8, 4>>(G, A, mag, glm, tm, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_mixed_tl<Tile<16, 16, 1>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_mixed_tl<Tile<16, 1, 16>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_mixed_tl<Tile<1, 16, 16>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_mixed_tl<Tile<256, 1, 1>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_mixed_tl<Tile<1, 256, 1>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_mixed_tl<Tile<1, 1, 256>>(G, A, mag, glm, nullptr, st);
   return cudaErrorInvalidValue;
 }
 
@@ -396,14 +408,14 @@ cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, b
 template <bool MAG, bool GLM, class TL>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel_mixed(SimDesc* sims, const int2* items,
                                                                               int nitems, int stage, int rk) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = items[it];
     SimDesc& S = sims[w.x];
     if (!S.active || S.sc.done) continue;
     const StageArgs A = batch_stage_args(S, stage, rk);
-    stage_tile_mixed<MAG, GLM, TL>(S.G, A, sm, w.y);
+    stage_tile_mixed<MAG, GLM, TL>(S.G, A, sm, w.y, nullptr);
     __syncthreads();
   }
 }

@@ -7,6 +7,7 @@
 
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
+#include "hmn_tma.cuh"
 
 namespace hmn {
 
@@ -52,11 +53,14 @@ struct Tile {
                                   HZ ? TX * TY * (TZ + 2) : 1);
   static constexpr int NFB = maxi(maxi(HX ? (TX + 1) * TY * TZ : 1, HY ? TX * (TY + 1) * TZ : 1),
                                   HZ ? TX * TY * (TZ + 1) : 1);
-  // shared-memory slot of local cell (i,j,k); at most one coordinate lies outside the tile
+  // shared-memory slot of local cell (i,j,k); at most one coordinate lies outside the tile.
+  // Part 1 holds the low y halo (TX x 2 x TZ, x fastest) and then the high one, part 2 the
+  // low and then the high z halo (TX x TY x 2): each is one box of the 4-D plane tensor.
   __device__ static __forceinline__ int pidx(int i, int j, int k) {
     if (HY && (j < 0 || j >= TY)) {
-      const int jj = j < 0 ? j + 2 : j - TY + 2;
-      return N0 + i + TX * (jj + 4 * k);
+      const int hi = j < 0 ? 0 : 1;
+      const int jl = j < 0 ? j + 2 : j - TY;
+      return N0 + hi * (N1 / 2) + i + TX * (jl + 2 * k);
     }
     if (HZ && (k < 0 || k >= TZ)) {
       const int kk = k < 0 ? k + 2 : k - TZ + 2;
@@ -72,11 +76,13 @@ struct Tile {
       j = (w / RX) % TY;
       k = w / (RX * TY);
     } else if (w < N0 + N1) {
+      constexpr int H1 = N1 > 0 ? N1 / 2 : 1;  // one y halo (only reached when there are y halos)
       const int v = w - N0;
-      i = v % TX;
-      const int jj = (v / TX) % 4;
-      k = v / (TX * 4);
-      j = jj < 2 ? jj - 2 : TY + jj - 2;
+      const int hi = v / H1, r = v % H1;
+      i = r % TX;
+      const int jl = (r / TX) % 2;
+      k = r / (TX * 2);
+      j = hi ? TY + jl : jl - 2;
     } else {
       const int v = w - N0 - N1;
       i = v % TX;
@@ -163,6 +169,80 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
   q[Q_B + 2] = b3;
   q[Q_PHI] = phig;
   q[Q_EINT] = eg;
+}
+
+// Stage the tile's cross-shaped stencil region (tile origin t0, real extent
+// T) into P[NQ][NR], ending with __syncthreads().  With tensor maps (3-D
+// tiles) the cells inside the grid arrive by TMA as raw primitive planes and
+// are converted in place exactly as stage_cell converts them (m = d*v,
+// phi*phifac); ghost cells are then written by stage_cell from the boundary
+// codes.  Without maps every slot is loaded by stage_cell.
+template <bool MAG, bool GLM, class TL>
+__device__ __forceinline__ void stage_region(const GridDev& G, const StageArgs& A, double (*P)[TL::NR],
+                                             uint64_t* bar, const TmaMaps* tm, const int t0[3], const int T[3]) {
+  constexpr int TT[3] = {TL::TX, TL::TY, TL::TZ};
+  const int tid = threadIdx.x;
+  const bool tma = tm != nullptr;
+  if (tma) {
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      mbar_arrive_expect_tx(bar, (uint32_t)(NQ * TL::NR * sizeof(double)));
+      // HBM plane p -> staged slot (d, v1..3 (made m below), e, b1..3, phi, eint)
+      constexpr int dst[NP] = {Q_D, Q_M, Q_M + 1, Q_M + 2, Q_E, Q_B, Q_B + 1, Q_B + 2, Q_PHI, Q_EINT};
+#pragma unroll
+      for (int p = 0; p < NP; p++) {
+        double* base = P[dst[p]];
+        tma_load_4d(base, &tm->box[0], bar, t0[0] - 2, t0[1], t0[2], p);
+        tma_load_4d(base + TL::N0, &tm->box[1], bar, t0[0], t0[1] - 2, t0[2], p);
+        tma_load_4d(base + TL::N0 + TL::N1 / 2, &tm->box[1], bar, t0[0], t0[1] + TL::TY, t0[2], p);
+        tma_load_4d(base + TL::N0 + TL::N1, &tm->box[2], bar, t0[0], t0[1], t0[2] - 2, p);
+        tma_load_4d(base + TL::N0 + TL::N1 + TL::N2 / 2, &tm->box[2], bar, t0[0], t0[1], t0[2] + TL::TZ, p);
+      }
+    }
+    if (!mbar_try_wait(bar, 0)) {
+      const unsigned long long t_start = global_ns();
+      while (!mbar_try_wait(bar, 0)) {
+        if (global_ns() - t_start > kTmaWaitNs) {
+          record_error(A.sc, kETIMEOUT, t0[0], t0[1], t0[2]);
+          break;
+        }
+      }
+    }
+  }
+  for (int w = tid; w < TL::NR; w += TL::NT) {
+    int lc[3];
+    TL::region_cell(w, lc[0], lc[1], lc[2]);
+    int out = 0;
+    bool need = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (lc[a] < 0 || lc[a] >= T[a]) {
+        out++;
+        if (TT[a] == 1 || lc[a] < -2 || lc[a] > T[a] + 1) need = false;
+      }
+    }
+    if (!need || out > 1) continue;
+    const int gi = t0[0] + lc[0], gj = t0[1] + lc[1], gk = t0[2] + lc[2];
+    const bool ghost = gi < 0 || gi >= G.n[0] || gj < 0 || gj >= G.n[1] || gk < 0 || gk >= G.n[2];
+    if (tma && !ghost) {
+      const double d = P[Q_D][w];
+      P[Q_M + 0][w] = d * P[Q_M + 0][w];
+      P[Q_M + 1][w] = d * P[Q_M + 1][w];
+      P[Q_M + 2][w] = d * P[Q_M + 2][w];
+      if (!MAG) P[Q_B + 0][w] = P[Q_B + 1][w] = P[Q_B + 2][w] = 0.0;
+      P[Q_PHI][w] = GLM ? P[Q_PHI][w] * A.phifac : 0.0;
+      continue;
+    }
+    double q[NQ];
+    stage_cell<MAG, GLM>(G, A, gi, gj, gk, q);
+#pragma unroll
+    for (int s = 0; s < NQ; s++) P[s][w] = q[s];
+  }
+  __syncthreads();
 }
 
 

@@ -109,3 +109,19 @@ def test_mixed_brio_wu_1024_cells():
     l1 = l1_rel(b["d"], a["d"])
     print(f"brio-wu 1024: L1(rho) mixed vs fp64 = {l1:.3e}")
     assert l1 <= 5e-4, l1
+
+
+def test_mixed_tma_and_plain_staging_agree(monkeypatch):
+    """The mixed form stages its region by TMA by default; staging with plain
+    loads gives the same bits (the arithmetic after staging is identical)."""
+    cfg, prims = cases.ot3d(24)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("HMN_TMA", flag)
+        s = Simulation(cfg, prims, precision=1)
+        for _ in range(3):
+            s.step()
+        out.append(s.state())
+        s.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k

@@ -113,3 +113,14 @@ def test_runge_kutta_orders(rktype):
     cfg, prims = cases.golden_case("briowushock_x")
     cfg = dict(cfg, rktype=rktype, courant=0.4)
     run_pair(cfg, prims, 30)
+
+
+@pytest.mark.parametrize("make", [lambda: cases.ot3d(16), lambda: cases.blast3d(14, bc=1, mag=True),
+                                  lambda: cases.riemann3d()])
+def test_tma_staged_region_fp64(monkeypatch, make):
+    """The stencil region staged by TMA bulk tensor copies (forced on for
+    FP64; even x extents, ragged tiles, every boundary code) gives the
+    oracle's bits."""
+    monkeypatch.setenv("HMN_TMA", "1")
+    cfg, prims = make()
+    run_pair(cfg, prims, 4)
