@@ -381,7 +381,7 @@ def run_ours(args, rank, world, local_rank):
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "grid": [n, n, n], "cells_per_gpu": cells, "limiter": "modified_mc",
                            "rktype": 3, "courant": 0.9, "precision": "fp64 bit-compatible (no FMA)",
-                           "l2": "inputs larger than L2 (9 x 8 B x 256^3 = 1.2 GB per RK buffer)",
+                           "l2": f"inputs larger than L2 (9 x 8 B x {n}^3 = {9 * 8 * n ** 3 / 1e9:.2f} GB per RK buffer)",
                            "parallelism": f"replicas{world}"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "mixed": mixed,
                 "clocks": clocks}
