@@ -79,13 +79,16 @@ def lib():
         L.hmn_sync.argtypes = [_P]
         L.hmn_destroy.argtypes = [_P]
         L.hmn_set_gravity_clock.argtypes = [_P, _D, _D]
+        L.hmn_gravity_clock.argtypes = [_P, _DP, _DP]
+        L.hmn_checkpoint_begin.argtypes = [_P, _DP, _DPP, _DP, _DP]
+        L.hmn_checkpoint_wait.argtypes = [_P]
         L.hmn_stream.argtypes = [_P]
         L.hmn_stream.restype = _P
         L.hmn_timestep_noalloc.argtypes = [ctypes.POINTER(HmnGrid), ctypes.POINTER(HmnParams), _P, _D, _D, _D, _P, _P]
         L.hmn_timestep_noalloc.restype = _I
         for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
-                     "hmn_set_gravity_clock"):
+                     "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait"):
             getattr(L, name).restype = _I
         _lib = L
     return _lib
@@ -216,6 +219,34 @@ class Context:
         if gravity:
             out["grvphi"], out["grvpsi"] = gphi, gpsi
         return out
+
+    def checkpoint_begin(self, u=True, gravity=False) -> Dict[str, np.ndarray]:
+        """Start an asynchronous snapshot of the current state; the returned
+        arrays are filled by checkpoint_wait (keep them alive until then)."""
+        out: Dict[str, np.ndarray] = {}
+        if u:
+            out["u"] = np.empty((self.nvar,) + self.shape)
+        P = np.empty((9,) + self.shape)
+        pp = (_DP * 9)()
+        for q, k in enumerate(("d", "v1", "v2", "v3", "e", "b1", "b2", "b3", "phi")):
+            out[k] = P[q]
+            pp[q] = _dp(P[q])
+        if gravity:
+            out["grvphi"], out["grvpsi"] = np.empty(self.shape), np.empty(self.shape)
+        self._ck = out
+        self._check(lib().hmn_checkpoint_begin(self.h, _dp(out.get("u")), pp, _dp(out.get("grvphi")),
+                                               _dp(out.get("grvpsi"))), "hmn_checkpoint_begin")
+        return out
+
+    def checkpoint_wait(self) -> Dict[str, np.ndarray]:
+        self._check(lib().hmn_checkpoint_wait(self.h), "hmn_checkpoint_wait")
+        out, self._ck = getattr(self, "_ck", None), None
+        return out
+
+    def gravity_clock(self):
+        g, c = _D(), _D()
+        self._check(lib().hmn_gravity_clock(self.h, ctypes.byref(g), ctypes.byref(c)), "hmn_gravity_clock")
+        return g.value, c.value
 
     def pressure(self) -> np.ndarray:
         p = np.empty(self.shape)

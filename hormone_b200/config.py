@@ -128,6 +128,9 @@ SIMTYPES: Dict[str, Dict[str, Any]] = {
                           dt_out=500.0, tn_out=1, dt_unit="ms", test_tol=7e-15),
     "orszagtang_xz": dict(ie=128, ke=128, mag_on=True, outstyle=1, endstyle=1, tnlim=100000, t_end=500.0,
                           dt_out=500.0, tn_out=1, dt_unit="ms", test_tol=7e-15),
+    # para/parameters_KHinstability (two passive scalars)
+    "KHinstability": dict(xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5, ie=128, je=128, outstyle=1, endstyle=1,
+                          tnlim=100000, t_end=1000.0, dt_out=100.0, tn_out=1, dt_unit="ms", compswitch=2, spn=2),
 }
 
 _UNITS = {"yr": 3600.0 * 24.0 * 365.25, "d": 3600 * 24.0, "hr": 3600.0, "ks": 1000.0, "min": 60.0, "s": 1.0,
@@ -235,6 +238,14 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     lim = str(cfg["flux_limiter"])
     if lim not in _LIMITERS:
         raise ValueError(f"Error in flux_limiter {lim}")
+    comp = int(cfg.get("compswitch", 0))
+    if comp not in (0, 1, 2):
+        raise ValueError(f"Error in compswitch {comp}")
+    # passive scalars are carried with compswitch 2 (compswitch 1 only changes
+    # the mean molecular weight, which the ideal-gas step does not use)
+    nspc = int(cfg.get("spn", 0)) if comp == 2 else 0
+    if nspc < 0 or nspc > 4:
+        raise ValueError("at most 4 passive scalars are on this path")
     grav = int(cfg.get("gravswitch", 0))
     if grav not in (0, 3):
         raise ValueError("only gravswitch 0 (off) or 3 (hyperbolic) is on this path")
@@ -249,6 +260,6 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
         alpha9wave=float(cfg["alpha9wave"]), outstyle=int(cfg["outstyle"]), endstyle=int(cfg["endstyle"]),
         tnlim=int(cfg["tnlim"]), gravswitch=grav, HGfac=float(cfg["HGfac"]), hgcfl=float(cfg["hgcfl"]),
         alphagrv=float(cfg["alphagrv"]), G=float(cfg["G"]), grktype=int(cfg["grktype"]),
-        maxtngrv=int(cfg["maxtngrv"]),
+        maxtngrv=int(cfg["maxtngrv"]), compswitch=comp, nspc=nspc,
     )
     return cfg

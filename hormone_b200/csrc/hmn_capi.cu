@@ -50,6 +50,16 @@ struct hmn_ctx {
   int graph_steps;
   TmaMaps tmaps[2];          // tensor maps of pbuf[0], pbuf[1] for TMA staging of 3-D tiles
   int tma_ok;
+  // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
+  cudaStream_t cst;
+  cudaEvent_t ck_snap, ck_done;
+  double* ck_dev;            // nvar u planes, 9 primitive planes, grvphi, grvpsi
+  double* ck_h;              // pinned host staging of the same
+  int ck_pending;
+  double* ck_u;              // destinations given to hmn_checkpoint_begin
+  double* ck_prim[9];
+  double* ck_gphi;
+  double* ck_gpsi;
 };
 
 static int cuda_fail(hmn_ctx* c, cudaError_t e, const char* what) {
@@ -383,6 +393,12 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
 extern "C" int hmn_destroy(hmn_ctx* ctx) {
   if (!ctx) return HMN_EINVAL;
   if (ctx->st) cudaStreamSynchronize(ctx->st);
+  if (ctx->ck_pending) cudaEventSynchronize(ctx->ck_done);
+  if (ctx->cst) cudaStreamDestroy(ctx->cst);
+  if (ctx->ck_snap) cudaEventDestroy(ctx->ck_snap);
+  if (ctx->ck_done) cudaEventDestroy(ctx->ck_done);
+  cudaFree(ctx->ck_dev);
+  if (ctx->ck_h) cudaFreeHost(ctx->ck_h);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
   for (int b = 0; b < 2; b++) cudaFree(ctx->pbuf[b]);
@@ -620,6 +636,13 @@ extern "C" int hmn_set_gravity_clock(hmn_ctx* ctx, double grvtime, double cgrav_
   return HMN_OK;
 }
 
+extern "C" int hmn_gravity_clock(hmn_ctx* ctx, double* grvtime, double* cgrav_old) {
+  if (!ctx) return HMN_EINVAL;
+  if (grvtime) *grvtime = ctx->grvtime;
+  if (cgrav_old) *cgrav_old = ctx->cgrav_old;
+  return HMN_OK;
+}
+
 extern "C" int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi) {
   if (!ctx) return HMN_EINVAL;
   const size_t gp = ghosted_plane(ctx);
@@ -648,6 +671,95 @@ extern "C" int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], doub
     if (rc) return rc;
   }
   return fetch_scalars(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// asynchronous checkpoint (the data of output.f90:697-795 write_bin)
+
+static int ck_planes(const hmn_ctx* ctx) { return ctx->nvar + 9 + 2; }
+
+static int ck_ensure(hmn_ctx* ctx) {
+  if (ctx->ck_dev) return HMN_OK;
+  const size_t bytes = (size_t)ck_planes(ctx) * ctx->plane * sizeof(double);
+  CK(cudaStreamCreateWithFlags(&ctx->cst, cudaStreamNonBlocking), "checkpoint stream");
+  CK(cudaEventCreateWithFlags(&ctx->ck_snap, cudaEventDisableTiming), "checkpoint event");
+  CK(cudaEventCreateWithFlags(&ctx->ck_done, cudaEventDisableTiming), "checkpoint event");
+  CK(cudaMalloc((void**)&ctx->ck_dev, bytes), "checkpoint buffer");
+  CK(cudaMallocHost((void**)&ctx->ck_h, bytes), "checkpoint staging");
+  return HMN_OK;
+}
+
+extern "C" int hmn_checkpoint_wait(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  if (!ctx->ck_pending) return HMN_OK;
+  CK(cudaEventSynchronize(ctx->ck_done), "checkpoint copy");
+  ctx->ck_pending = 0;
+  const size_t P = ctx->plane;
+  const size_t gp = ghosted_plane(ctx);
+  auto place = [&](double* dst, const double* src, int nplanes) {
+    if (!dst) return;
+    if (ctx->ghost == 0) {
+      memcpy(dst, src, (size_t)nplanes * P * sizeof(double));
+      return;
+    }
+    size_t o = 0;
+    for (int q = 0; q < nplanes; q++)
+      for (int k = 0; k < ctx->n[2]; k++)
+        for (int j = 0; j < ctx->n[1]; j++)
+          for (int i = 0; i < ctx->n[0]; i++) dst[q * gp + ghosted_index(ctx, i, j, k)] = src[o++];
+  };
+  place(ctx->ck_u, ctx->ck_h, ctx->nvar);
+  for (int q = 0; q < 9; q++) place(ctx->ck_prim[q], ctx->ck_h + (size_t)(ctx->nvar + q) * P, 1);
+  place(ctx->ck_gphi, ctx->ck_h + (size_t)(ctx->nvar + 9) * P, 1);
+  place(ctx->ck_gpsi, ctx->ck_h + (size_t)(ctx->nvar + 10) * P, 1);
+  return HMN_OK;
+}
+
+extern "C" int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi,
+                                    double* grvpsi) {
+  if (!ctx) return HMN_EINVAL;
+  int rc = hmn_checkpoint_wait(ctx);  // one checkpoint in flight at a time
+  if (rc) return rc;
+  rc = ck_ensure(ctx);
+  if (rc) return rc;
+  const size_t P = ctx->plane;
+  double* const du = ctx->ck_dev;
+  double* const dp = ctx->ck_dev + (size_t)ctx->nvar * P;
+  double* const dg = ctx->ck_dev + (size_t)(ctx->nvar + 9) * P;
+  // device snapshot on the step stream, ordered after the work enqueued so far
+  if (u) CK(cudaMemcpyAsync(du, ctx->buf[0], (size_t)ctx->nvar * P * sizeof(double), cudaMemcpyDeviceToDevice,
+                            ctx->st), "checkpoint snapshot");
+  CK(launch_prim_out(ctx->pbuf[ctx->pcur], P, ctx->phifac, ctx->par.gamma - 1.0, dp, nullptr, blocks_for(ctx),
+                     ctx->st),
+     "checkpoint snapshot");
+  ctx->launches += 1;
+  const bool grav = ctx->par.gravswitch == 3;
+  if (grav && grvphi)
+    CK(cudaMemcpyAsync(dg, ctx->gphi[ctx->gcur], P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st),
+       "checkpoint snapshot");
+  if (grav && grvpsi)
+    CK(cudaMemcpyAsync(dg + P, ctx->gpsi[ctx->gcur], P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st),
+       "checkpoint snapshot");
+  CK(cudaEventRecord(ctx->ck_snap, ctx->st), "checkpoint event");
+  // device -> host on the copy stream while later steps run on the step stream
+  CK(cudaStreamWaitEvent(ctx->cst, ctx->ck_snap, 0), "checkpoint wait");
+  if (u) CK(cudaMemcpyAsync(ctx->ck_h, du, (size_t)ctx->nvar * P * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->cst), "checkpoint copy");
+  CK(cudaMemcpyAsync(ctx->ck_h + (size_t)ctx->nvar * P, dp, 9 * P * sizeof(double), cudaMemcpyDeviceToHost,
+                     ctx->cst),
+     "checkpoint copy");
+  if (grav && (grvphi || grvpsi))
+    CK(cudaMemcpyAsync(ctx->ck_h + (size_t)(ctx->nvar + 9) * P, dg, 2 * P * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->cst),
+       "checkpoint copy");
+  CK(cudaEventRecord(ctx->ck_done, ctx->cst), "checkpoint event");
+  // the next snapshot overwrites ck_dev only after this copy (hmn_checkpoint_wait above)
+  ctx->ck_u = u;
+  for (int q = 0; q < 9; q++) ctx->ck_prim[q] = prim ? prim[q] : nullptr;
+  ctx->ck_gphi = grav ? grvphi : nullptr;
+  ctx->ck_gpsi = grav ? grvpsi : nullptr;
+  ctx->ck_pending = 1;
+  return HMN_OK;
 }
 
 extern "C" int hmn_download_pressure(hmn_ctx* ctx, double* p) {

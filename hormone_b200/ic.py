@@ -139,6 +139,41 @@ def kelvin_helmholtz(cfg, grid, rho_ratio: float, bx: float, width: float = 0.05
     return out
 
 
+def kh_instability(cfg, grid) -> Dict[str, np.ndarray]:
+    """src/init/KHtests.f90:14-58: exponential shear layer at |y| = 1/4
+    (width 0.025, densities 1 and 2, velocities +-0.5), vy = 0.01 sin(4 pi x),
+    p = 2.5, and two passive scalars marking the two fluids.  Returns the
+    primitives with 'spc' of shape (2, nz, ny, nx)."""
+    out = _blank(cfg)
+    rho1, rho2, vv1, vv2 = 1.0, 2.0, 0.5, -0.5
+    rhom, vvm = 0.5 * (rho1 - rho2), 0.5 * (vv1 - vv2)
+    ptb, width = 1e-2, 0.025
+    x, y = centres(grid, 0), centres(grid, 1)
+    v1 = np.empty(len(y))
+    d = np.empty(len(y))
+    outer = np.empty(len(y), dtype=bool)
+    for j, yy in enumerate(y):
+        if abs(yy) > 0.25:
+            ex = math.exp((-abs(yy) + 0.25) / width)
+            v1[j] = vv1 - vvm * ex
+            d[j] = rho1 - rhom * ex
+            outer[j] = True
+        else:
+            ex = math.exp((abs(yy) - 0.25) / width)
+            v1[j] = vv2 + vvm * ex
+            d[j] = rho2 + rhom * ex
+            outer[j] = False
+    out["v1"][:] = v1[None, :, None]
+    out["d"][:] = d[None, :, None]
+    out["v2"][:] = np.array([ptb * math.sin(4.0 * PI * v) for v in x])[None, None, :]
+    out["p"][:] = 2.5
+    spc = np.zeros((2,) + out["d"].shape)
+    spc[0][:] = np.where(outer, 1.0, 0.0)[None, :, None]
+    spc[1][:] = np.where(outer, 0.0, 1.0)[None, :, None]
+    out["spc"] = spc
+    return out
+
+
 def polytrope_n1(cfg, grid, rho_floor: float = 1e-6):
     """n=1 polytrope of unit radius centred on the origin (G=1, K=2/pi).
 
@@ -207,11 +242,38 @@ def to_state(cfg, prims: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
         u += [b1, b2, b3]
         if cfg["dim"] > 1:
             u.append(prims["phi"])
-    return {"prim": np.ascontiguousarray(prim), "u": np.ascontiguousarray(np.stack(u))}
+    out = {"prim": np.ascontiguousarray(prim), "u": np.ascontiguousarray(np.stack(u))}
+    if cfg.get("nspc", 0):
+        out["spc"] = np.ascontiguousarray(prims["spc"][:cfg["nspc"]])
+    return out
+
+
+def restart_state(cfg, fields: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+    """State after a restart from a dump (restart.f90 -> readbin.f90, then
+    conserve.f90:13-50): the primitives d, v1..3, e (total energy), B, phi
+    as the dump holds them, U rebuilt from them.  Returns the layout of
+    ``to_state``."""
+    d = fields["d"]
+    v1, v2, v3, e = fields["v1"], fields["v2"], fields["v3"], fields["e"]
+    z = np.zeros_like(d)
+    b1, b2, b3 = (fields.get(k, z) for k in ("b1", "b2", "b3"))
+    phi = fields.get("phi", z)
+    prim = np.stack([d, v1, v2, v3, e, b1, b2, b3, phi])
+    u = [d, d * v1, d * v2, d * v3, e]
+    if cfg["mag_on"]:
+        u += [b1, b2, b3]
+        if cfg["dim"] > 1:
+            u.append(phi)
+    out = {"prim": np.ascontiguousarray(prim), "u": np.ascontiguousarray(np.stack(u))}
+    if cfg.get("nspc", 0):
+        out["spc"] = np.ascontiguousarray(np.moveaxis(fields["spc"], -1, 0)[:cfg["nspc"]])
+    return out
 
 
 def make(cfg, grid, **kw):
     st = cfg["simtype"]
+    if st == "KHinstability":
+        return kh_instability(cfg, grid)
     if st.startswith(("sodshock", "briowushock")):
         return shocktube(cfg, grid)
     if st.startswith("orszagtang"):

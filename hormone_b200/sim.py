@@ -13,33 +13,79 @@ from typing import Dict, Optional
 
 import numpy as np
 
-from . import capi, grid as gridmod, ic
+from . import binio, capi, grid as gridmod, ic
 
 
 class Simulation:
     def __init__(self, cfg: dict, prims: Optional[Dict[str, np.ndarray]] = None, grvphi=None, grvpsi=None,
-                 cgrav_old: float = 0.0, precision: int = 0):
+                 cgrav_old: float = 0.0, precision: int = 0, _state=None, _clock=None):
         self.cfg = cfg
         self.grid = gridmod.make_grid(cfg)
-        if prims is None:
-            prims = ic.make(cfg, self.grid)
-        st = ic.to_state(cfg, prims)
+        if _state is None:
+            if prims is None:
+                prims = ic.make(cfg, self.grid)
+            _state = ic.to_state(cfg, prims)
+        st = _state
         self.ctx = capi.Context(cfg, self.grid, precision=precision)
         self.ctx.upload(u=st["u"], prim=list(st["prim"]), grvphi=grvphi, grvpsi=grvpsi)
-        self.time = 0.0
-        self.tn = 0
-        self.t_out = cfg["t_out"]
+        self.time, self.tn = (0.0, 0) if _clock is None else _clock
+        # restart.f90: t_out = time + dt_out after a restart
+        self.t_out = cfg["t_out"] if _clock is None else self.time + cfg["dt_out"]
         self.t_end = cfg["t_end"]
         self.dt = 0.0
         self.ch = 0.0
         self.mag_glm = bool(cfg["mag_on"]) and cfg["dim"] > 1
         self.gravity = cfg["gravswitch"] == 3
         if self.gravity:
-            self.ctx.set_gravity_clock(0.0, cgrav_old)
-        # hormone.f90:107-113
+            self.ctx.set_gravity_clock(self.time, cgrav_old)
+        # hormone.f90:107-113 (gravity only at tn == 0)
         self.dt, self.ch = self.ctx.timestep(self.time, self.t_out, self.t_end)
-        if self.gravity:
+        if self.gravity and self.tn == 0:
             self.ctx.gravity_step(self.time, self.dt, self.tn)
+
+    # -- checkpoints: output.f90:697-795 (write_bin) / restart.f90 -------------
+    def checkpoint_begin(self, exact: bool = False):
+        """Snapshot the current state on the device and copy it to the host
+        in the background; the steps that follow run meanwhile.  exact=True
+        also keeps the conserved planes, for a bit-exact resume."""
+        arrays = self.ctx.checkpoint_begin(u=exact, gravity=self.gravity)
+        cgrav_old = self.ctx.gravity_clock()[1] if self.gravity else 0.0
+        self._ck = (self.tn, self.time, cgrav_old)
+        return arrays
+
+    def checkpoint_finish(self, path: Optional[str] = None) -> Dict[str, object]:
+        """Wait for the snapshot; with a path, write it as a HORMONE dump
+        (and, for an exact checkpoint, the conserved planes beside it as
+        <path>.u.npy).  Returns the snapshot's fields, tn and time."""
+        fields = self.ctx.checkpoint_wait()
+        tn, time, cgrav_old = self._ck
+        if path:
+            binio.writebin(path, tn, time, fields, bool(self.cfg["mag_on"]), self.cfg["gravswitch"], cgrav_old)
+            if "u" in fields:
+                np.save(path + ".u.npy", fields["u"])
+        out = dict(fields)
+        out.update(tn=tn, time=time, cgrav_old=cgrav_old)
+        return out
+
+    def write_bin(self, path: str, exact: bool = False) -> Dict[str, object]:
+        self.checkpoint_begin(exact=exact)
+        return self.checkpoint_finish(path)
+
+    @classmethod
+    def restart(cls, cfg: dict, path: str, precision: int = 0) -> "Simulation":
+        """Resume from a dump as restart.f90 does: read it (readbin.f90),
+        rebuild U from the primitives (conserve.f90), continue the clock.  If
+        the dump has the conserved planes beside it (<path>.u.npy, written
+        by an exact checkpoint) they are used instead, and the run resumes
+        bit for bit."""
+        import os
+
+        f = binio.readbin(path, cfg["n"], bool(cfg["mag_on"]), cfg["gravswitch"])
+        st = ic.restart_state(cfg, f)
+        if os.path.exists(path + ".u.npy"):
+            st["u"] = np.ascontiguousarray(np.load(path + ".u.npy"))
+        return cls(cfg, None, grvphi=f.get("grvphi"), grvpsi=f.get("grvpsi"), cgrav_old=float(f.get("cgrav_old", 0.0)),
+                   precision=precision, _state=st, _clock=(float(f["time"]), int(f["tn"])))
 
     def step(self) -> bool:
         """One pass of hormone.f90:126-172; returns True when the run ended."""

@@ -107,6 +107,24 @@ int hmn_download_pressure(hmn_ctx* ctx, double* p);
  * (restored from a dump by readbin.f90:60-65). */
 int hmn_set_gravity_clock(hmn_ctx* ctx, double grvtime, double cgrav_old);
 
+/* Read the hyperbolic solver's clock (grvtime, cgrav_old), e.g. for the
+ * cgrav_old record of a dump (output.f90:697-795).  Either pointer may be
+ * NULL. */
+int hmn_gravity_clock(hmn_ctx* ctx, double* grvtime, double* cgrav_old);
+
+/* Asynchronous checkpoint of the current state: the data that write_bin
+ * (src/main/output.f90:697-795) dumps for output and restart (d, v1, v2,
+ * v3, e, b1, b2, b3, phi; grvphi and grvpsi with gravswitch 3), plus, when u
+ * is not NULL, the conserved planes for an exact resume.  begin snapshots
+ * the state on the device, ordered after the work enqueued so far, and
+ * copies it to host staging on a separate stream while later steps run;
+ * wait blocks until that copy is done and fills the caller's arrays (laid
+ * out as for hmn_download).  The arrays given to begin must stay valid until
+ * wait returns.  One checkpoint is in flight at a time: begin first waits
+ * for the previous one. */
+int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi);
+int hmn_checkpoint_wait(hmn_ctx* ctx);
+
 /* Advance whole steps on the device without host round trips: the loop of
  * hormone.f90:126-155 (timestep, gravity, hydro_step, phidamp, time += dt)
  * until time >= t_end or max_steps steps; the clamps use t_out = t_end.

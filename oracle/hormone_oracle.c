@@ -30,6 +30,11 @@
  *   hyperbolic grav src/main/gravity_hyperbolic.f90:19-125,230-280 with a
  *                   Cartesian Laplacian (the reference has no Cartesian form;
  *                   parity of that part is unpinned)
+ *   passive scalars src/main/interpolation.f90:126-145 (slopes),
+ *                   src/main/numflux.f90:200-212 (upwinded, renormalised
+ *                   fluxes), src/main/rungekutta.f90:61-86 (update),
+ *                   src/main/boundarycondition.f90 (scalar images),
+ *                   pinned by tests/KHinstability[_flat].bin
  *   step order      src/main/hormone.f90:124-179, src/main/hydro.f90:15-52
  *
  * Build with -ffp-contract=off: every + - * / sqrt is a single IEEE binary64
@@ -47,6 +52,7 @@
 
 enum { ICNT = 0, IMO1 = 1, IMO2 = 2, IMO3 = 3, IENE = 4, IMG1 = 5, IMG2 = 6, IMG3 = 7, I9WV = 8 };
 enum { S_D = 0, S_E, S_M1, S_M2, S_M3, S_B1, S_B2, S_B3, NSLOPE };
+#define MAXSPC 4
 
 typedef struct {
   int n[3];           /* interior cells per axis */
@@ -67,6 +73,9 @@ typedef struct {
   double *u[9], *uorg[9], *flux[3][9], *src[9];
   double *slope[3][NSLOPE], *dphi;
   double *grvphi, *grvpsi, *gorg1, *gorg2, *lapphi, *hgsrc, *gsrc, *grv[3];
+  /* passive scalars (compswitch 2): mass fractions, ghosted */
+  int spn;
+  double *spc[MAXSPC], *spcorg[MAXSPC], *dspc[3][MAXSPC], *spcflx[3][MAXSPC];
   /* scalars */
   double dt, ch, time, t_out, t_end, dt_out, cfmax;
   double cgrav, cgrav_old, dtgrav, dtg_unit, grvtime;
@@ -142,7 +151,30 @@ void hmo_destroy(Oracle *o) {
     for (int a = 0; a < 3; a++) free(o->flux[a][q]);
   }
   free(o->grvphi); free(o->grvpsi); free(o->gorg1); free(o->gorg2); free(o->lapphi); free(o->hgsrc); free(o->gsrc);
+  for (int n = 0; n < o->spn; n++) {
+    free(o->spc[n]); free(o->spcorg[n]);
+    for (int a = 0; a < 3; a++) { free(o->dspc[a][n]); free(o->spcflx[a][n]); }
+  }
   free(o);
+}
+
+/* compswitch 2 with spn passive scalars (allocations.f90) */
+int hmo_set_species(Oracle *o, int spn) {
+  if (spn < 0 || spn > MAXSPC || o->spn) return HMO_EBADCFG;
+  o->spn = spn;
+  for (int n = 0; n < spn; n++) {
+    o->spc[n] = zalloc(o->ncell); o->spcorg[n] = zalloc(o->ncell);
+    for (int a = 0; a < 3; a++) { o->dspc[a][n] = zalloc(o->ncell); o->spcflx[a][n] = zalloc(o->ncell); }
+  }
+  return HMO_OK;
+}
+
+/* interior values of scalar n (x fastest) */
+void hmo_set_spc(Oracle *o, int n, const double *val) {
+  size_t q = 0;
+  for (int k = 0; k < o->n[2]; k++)
+    for (int j = 0; j < o->n[1]; j++)
+      for (int i = 0; i < o->n[0]; i++, q++) o->spc[n][IX(o, i, j, k)] = val[q];
 }
 
 void hmo_set_times(Oracle *o, double time, double t_end, double dt_out, int outstyle, int endstyle, int tnlim) {
@@ -307,6 +339,7 @@ static void bc_axis(Oracle *o, int a) {
           }
           size_t cs_ = IXa(o, a, ss, t1, t2);
           o->d[cg] = o->d[cs_]; o->p[cg] = o->p[cs_];
+          for (int ns = 0; ns < o->spn; ns++) o->spc[ns][cg] = o->spc[ns][cs_];
           if (o->mag_on) o->phi[cg] = o->phi[cs_];
           int sv;
           switch (bv) {
@@ -415,6 +448,11 @@ static void interpolation(Oracle *o) {
             o->slope[a][sl][c0] = du;
             L[sl] = uu[1] - hl * du;
             R[sl] = uu[1] + hr * du;
+          }
+          /* interpolation.f90:135-141: scalar slopes, never zeroed below */
+          for (int ns = 0; ns < o->spn; ns++) {
+            uu[0] = o->spc[ns][cm]; uu[1] = o->spc[ns][c0]; uu[2] = o->spc[ns][cp];
+            o->dspc[a][ns][c0] = o->limiter == 1 ? minmod(uu, dx2) : modified_mc(uu, xx, xxi);
           }
           double eintl = L[S_E] - 0.5 * (L[S_M1] * L[S_M1] + L[S_M2] * L[S_M2] + L[S_M3] * L[S_M3]) / L[S_D];
           double eintr = R[S_E] - 0.5 * (R[S_M1] * R[S_M1] + R[S_M2] * R[S_M2] + R[S_M3] * R[S_M3]) / R[S_D];
@@ -586,6 +624,20 @@ static void numflux(Oracle *o) {
             F[IMG1 + c2][L] = f[7];
             if (o->dim > 1) F[I9WV][L] = f[8];
           }
+          if (o->spn) {
+            /* numflux.f90:200-212: upwinded face fractions renormalised to sum 1 */
+            double spl[MAXSPC], spr[MAXSPC], suml = 0.0, sumr = 0.0;
+            for (int ns = 0; ns < o->spn; ns++) {
+              spl[ns] = o->spc[ns][L] + dx1 * o->dspc[a][ns][L];
+              spr[ns] = o->spc[ns][R] - dx2 * o->dspc[a][ns][R];
+            }
+            for (int ns = 0; ns < o->spn; ns++) suml = suml + spl[ns]; /* Fortran sum(), left to right */
+            for (int ns = 0; ns < o->spn; ns++) sumr = sumr + spr[ns];
+            double sg = fsign(0.5, f[0]);
+            double fix = 1.0 / (suml * (0.5 + sg) + sumr * (0.5 - sg));
+            for (int ns = 0; ns < o->spn; ns++)
+              o->spcflx[a][ns][L] = fix * f[0] * (spl[ns] * (0.5 + sg) + spr[ns] * (0.5 - sg));
+          }
         }
     if (bad) set_err(o, HMO_ENEG_EINT, bi, bj, bk);
   }
@@ -691,6 +743,24 @@ static void rungekutta(Oracle *o) {
                      (idxi1[i] * (1.0 * F1[IX(o, i - 1, j, k)] - 1.0 * F1[c]) +
                       idxi2[j] * (1.0 * F2[IX(o, i, j - 1, k)] - 1.0 * F2[c]) +
                       idxi3[k] * (F3[IX(o, i, j, k - 1)] - F3[c]) + S[c]);
+        }
+  }
+  /* rungekutta.f90:61-86: scalars from the new density */
+  for (int ns = 0; ns < o->spn; ns++) {
+    double *X = o->spc[ns], *XO = o->spcorg[ns];
+    double *F1 = o->spcflx[0][ns], *F2 = o->spcflx[1][ns], *F3 = o->spcflx[2][ns];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          size_t c = IX(o, i, j, k);
+          if (o->rungen == 1) XO[c] = X[c] * o->uorg[ICNT][c];
+          X[c] = (faco * XO[c] + facn * X[c] * o->d[c] +
+                  fact * dt *
+                      (idxi1[i] * (1.0 * F1[IX(o, i - 1, j, k)] - 1.0 * F1[c]) +
+                       idxi2[j] * (1.0 * F2[IX(o, i, j - 1, k)] - 1.0 * F2[c]) +
+                       idxi3[k] * (F3[IX(o, i, j, k - 1)] - F3[c]))) /
+                 o->u[ICNT][c];
         }
   }
   primitive(o);
@@ -1038,7 +1108,7 @@ int hmo_run(Oracle *o, int max_steps) {
 /* accessors                                                                  */
 
 /* which: 0 d,1 p,2 e,3 v1,4 v2,5 v3,6 b1,7 b2,8 b3,9 phi,10 eint,11 cs,
-   12 grvphi, 13 grvpsi, 20+q u(q) */
+   12 grvphi, 13 grvpsi, 20+q u(q), 30+n spc(n) */
 int hmo_get(Oracle *o, int which, double *out) {
   const int nx = o->n[0], ny = o->n[1], nz = o->n[2];
   const double *src;
@@ -1055,6 +1125,7 @@ int hmo_get(Oracle *o, int which, double *out) {
     case 13: src = o->grvpsi; break;
     default:
       if (which >= 20 && which < 29) { src = o->u[which - 20]; break; }
+      if (which >= 30 && which < 30 + o->spn) { src = o->spc[which - 30]; break; }
       return -1;
   }
   size_t q = 0;

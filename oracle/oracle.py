@@ -52,6 +52,9 @@ def lib():
         L.hmo_get_axis.argtypes = [_P, _I] + [_DP] * 6
         L.hmo_set_prims.argtypes = [_P] + [_DP] * 9
         L.hmo_set_grvphi.argtypes = [_P, _DP, _DP]
+        L.hmo_set_species.argtypes = [_P, _I]
+        L.hmo_set_species.restype = _I
+        L.hmo_set_spc.argtypes = [_P, _I, _DP]
         L.hmo_gravity_setup.argtypes = [_P, _D]
         L.hmo_start.argtypes = [_P]
         L.hmo_start.restype = _I
@@ -107,6 +110,9 @@ class Oracle:
                         int(cfg["endstyle"]), int(cfg["tnlim"]))
         if cfg.get("is_test", False):
             L.hmo_set_test_mode(self.h)
+        self.nspc = int(cfg.get("nspc", 0))
+        if self.nspc:
+            L.hmo_set_species(self.h, self.nspc)
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -125,6 +131,11 @@ class Oracle:
         f = {k: (np.ascontiguousarray(prims[k], dtype=np.float64).reshape(-1) if prims.get(k) is not None else None)
              for k in ["d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi"]}
         self._keep = f
+        if self.nspc:
+            spc = np.ascontiguousarray(prims["spc"], dtype=np.float64)
+            self._keep_spc = spc
+            for n in range(self.nspc):
+                lib().hmo_set_spc(self.h, n, _dp(spc[n].reshape(-1)))
         lib().hmo_set_prims(self.h, *[_dp(f[k]) for k in ["d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi"]])
 
     def set_gravity_state(self, grvphi, grvpsi=None, cgrav_old=0.0):
@@ -169,7 +180,12 @@ class Oracle:
     # -- state ------------------------------------------------------------
     def get(self, name: str) -> np.ndarray:
         out = np.zeros(self.shape)
-        code = FIELDS[name] if name in FIELDS else 20 + int(name[1:])  # 'u0'..'u8'
+        if name in FIELDS:
+            code = FIELDS[name]
+        elif name.startswith("spc"):
+            code = 30 + int(name[3:])  # 'spc0', 'spc1', ...
+        else:
+            code = 20 + int(name[1:])  # 'u0'..'u8'
         if lib().hmo_get(self.h, code, _dp(out)) != 0:
             raise KeyError(name)
         return out

@@ -18,7 +18,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from hormone_b200 import binio, config  # noqa: E402
 
 CASES = [f"{k}_{d}" for k in ("sodshock", "briowushock") for d in "xyz"] + \
-        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")]
+        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability"]
 
 
 def main(ref_root):
@@ -26,8 +26,11 @@ def main(ref_root):
         cfg = config.resolve(st + " test")
         for flat in (False, True):
             name = st + ("_flat" if flat else "")
-            data = binio.readbin(os.path.join(ref_root, "tests", name + ".bin"), cfg["n"], cfg["mag_on"])
+            data = binio.readbin(os.path.join(ref_root, "tests", name + ".bin"), cfg["n"], cfg["mag_on"],
+                                 cfg["gravswitch"], cfg["compswitch"])
             arrays = {k: v for k, v in data.items() if isinstance(v, np.ndarray)}
+            if "spc" in arrays:  # (nz, ny, nx, spn) as stored -> (spn, nz, ny, nx)
+                arrays["spc"] = np.ascontiguousarray(np.moveaxis(arrays["spc"], -1, 0))
             np.savez_compressed(os.path.join(HERE, name + ".npz"), tn=data["tn"], time=data["time"], **arrays)
             print(name, data["tn"], data["time"])
 

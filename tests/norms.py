@@ -63,6 +63,8 @@ def compare(sim: dict, gold: dict, cfg: dict, dvol=None, fast_l2_if_identical=Tr
         labels += ["b1", "b2", "b3"]
         if cfg["dim"] >= 2:
             labels += ["phi"]
+    # passive scalars (tests.f90:84-87,106-110): scaled by their own magnitude
+    labels += [f"spc{n}" for n in range(cfg.get("nspc", 0))]
     g = gold
     vmag = np.sqrt(g["v1"] ** 2 + g["v2"] ** 2 + g["v3"] ** 2)
     bmag = np.sqrt(g["b1"] ** 2 + g["b2"] ** 2 + g["b3"] ** 2) if cfg["mag_on"] else np.zeros_like(vmag)
@@ -80,10 +82,13 @@ def compare(sim: dict, gold: dict, cfg: dict, dvol=None, fast_l2_if_identical=Tr
             scale = np.maximum(vmag, cs * cfg.get("Mach_tol", 1e-5))
         elif lab in ("b1", "b2", "b3"):
             scale = bmag.copy()
+        elif lab.startswith("spc"):
+            scale = np.abs(g["spc"][int(lab[3:])])
         else:
             scale = np.abs(g[lab])
         scale = np.maximum(scale, EPS)
-        var, var0 = np.asarray(sim[lab], dtype=np.float64), np.asarray(g[lab], dtype=np.float64)
+        ref = g["spc"][int(lab[3:])] if lab.startswith("spc") else g[lab]
+        var, var0 = np.asarray(sim[lab], dtype=np.float64), np.asarray(ref, dtype=np.float64)
         same = bool(np.array_equal(var, var0))
         l2 = 0.0 if (same and fast_l2_if_identical) else _l2_norm(var, var0, scale, w)
         out[lab] = dict(max=_max_norm(var, var0, scale), L1=_l1_norm(var, var0, scale, w), L2=l2,

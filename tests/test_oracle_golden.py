@@ -18,7 +18,7 @@ import norms
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = [f"{k}_{d}" for k in ("sodshock", "briowushock") for d in "xyz"] + \
-        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")]
+        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability"]
 CASES = CASES + [c + "_flat" for c in CASES]
 
 
@@ -46,6 +46,8 @@ def test_oracle_matches_golden(name):
     assert sc["tn"] == int(gold["tn"])
     assert sc["time"] == float(gold["time"])
     sim = {k: o.get(k) for k in ("d", "e", "v1", "v2", "v3", "b1", "b2", "b3", "phi")}
+    for n in range(cfg["nspc"]):
+        sim[f"spc{n}"] = o.get(f"spc{n}")
     dvol = np.full(sim["d"].shape, G.make_grid(cfg)[0]["dxi"][2] * G.make_grid(cfg)[1]["dxi"][2]
                    * G.make_grid(cfg)[2]["dxi"][2])
     res = norms.compare(sim, gold, cfg, dvol=dvol)
