@@ -82,9 +82,11 @@ def readbin(path_or_bytes, n, mag_on: bool, gravswitch: int = 0, compswitch: int
 
 
 def writebin(path: Optional[str], tn: int, time: float, fields: Dict[str, np.ndarray], mag_on: bool,
-             gravswitch: int = 0, cgrav_old: float = 0.0) -> bytes:
+             gravswitch: int = 0, cgrav_old: float = 0.0, species=None) -> bytes:
     """Write a dump in the layout above; returns the bytes (and writes them
-    to ``path`` if given)."""
+    to ``path`` if given).  With ``fields['spc']`` ((spn, nz, ny, nx) mass
+    fractions) the compswitch>=2 block is written, with ``species`` names
+    (10 characters each, default scalar1, scalar2, ...)."""
     parts = []
 
     def mark():
@@ -102,6 +104,12 @@ def writebin(path: Optional[str], tn: int, time: float, fields: Dict[str, np.nda
         mark(); arr(fields["grvphi"]); mark()
     if gravswitch == 3:
         mark(); arr(fields["grvpsi"]); parts.append(np.float64(cgrav_old).tobytes()); mark()
+    if fields.get("spc") is not None:
+        spc = np.asarray(fields["spc"], dtype="<f8")
+        spn = spc.shape[0]
+        names = species or [f"scalar{n + 1}" for n in range(spn)]
+        mark(); parts.append(np.int32(spn).tobytes()); arr(np.moveaxis(spc, 0, -1))
+        parts.append(b"".join(nm.encode("ascii")[:10].ljust(10) for nm in names)); mark()
     if mag_on:
         mark()
         for k in ("b1", "b2", "b3", "phi"):

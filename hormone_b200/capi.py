@@ -35,7 +35,8 @@ class HmnGrid(ctypes.Structure):
 class HmnParams(ctypes.Structure):
     _fields_ = [("gamma", _D), ("courant", _D), ("alpha9wave", _D), ("HGfac", _D), ("hgcfl", _D),
                 ("alphagrv", _D), ("G", _D), ("rktype", _I), ("grktype", _I), ("limiter", _I), ("mag_on", _I),
-                ("gravswitch", _I), ("maxtngrv", _I), ("outstyle", _I), ("endstyle", _I), ("precision", _I)]
+                ("gravswitch", _I), ("maxtngrv", _I), ("outstyle", _I), ("endstyle", _I), ("precision", _I),
+                ("nspc", _I)]
 
 
 class HmnError(RuntimeError):
@@ -80,7 +81,9 @@ def lib():
         L.hmn_destroy.argtypes = [_P]
         L.hmn_set_gravity_clock.argtypes = [_P, _D, _D]
         L.hmn_gravity_clock.argtypes = [_P, _DP, _DP]
-        L.hmn_checkpoint_begin.argtypes = [_P, _DP, _DPP, _DP, _DP]
+        L.hmn_checkpoint_begin.argtypes = [_P, _DP, _DPP, _DP, _DP, _DP]
+        L.hmn_upload_scalars.argtypes = [_P, _DP]
+        L.hmn_download_scalars.argtypes = [_P, _DP]
         L.hmn_checkpoint_wait.argtypes = [_P]
         L.hmn_stream.argtypes = [_P]
         L.hmn_stream.restype = _P
@@ -88,7 +91,8 @@ def lib():
         L.hmn_timestep_noalloc.restype = _I
         for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
-                     "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait"):
+                     "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait",
+                     "hmn_upload_scalars", "hmn_download_scalars"):
             getattr(L, name).restype = _I
         _lib = L
     return _lib
@@ -122,7 +126,7 @@ def params_struct(cfg: dict, precision: int = 0) -> HmnParams:
                      hgcfl=cfg["hgcfl"], alphagrv=cfg["alphagrv"], G=cfg["G"], rktype=cfg["rktype"],
                      grktype=cfg["grktype"], limiter=cfg["limiter_code"], mag_on=int(cfg["mag_on"]),
                      gravswitch=cfg["gravswitch"], maxtngrv=cfg["maxtngrv"], outstyle=cfg["outstyle"],
-                     endstyle=cfg["endstyle"], precision=precision)
+                     endstyle=cfg["endstyle"], precision=precision, nspc=int(cfg.get("nspc", 0)))
 
 
 class Context:
@@ -134,6 +138,7 @@ class Context:
         n = cfg["n"]
         self.shape = (n[2], n[1], n[0])
         self.nvar = cfg["nvar"]
+        self.nspc = int(cfg.get("nspc", 0))
         self._grid_arrays = []
         g = HmnGrid()
         for a in range(3):
@@ -148,11 +153,7 @@ class Context:
                 v = np.ascontiguousarray(grid[a][key], dtype=np.float64)
                 self._grid_arrays.append(v)
                 arr[a] = _dp(v)
-        p = HmnParams(gamma=cfg["gamma"], courant=cfg["courant"], alpha9wave=cfg["alpha9wave"], HGfac=cfg["HGfac"],
-                      hgcfl=cfg["hgcfl"], alphagrv=cfg["alphagrv"], G=cfg["G"], rktype=cfg["rktype"],
-                      grktype=cfg["grktype"], limiter=cfg["limiter_code"], mag_on=int(cfg["mag_on"]),
-                      gravswitch=cfg["gravswitch"], maxtngrv=cfg["maxtngrv"], outstyle=cfg["outstyle"],
-                      endstyle=cfg["endstyle"], precision=precision)
+        p = params_struct(cfg, precision)
         h = _P()
         rc = L.hmn_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h))
         if rc != 0:
@@ -233,15 +234,28 @@ class Context:
             pp[q] = _dp(P[q])
         if gravity:
             out["grvphi"], out["grvpsi"] = np.empty(self.shape), np.empty(self.shape)
-        self._ck = out
+        spc = np.empty(self.shape + (self.nspc,)) if self.nspc else None
+        self._ck = (out, spc)
         self._check(lib().hmn_checkpoint_begin(self.h, _dp(out.get("u")), pp, _dp(out.get("grvphi")),
-                                               _dp(out.get("grvpsi"))), "hmn_checkpoint_begin")
+                                               _dp(out.get("grvpsi")), _dp(spc)), "hmn_checkpoint_begin")
         return out
 
     def checkpoint_wait(self) -> Dict[str, np.ndarray]:
         self._check(lib().hmn_checkpoint_wait(self.h), "hmn_checkpoint_wait")
-        out, self._ck = getattr(self, "_ck", None), None
+        (out, spc), self._ck = getattr(self, "_ck", (None, None)), None
+        if out is not None and spc is not None:
+            out["spc"] = np.ascontiguousarray(np.moveaxis(spc, -1, 0))
         return out
+
+    def upload_scalars(self, spc: np.ndarray):
+        """spc: (nspc, nz, ny, nx) mass fractions."""
+        a = np.ascontiguousarray(np.moveaxis(np.asarray(spc, dtype=np.float64), 0, -1))
+        self._check(lib().hmn_upload_scalars(self.h, _dp(a)), "hmn_upload_scalars")
+
+    def download_scalars(self) -> np.ndarray:
+        a = np.empty(self.shape + (self.nspc,))
+        self._check(lib().hmn_download_scalars(self.h, _dp(a)), "hmn_download_scalars")
+        return np.ascontiguousarray(np.moveaxis(a, -1, 0))
 
     def gravity_clock(self):
         g, c = _D(), _D()

@@ -209,7 +209,7 @@ extern "C" int hmn_batch_add(hmn_batch* b, const hmn_grid* grid, const hmn_param
                              const double* const prim[9], double time, double t_end, int* sim) {
   if (!b || !grid || !par || !u || !sim) return HMN_EINVAL;
   if (grid->ghost != 0 || par->gravswitch != 0 || par->rktype != b->rktype || par->limiter < 0 ||
-      par->limiter > 2)
+      par->limiter > 2 || par->nspc != 0)
     return HMN_EBADCFG;
   int solve[3], dim = 0;
   for (int a = 0; a < 3; a++) {

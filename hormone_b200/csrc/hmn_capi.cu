@@ -50,6 +50,7 @@ struct hmn_ctx {
   int graph_steps;
   TmaMaps tmaps[2];          // tensor maps of pbuf[0], pbuf[1] for TMA staging of 3-D tiles
   int tma_ok;
+  double* spcorg;            // passive scalars times density at RK stage 1
   // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
   cudaStream_t cst;
   cudaEvent_t ck_snap, ck_done;
@@ -60,6 +61,7 @@ struct hmn_ctx {
   double* ck_prim[9];
   double* ck_gphi;
   double* ck_gpsi;
+  double* ck_spc;
 };
 
 static int cuda_fail(hmn_ctx* c, cudaError_t e, const char* what) {
@@ -125,7 +127,7 @@ static void setup_tma(hmn_ctx* ctx) {
   const char* env = getenv("HMN_TMA");
   if (env && env[0]) want = env[0] != '0';
   if (!want) return;
-  if (!(ctx->solve[0] && ctx->solve[1] && ctx->solve[2])) return;
+  if (!(ctx->solve[0] && ctx->solve[1] && ctx->solve[2]) || ctx->par.nspc > 0) return;
   bool ok = true;
   for (int b = 0; b < 2 && ok; b++)
     ok = encode_region_maps(ctx->pbuf[b], ctx->n, ctx->plane, ctx->tile, &ctx->tmaps[b]);
@@ -218,6 +220,8 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   if (par->rktype < 1 || par->rktype > 3 || par->limiter < 0 || par->limiter > 2) return HMN_EBADCFG;
   if (par->gravswitch != 0 && par->gravswitch != 3) return HMN_EBADCFG;
   if (par->precision != 0 && par->precision != 1) return HMN_EBADCFG;
+  // passive scalars: at most 4, FP64 form only
+  if (par->nspc < 0 || par->nspc > 4 || (par->nspc > 0 && par->precision != 0)) return HMN_EBADCFG;
   hmn_ctx* ctx = new (std::nothrow) hmn_ctx();
   if (!ctx) return HMN_ENOMEM;
   memset(ctx, 0, sizeof(*ctx));
@@ -298,7 +302,9 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   int nplanes = 9;  // every RK buffer can also hold the 9 primitive planes
   e = cudaMalloc((void**)&ctx->geo, geo_len * sizeof(double));
   for (int b = 0; b < 3 && e == cudaSuccess; b++) e = cudaMalloc((void**)&ctx->buf[b], nplanes * bytes);
-  for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMalloc((void**)&ctx->pbuf[b], 10 * bytes);
+  for (int b = 0; b < 2 && e == cudaSuccess; b++)
+    e = cudaMalloc((void**)&ctx->pbuf[b], (size_t)(10 + par->nspc) * bytes);
+  if (e == cudaSuccess && par->nspc > 0) e = cudaMalloc((void**)&ctx->spcorg, (size_t)par->nspc * bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->prim_out, 10 * bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->sc, sizeof(DevScalars));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->sc_h, sizeof(DevScalars));
@@ -312,7 +318,8 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->geo, geo.data(), geo_len * sizeof(double), cudaMemcpyHostToDevice, ctx->st);
   if (e == cudaSuccess) {
     for (int b = 0; b < 3 && e == cudaSuccess; b++) e = cudaMemsetAsync(ctx->buf[b], 0, nplanes * bytes, ctx->st);
-    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMemsetAsync(ctx->pbuf[b], 0, 10 * bytes, ctx->st);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++)
+      e = cudaMemsetAsync(ctx->pbuf[b], 0, (size_t)(10 + par->nspc) * bytes, ctx->st);
     for (int b = 0; b < 2 && e == cudaSuccess && par->gravswitch == 3; b++) {
       e = cudaMemsetAsync(ctx->gphi[b], 0, bytes, ctx->st);
       if (e == cudaSuccess) e = cudaMemsetAsync(ctx->gpsi[b], 0, bytes, ctx->st);
@@ -383,7 +390,7 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     G.g[a].risum = base + 14 * L;
   }
   memcpy(G.bc, ctx->bc, sizeof(G.bc));
-  stage_tile(ctx->solve, par->precision, ctx->tile);
+  stage_tile(ctx->solve, par->precision, par->nspc, ctx->tile);
   for (int a = 0; a < 3; a++) ctx->tiles[a] = (ctx->n[a] + ctx->tile[a] - 1) / ctx->tile[a];
   setup_tma(ctx);
   *out = ctx;
@@ -402,6 +409,7 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
   for (int b = 0; b < 2; b++) cudaFree(ctx->pbuf[b]);
+  cudaFree(ctx->spcorg);
   for (int b = 0; b < 2; b++) {
     cudaFree(ctx->gphi[b]);
     cudaFree(ctx->gpsi[b]);
@@ -550,6 +558,9 @@ static int enqueue_hydro(hmn_ctx* ctx) {
       a.tile[d] = ctx->tile[d];
       a.tiles[d] = ctx->tiles[d];
     }
+    a.stage = s;
+    a.nspc = ctx->par.nspc;
+    a.spcorg = ctx->spcorg;
     const TmaMaps* tm = ctx->tma_ok ? &ctx->tmaps[ctx->pcur] : nullptr;
     if (ctx->par.precision == 1)
       CK(launch_stage_mixed(ctx->G, a, ctx->mag, ctx->glm, tm, ctx->st), "stage");
@@ -676,7 +687,7 @@ extern "C" int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], doub
 // ---------------------------------------------------------------------------
 // asynchronous checkpoint (the data of output.f90:697-795 write_bin)
 
-static int ck_planes(const hmn_ctx* ctx) { return ctx->nvar + 9 + 2; }
+static int ck_planes(const hmn_ctx* ctx) { return ctx->nvar + 9 + 2 + ctx->par.nspc; }
 
 static int ck_ensure(hmn_ctx* ctx) {
   if (ctx->ck_dev) return HMN_OK;
@@ -712,11 +723,22 @@ extern "C" int hmn_checkpoint_wait(hmn_ctx* ctx) {
   for (int q = 0; q < 9; q++) place(ctx->ck_prim[q], ctx->ck_h + (size_t)(ctx->nvar + q) * P, 1);
   place(ctx->ck_gphi, ctx->ck_h + (size_t)(ctx->nvar + 9) * P, 1);
   place(ctx->ck_gpsi, ctx->ck_h + (size_t)(ctx->nvar + 10) * P, 1);
+  if (ctx->ck_spc) {  // species fastest, as hmn_download_scalars
+    const int ns = ctx->par.nspc;
+    const double* src = ctx->ck_h + (size_t)(ctx->nvar + 11) * P;
+    size_t o = 0;
+    for (int k = 0; k < ctx->n[2]; k++)
+      for (int j = 0; j < ctx->n[1]; j++)
+        for (int i = 0; i < ctx->n[0]; i++, o++) {
+          const size_t g = ghosted_index(ctx, i, j, k);
+          for (int n = 0; n < ns; n++) ctx->ck_spc[(size_t)ns * g + n] = src[(size_t)n * P + o];
+        }
+  }
   return HMN_OK;
 }
 
 extern "C" int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi,
-                                    double* grvpsi) {
+                                    double* grvpsi, double* spc) {
   if (!ctx) return HMN_EINVAL;
   int rc = hmn_checkpoint_wait(ctx);  // one checkpoint in flight at a time
   if (rc) return rc;
@@ -740,6 +762,12 @@ extern "C" int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[
   if (grav && grvpsi)
     CK(cudaMemcpyAsync(dg + P, ctx->gpsi[ctx->gcur], P * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st),
        "checkpoint snapshot");
+  const int ns = ctx->par.nspc;
+  double* const dsp = ctx->ck_dev + (size_t)(ctx->nvar + 11) * P;
+  if (spc && ns > 0)
+    CK(cudaMemcpyAsync(dsp, ctx->pbuf[ctx->pcur] + 10 * P, (size_t)ns * P * sizeof(double),
+                       cudaMemcpyDeviceToDevice, ctx->st),
+       "checkpoint snapshot");
   CK(cudaEventRecord(ctx->ck_snap, ctx->st), "checkpoint event");
   // device -> host on the copy stream while later steps run on the step stream
   CK(cudaStreamWaitEvent(ctx->cst, ctx->ck_snap, 0), "checkpoint wait");
@@ -752,13 +780,63 @@ extern "C" int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[
     CK(cudaMemcpyAsync(ctx->ck_h + (size_t)(ctx->nvar + 9) * P, dg, 2 * P * sizeof(double),
                        cudaMemcpyDeviceToHost, ctx->cst),
        "checkpoint copy");
+  if (spc && ns > 0)
+    CK(cudaMemcpyAsync(ctx->ck_h + (size_t)(ctx->nvar + 11) * P, dsp, (size_t)ns * P * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->cst),
+       "checkpoint copy");
   CK(cudaEventRecord(ctx->ck_done, ctx->cst), "checkpoint event");
   // the next snapshot overwrites ck_dev only after this copy (hmn_checkpoint_wait above)
   ctx->ck_u = u;
   for (int q = 0; q < 9; q++) ctx->ck_prim[q] = prim ? prim[q] : nullptr;
   ctx->ck_gphi = grav ? grvphi : nullptr;
   ctx->ck_gpsi = grav ? grvpsi : nullptr;
+  ctx->ck_spc = ns > 0 ? spc : nullptr;
   ctx->ck_pending = 1;
+  return HMN_OK;
+}
+
+// passive scalars: caller layout spc(1:nspc, i, j, k) (species fastest) with
+// the context's ghost layers <-> device planes NP.. of the primitive buffer
+extern "C" int hmn_upload_scalars(hmn_ctx* ctx, const double* spc) {
+  if (!ctx || !spc) return HMN_EINVAL;
+  const int ns = ctx->par.nspc;
+  if (ns == 0) return HMN_OK;
+  const size_t P = ctx->plane;
+  int rc = ensure_stage(ctx, (size_t)ns * P * sizeof(double));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  size_t o = 0;
+  for (int k = 0; k < ctx->n[2]; k++)
+    for (int j = 0; j < ctx->n[1]; j++)
+      for (int i = 0; i < ctx->n[0]; i++, o++) {
+        const size_t g = ghosted_index(ctx, i, j, k);
+        for (int n = 0; n < ns; n++) ctx->stage_h[(size_t)n * P + o] = spc[(size_t)ns * g + n];
+      }
+  CK(cudaMemcpyAsync(ctx->pbuf[ctx->pcur] + 10 * P, ctx->stage_h, (size_t)ns * P * sizeof(double),
+                     cudaMemcpyHostToDevice, ctx->st),
+     "upload");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  return HMN_OK;
+}
+
+extern "C" int hmn_download_scalars(hmn_ctx* ctx, double* spc) {
+  if (!ctx || !spc) return HMN_EINVAL;
+  const int ns = ctx->par.nspc;
+  if (ns == 0) return HMN_OK;
+  const size_t P = ctx->plane;
+  int rc = ensure_stage(ctx, (size_t)ns * P * sizeof(double));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->stage_h, ctx->pbuf[ctx->pcur] + 10 * P, (size_t)ns * P * sizeof(double),
+                     cudaMemcpyDeviceToHost, ctx->st),
+     "download");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  size_t o = 0;
+  for (int k = 0; k < ctx->n[2]; k++)
+    for (int j = 0; j < ctx->n[1]; j++)
+      for (int i = 0; i < ctx->n[0]; i++, o++) {
+        const size_t g = ghosted_index(ctx, i, j, k);
+        for (int n = 0; n < ns; n++) spc[(size_t)ns * g + n] = ctx->stage_h[(size_t)n * P + o];
+      }
   return HMN_OK;
 }
 

@@ -72,6 +72,9 @@ struct StageArgs {
   int nvar;
   int tile[3];          // tile extent
   int tiles[3];         // tiles per axis
+  int nspc;             // passive scalars (primitive planes NP.. of pin/pout)
+  int stage;            // RK stage, 1-based
+  double* spcorg;       // spc * density at stage 1 (rungekutta.f90:67), nspc planes
 };
 
 // Arguments of one hyperbolic-gravity RK stage (hmn_kernels.cu: hg_stage_kernel).
@@ -114,7 +117,7 @@ enum : int { kOK = 0, kEINVAL = -1, kENEG_EINT = -2, kECUDA = -3, kEBADCFG = -4,
 
 namespace hmn {
 // launchers (hmn_kernels.cu)
-void stage_tile(const int solve[3], int precision, int tile[3]);
+void stage_tile(const int solve[3], int precision, int nspc, int tile[3]);
 // tm: tensor maps of A.pin for TMA staging (3-D tiles; nullptr stages with plain loads)
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st);

@@ -38,17 +38,17 @@ namespace hmn {
 
 template <class TL>
 struct SmemT {
-  double P[NQ][TL::NR];  // first: every TMA box destination in it is 128-byte aligned
-  double S[NS][TL::NSB];
-  double F[9][TL::NFB];
-  uint64_t bar;          // completion barrier of the region's bulk copies
+  double P[NQ + TL::SP][TL::NR];  // first: every TMA box destination in it is 128-byte aligned
+  double S[NS + TL::SP][TL::NSB];
+  double F[9 + TL::SP][TL::NFB];
+  uint64_t bar;                   // completion barrier of the region's bulk copies
 };
 
 // One axis of the fused stage: slopes, face fluxes, flux divergence of the
 // thread's own cell added to acc[].
 template <int AX, bool MAG, bool GLM, class TL>
 __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, const int t0[3],
-                                          const int T[3], double acc[9], double ch) {
+                                          const int T[3], double acc[9], double accs[], double ch) {
   constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ;
   constexpr int SBX = TX + (AX == 0 ? 2 : 0), SBY = TY + (AX == 1 ? 2 : 0), SBZ = TZ + (AX == 2 ? 2 : 0);
   constexpr int FBX = TX + (AX == 0 ? 1 : 0), FBY = TY + (AX == 1 ? 1 : 0), FBZ = TZ + (AX == 2 ? 1 : 0);
@@ -78,6 +78,8 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
     if (A.limiter == 0) {
 #pragma unroll
       for (int q = 0; q < NS; q++) sl[q] = 0.0;
+      if constexpr (TL::SP > 0)
+        for (int n = 0; n < A.nspc; n++) sm.S[NS + n][w] = 0.0;
     } else {
       constexpr int qmap[NS] = {Q_D, Q_E, Q_M + 0, Q_M + 1, Q_M + 2, Q_B + 0, Q_B + 1, Q_B + 2};
       const double hl = g.hl[cg + 2], hr = g.hr[cg + 2];
@@ -105,6 +107,18 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
       }
 #pragma unroll
       for (int q = nsl; q < NS; q++) sl[q] = 0.0;
+      // passive-scalar slopes (interpolation.f90:135-141), not zeroed below
+      if constexpr (TL::SP > 0) {
+        for (int n = 0; n < A.nspc; n++) {
+          const double u0 = sm.P[NQ + n][rm], u1 = sm.P[NQ + n][r], u2 = sm.P[NQ + n][rp];
+          double du;
+          if (A.limiter == 1)
+            du = lim_minmod(u0, u1, u2, g.idx[cg + 2], g.idx[cg + 3], g.isum[cg + 2]);
+          else
+            du = lim_mmc(u0, u1, u2, g.mcf[cg + 2], g.mcb[cg + 2], g.ga[cg + 2], g.gb[cg + 2]);
+          sm.S[NS + n][w] = du;
+        }
+      }
       // admissibility of the face internal energies (interpolation.f90:147-163)
       double eintl = L[S_E] - 0.5 * (L[S_M] * L[S_M] + L[S_M + 1] * L[S_M + 1] + L[S_M + 2] * L[S_M + 2]) / L[S_D];
       double eintr = R[S_E] - 0.5 * (R[S_M] * R[S_M] + R[S_M + 1] * R[S_M + 1] + R[S_M + 2] * R[S_M + 2]) / R[S_D];
@@ -193,6 +207,28 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
       sm.F[IMG1 + c2][w] = fl[7];
       if (GLM) sm.F[I9WV][w] = fl[8];
     }
+    // passive scalars: face fractions upwinded by the mass flux and
+    // renormalised to sum 1 (numflux.f90:200-212)
+    if constexpr (TL::SP > 0) {
+      if (A.nspc > 0) {
+        double spl[TL::SP], spr[TL::SP];
+        double suml = 0.0, sumr = 0.0;
+#pragma unroll
+        for (int n = 0; n < TL::SP; n++) {
+          if (n < A.nspc) {
+            spl[n] = sm.P[NQ + n][rL] + dx1 * sm.S[NS + n][sL];
+            spr[n] = sm.P[NQ + n][rR] - dx2 * sm.S[NS + n][sR];
+            suml = suml + spl[n];
+            sumr = sumr + spr[n];
+          }
+        }
+        const double sg = fsign(0.5, fl[0]);
+        const double fix = 1.0 / (suml * (0.5 + sg) + sumr * (0.5 - sg));
+#pragma unroll
+        for (int n = 0; n < TL::SP; n++)
+          if (n < A.nspc) sm.F[9 + n][w] = fix * fl[0] * (spl[n] * (0.5 + sg) + spr[n] * (0.5 - sg));
+      }
+    }
   }
   __syncthreads();
 
@@ -207,6 +243,11 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
       constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
 #pragma unroll
       for (int q = 0; q < nv; q++) acc[q] = acc[q] + idxi * (sm.F[q][wm] - sm.F[q][wp]);
+      if constexpr (TL::SP > 0) {
+#pragma unroll
+        for (int n = 0; n < TL::SP; n++)
+          if (n < A.nspc) accs[n] = accs[n] + idxi * (sm.F[9 + n][wm] - sm.F[9 + n][wp]);
+      }
     }
   }
   __syncthreads();  // S and F are reused by the next axis
@@ -239,10 +280,13 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
   double acc[9];
 #pragma unroll
   for (int q = 0; q < 9; q++) acc[q] = 0.0;
+  double accs[TL::SP > 0 ? TL::SP : 1];
+#pragma unroll
+  for (int n = 0; n < (TL::SP > 0 ? TL::SP : 1); n++) accs[n] = 0.0;
   const double ch = A.sc->ch;
-  if (TL::TX > 1 && G.solve[0]) axis_pass<0, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
-  if (TL::TY > 1 && G.solve[1]) axis_pass<1, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
-  if (TL::TZ > 1 && G.solve[2]) axis_pass<2, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
+  if (TL::TX > 1 && G.solve[0]) axis_pass<0, MAG, GLM, TL>(G, A, sm, t0, T, acc, accs, ch);
+  if (TL::TY > 1 && G.solve[1]) axis_pass<1, MAG, GLM, TL>(G, A, sm, t0, T, acc, accs, ch);
+  if (TL::TZ > 1 && G.solve[2]) axis_pass<2, MAG, GLM, TL>(G, A, sm, t0, T, acc, accs, ch);
 
   // ---- RK combination (rungekutta.f90:35-59) + source (source.f90:70-85) -------
   if (tid >= TL::NC) return;
@@ -313,6 +357,22 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
   Po[PPHI * pl + c] = GLM ? un[8] : 0.0;
   Po[PEINT * pl + c] = eint;
   if (eint <= 0.0) record_error(A.sc, kENEG_EINT, i, j, k);
+  // passive scalars from the new density (rungekutta.f90:61-86)
+  if constexpr (TL::SP > 0) {
+#pragma unroll
+    for (int n = 0; n < TL::SP; n++) {
+      if (n >= A.nspc) break;
+      const double x = A.pin[(size_t)(NP + n) * pl + c];
+      double xo;
+      if (A.stage == 1) {
+        xo = x * A.uorg[c];
+        A.spcorg[(size_t)n * pl + c] = xo;
+      } else {
+        xo = A.spcorg[(size_t)n * pl + c];
+      }
+      Po[(size_t)(NP + n) * pl + c] = (A.faco * xo + A.facn * x * A.pin[c] + dtf * accs[n]) / d;
+    }
+  }
 }
 
 template <bool MAG, bool GLM, class TL>
@@ -552,11 +612,16 @@ static cudaError_t launch_stage_tl(const GridDev& G, const StageArgs& A, bool ma
 
 // tile shapes by solved axes: 3-D 8x8x8 for FP64 (one CTA of 640 threads per
 // SM) and 8x8x4 for the mixed form (two CTAs per SM), either one forced by
-// HMN_TILE3D=888 or 884; 2-D 16x16, 1-D 256
-void stage_tile(const int solve[3], int precision, int tile[3]) {
+// HMN_TILE3D=888 or 884, and 8x8x4 whenever there are passive scalars;
+// 2-D 16x16, 1-D 256
+void stage_tile(const int solve[3], int precision, int nspc, int tile[3]) {
   const int dim = solve[0] + solve[1] + solve[2];
   for (int a = 0; a < 3; a++) tile[a] = 1;
-  if (dim == 3) {
+  if (dim == 3 && nspc > 0) {  // the scalar planes only fit the smaller tile
+    tile[0] = 8;
+    tile[1] = 8;
+    tile[2] = 4;
+  } else if (dim == 3) {
     const char* env = getenv("HMN_TILE3D");
     bool t884 = precision == 1;
     if (env && env[0] == '8' && env[1] == '8' && (env[2] == '4' || env[2] == '8')) t884 = env[2] == '4';
@@ -572,6 +637,23 @@ void stage_tile(const int solve[3], int precision, int tile[3]) {
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st) {
   const int* t = A.tile;
+  if (A.nspc > 0) {  // tiles with room for up to 4 passive scalars
+    using S3 = Tile<8, 8, 4, 256, 2, 4>;
+    if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<S3>(G, A, mag, glm, nullptr, st);
+    if (t[0] == 16 && t[1] == 16 && t[2] == 1)
+      return launch_stage_tl<Tile<16, 16, 1, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+    if (t[0] == 16 && t[1] == 1 && t[2] == 16)
+      return launch_stage_tl<Tile<16, 1, 16, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+    if (t[0] == 1 && t[1] == 16 && t[2] == 16)
+      return launch_stage_tl<Tile<1, 16, 16, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+    if (t[0] == 256 && t[1] == 1 && t[2] == 1)
+      return launch_stage_tl<Tile<256, 1, 1, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+    if (t[0] == 1 && t[1] == 256 && t[2] == 1)
+      return launch_stage_tl<Tile<1, 256, 1, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+    if (t[0] == 1 && t[1] == 1 && t[2] == 256)
+      return launch_stage_tl<Tile<1, 1, 256, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+    return cudaErrorInvalidValue;
+  }
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
   if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4>>(G, A, mag, glm, tm, st);
   if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1>>(G, A, mag, glm, nullptr, st);

@@ -35,9 +35,10 @@ __device__ __forceinline__ size_t cidx(const GridDev& G, int i, int j, int k) {
 
 // Compile-time description of a tile: TX x TY x TZ cells (256 in all) and a
 // halo of two cells beyond each face of every axis with extent > 1.
-template <int TX_, int TY_, int TZ_, int NT_ = 256, int MINB_ = 2>
+template <int TX_, int TY_, int TZ_, int NT_ = 256, int MINB_ = 2, int SP_ = 0>
 struct Tile {
   static constexpr int TX = TX_, TY = TY_, TZ = TZ_;
+  static constexpr int SP = SP_;      // passive scalars the shared-memory layout has room for
   static constexpr int NT = NT_;      // threads per CTA (at least the tile's cell count)
   static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget is sized for
   static constexpr int NC = TX * TY * TZ;
@@ -171,6 +172,26 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
   q[Q_EINT] = eg;
 }
 
+// Interior cell whose scalar values the cell (i,j,k) holds: itself, or for a
+// ghost (one coordinate outside the grid) its image under the scalar
+// boundary code (boundarycondition.f90: periodic, reflective, outgoing/free).
+__device__ __forceinline__ size_t scalar_image(const GridDev& G, int i, int j, int k) {
+  int c3[3] = {i, j, k};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int n = G.n[a], s = c3[a];
+    if (s >= 0 && s < n) continue;
+    const int io = s < 0 ? 0 : 1;
+    const int gl = io == 0 ? s + 2 : s - n;
+    const int per = io == 0 ? n - 2 + gl : gl;
+    const int refl = io == 0 ? 1 - gl : n - 1 - gl;
+    const int edge = io == 0 ? 0 : n - 1;
+    const int bs = G.bc[a][io][0];
+    c3[a] = bs == 0 ? per : (bs == 1 ? refl : edge);
+  }
+  return cidx(G, c3[0], c3[1], c3[2]);
+}
+
 // Stage the tile's cross-shaped stencil region (tile origin t0, real extent
 // T) into P[NQ][NR], ending with __syncthreads().  With tensor maps (3-D
 // tiles) the cells inside the grid arrive by TMA as raw primitive planes and
@@ -182,7 +203,7 @@ __device__ __forceinline__ void stage_region(const GridDev& G, const StageArgs& 
                                              uint64_t* bar, const TmaMaps* tm, const int t0[3], const int T[3]) {
   constexpr int TT[3] = {TL::TX, TL::TY, TL::TZ};
   const int tid = threadIdx.x;
-  const bool tma = tm != nullptr;
+  const bool tma = tm != nullptr && TL::SP == 0;  // scalar planes are staged by plain loads
   if (tma) {
     if (tid == 0) {
       mbar_init(bar, 1);
@@ -241,6 +262,10 @@ __device__ __forceinline__ void stage_region(const GridDev& G, const StageArgs& 
     stage_cell<MAG, GLM>(G, A, gi, gj, gk, q);
 #pragma unroll
     for (int s = 0; s < NQ; s++) P[s][w] = q[s];
+    if constexpr (TL::SP > 0) {
+      const size_t cs = scalar_image(G, gi, gj, gk);
+      for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = A.pin[(size_t)(NP + n) * A.plane + cs];
+    }
   }
   __syncthreads();
 }
@@ -275,6 +300,9 @@ __host__ __device__ __forceinline__ void rk_coefficients(int iter, int type, dou
 __device__ __forceinline__ StageArgs batch_stage_args(SimDesc& S, int stage, int rk) {
   StageArgs a;
   rk_coefficients(stage, rk, &a.faco, &a.fact, &a.facn);
+  a.stage = stage;
+  a.nspc = 0;
+  a.spcorg = nullptr;
   const int pin = (S.pcur + stage - 1) & 1;
   a.pin = S.P[pin];
   a.pout = S.P[pin ^ 1];

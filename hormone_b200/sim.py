@@ -28,6 +28,9 @@ class Simulation:
         st = _state
         self.ctx = capi.Context(cfg, self.grid, precision=precision)
         self.ctx.upload(u=st["u"], prim=list(st["prim"]), grvphi=grvphi, grvpsi=grvpsi)
+        self.nspc = int(cfg.get("nspc", 0))
+        if self.nspc:
+            self.ctx.upload_scalars(st["spc"])
         self.time, self.tn = (0.0, 0) if _clock is None else _clock
         # restart.f90: t_out = time + dt_out after a restart
         self.t_out = cfg["t_out"] if _clock is None else self.time + cfg["dt_out"]
@@ -60,7 +63,8 @@ class Simulation:
         fields = self.ctx.checkpoint_wait()
         tn, time, cgrav_old = self._ck
         if path:
-            binio.writebin(path, tn, time, fields, bool(self.cfg["mag_on"]), self.cfg["gravswitch"], cgrav_old)
+            binio.writebin(path, tn, time, fields, bool(self.cfg["mag_on"]), self.cfg["gravswitch"], cgrav_old,
+                           species=self.cfg.get("species"))
             if "u" in fields:
                 np.save(path + ".u.npy", fields["u"])
         out = dict(fields)
@@ -80,7 +84,7 @@ class Simulation:
         bit for bit."""
         import os
 
-        f = binio.readbin(path, cfg["n"], bool(cfg["mag_on"]), cfg["gravswitch"])
+        f = binio.readbin(path, cfg["n"], bool(cfg["mag_on"]), cfg["gravswitch"], cfg.get("compswitch", 0))
         st = ic.restart_state(cfg, f)
         if os.path.exists(path + ".u.npy"):
             st["u"] = np.ascontiguousarray(np.load(path + ".u.npy"))
@@ -121,7 +125,10 @@ class Simulation:
         return self.time >= self.t_end
 
     def state(self, gravity: bool = False) -> Dict[str, np.ndarray]:
-        return self.ctx.download(gravity=gravity)
+        out = self.ctx.download(gravity=gravity)
+        if self.nspc:
+            out["spc"] = self.ctx.download_scalars()
+        return out
 
     def close(self):
         self.ctx.close()

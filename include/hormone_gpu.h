@@ -63,6 +63,7 @@ typedef struct {
   int maxtngrv;
   int outstyle, endstyle;
   int precision;   /* 0 FP64 (bit-compatible), 1 FP32 flux / FP64 accumulation */
+  int nspc;        /* passive scalars: spn with compswitch 2, else 0 (at most 4; FP64 single grids) */
 } hmn_params;
 
 /* allocations.f90 + metric.f90 for this grid: allocates device state. */
@@ -100,6 +101,14 @@ int hmn_phidamp(hmn_ctx* ctx);
  * pointers are skipped. */
 int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi);
 
+/* Passive scalars (compswitch 2: module physval's spc(1:spn,i,j,k), species
+ * fastest, then i, j, k with the grid's ghost layers): upload the mass
+ * fractions of the initial or restart state, or copy the current ones back.
+ * They are advected with the mass flux as src/main/numflux.f90:200-212 and
+ * rungekutta.f90:61-86 do. */
+int hmn_upload_scalars(hmn_ctx* ctx, const double* spc);
+int hmn_download_scalars(hmn_ctx* ctx, double* spc);
+
 /* Gas pressure p = (gamma-1)*eint of the current state (eos.f90:742-794). */
 int hmn_download_pressure(hmn_ctx* ctx, double* p);
 
@@ -117,12 +126,14 @@ int hmn_gravity_clock(hmn_ctx* ctx, double* grvtime, double* cgrav_old);
  * v3, e, b1, b2, b3, phi; grvphi and grvpsi with gravswitch 3), plus, when u
  * is not NULL, the conserved planes for an exact resume.  begin snapshots
  * the state on the device, ordered after the work enqueued so far, and
- * copies it to host staging on a separate stream while later steps run;
+ * copies it to host staging on a separate stream while later steps run
+ * (spc, if not NULL, receives the passive scalars as hmn_download_scalars);
  * wait blocks until that copy is done and fills the caller's arrays (laid
  * out as for hmn_download).  The arrays given to begin must stay valid until
  * wait returns.  One checkpoint is in flight at a time: begin first waits
  * for the previous one. */
-int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi);
+int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi,
+                         double* spc);
 int hmn_checkpoint_wait(hmn_ctx* ctx);
 
 /* Advance whole steps on the device without host round trips: the loop of

@@ -29,8 +29,22 @@ def kh2d(n=32, ratio=2.0, bx=0.05, bc_y=0, limiter="modified_mc"):
     return cfg, ic.kelvin_helmholtz(cfg, G.make_grid(cfg), ratio, bx)
 
 
-def blast3d(n=16, bc=2, mag=False, limiter="minmod"):
+def add_scalars(cfg, prims, seed=11):
+    """Two passive scalars that sum to one: a smooth seeded field and its
+    complement (what compswitch 2 carries)."""
+    rng = np.random.default_rng(seed)
+    shape = prims["d"].shape
+    base = 0.5 + 0.4 * np.sin(np.arange(shape[2]) * 0.37)[None, None, :] * np.cos(np.arange(shape[1]) * 0.21)[None, :, None]
+    x = np.clip(base + 0.05 * rng.uniform(-1, 1, size=shape), 0.0, 1.0)
+    prims = dict(prims)
+    prims["spc"] = np.stack([x, 1.0 - x])
+    return prims
+
+
+def blast3d(n=16, bc=2, mag=False, limiter="minmod", nspc=0):
     ov = dict(ie=n, je=n, ke=n, mag_on=mag, gamma=1.4, flux_limiter=limiter, t_end=0.2, dt_out=0.2, courant=0.4)
+    if nspc:
+        ov.update(compswitch=2, spn=nspc)
     for a in (1, 2, 3):
         for tag in ("is", "os", "iv", "ov"):
             ov[f"bc{a}{tag}"] = bc
@@ -39,12 +53,16 @@ def blast3d(n=16, bc=2, mag=False, limiter="minmod"):
     if mag:
         prims["b1"][:] = 0.3
         prims["b3"][:] = -0.2
+    if nspc:
+        prims = add_scalars(cfg, prims)
     return cfg, prims
 
 
-def riemann3d(n=(12, 10, 8), seed=7, bc=(3, 1, 0)):
+def riemann3d(n=(12, 10, 8), seed=7, bc=(3, 1, 0), nspc=0):
     rng = np.random.default_rng(seed)
     ov = dict(ie=n[0], je=n[1], ke=n[2], mag_on=True, gamma=1.4, t_end=0.1, dt_out=0.1, courant=0.8)
+    if nspc:
+        ov.update(compswitch=2, spn=nspc)
     for a in (1, 2, 3):
         for tag in ("is", "os", "iv", "ov"):
             ov[f"bc{a}{tag}"] = bc[a - 1]
@@ -55,6 +73,8 @@ def riemann3d(n=(12, 10, 8), seed=7, bc=(3, 1, 0)):
     prims = ic.riemann(cfg, 0, st[0], st[1])
     # break the symmetry along y and z as well
     prims["d"] *= 1.0 + 0.1 * np.sin(np.arange(n[1]))[None, :, None] * np.cos(np.arange(n[2]))[:, None, None]
+    if nspc:
+        prims = add_scalars(cfg, prims)
     return cfg, prims
 
 

@@ -123,3 +123,28 @@ def test_restart_from_a_plain_dump_follows_the_reference(tmp_path):
     assert np.sum(np.abs(da - db)) / np.sum(np.abs(da)) <= 1e-3
     a.close()
     b.close()
+
+
+def test_dump_with_passive_scalars(tmp_path):
+    """compswitch 2: the dump carries the scalars block (readbin.f90:80-90)
+    and an exact restart resumes them bit for bit."""
+    cfg, prims = cases.golden_case("KHinstability")
+    a = Simulation(cfg, prims)
+    for _ in range(4):
+        a.step()
+    path = str(tmp_path / "kh.dat")
+    snap = a.write_bin(path, exact=True)
+    back = binio.readbin(path, cfg["n"], False, 0, 2)
+    assert back["species"] == ["scalar1", "scalar2"]
+    assert np.array_equal(np.moveaxis(back["spc"], -1, 0), snap["spc"])
+    assert np.array_equal(snap["spc"], a.state()["spc"])
+    for _ in range(5):
+        a.step()
+    b = Simulation.restart(cfg, path)
+    for _ in range(5):
+        b.step()
+    sa, sb = a.state(), b.state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+    a.close()
+    b.close()

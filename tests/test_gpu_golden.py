@@ -17,7 +17,7 @@ import norms
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 NAMES = [f"{k}_{d}" for k in ("sodshock", "briowushock") for d in "xyz"] + \
-        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")]
+        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability"]
 NAMES = NAMES + [n + "_flat" for n in NAMES]
 
 
@@ -30,6 +30,8 @@ def test_gpu_matches_golden(name):
     assert s.tn == int(gold["tn"]) and s.time == float(gold["time"])
     st = s.state()
     s.close()
+    for n in range(cfg["nspc"]):
+        st[f"spc{n}"] = st["spc"][n]
     res = norms.compare(st, gold, cfg)
     assert max(r["L2"] for r in res.values()) < cfg["test_tol"], res
     for lab, r in res.items():

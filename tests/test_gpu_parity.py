@@ -29,6 +29,8 @@ def compare(o, s, where):
         assert bad.size == 0, f"{where}: u[{q}] differs at {bad[:5]}: {st['u'][q].flat[bad[:3]]} vs {ou[q].flat[bad[:3]]}"
     for k in PRIMS:
         assert np.array_equal(st[k], o.get(k)), f"{where}: primitive {k} differs"
+    for n in range(int(s.cfg.get("nspc", 0))):
+        assert np.array_equal(st["spc"][n], o.get(f"spc{n}")), f"{where}: scalar {n} differs"
 
 
 def run_pair(cfg, prims, nsteps, grvphi=None, cgrav_old=0.0, check_every=1):
@@ -124,3 +126,15 @@ def test_tma_staged_region_fp64(monkeypatch, make):
     monkeypatch.setenv("HMN_TMA", "1")
     cfg, prims = make()
     run_pair(cfg, prims, 4)
+
+
+@pytest.mark.parametrize("make", [lambda: cases.golden_case("KHinstability"),
+                                  lambda: cases.golden_case("KHinstability_flat"),
+                                  lambda: cases.blast3d(14, bc=1, nspc=2),
+                                  lambda: cases.riemann3d(nspc=2)])
+def test_passive_scalars(make):
+    """Two passive scalars advected with the mass flux (numflux.f90:200-212,
+    rungekutta.f90:61-86): 2-D KH (the reference's own test), and 3-D with
+    reflective, free and periodic boundaries, MHD and hydro."""
+    cfg, prims = make()
+    run_pair(cfg, prims, 6)
