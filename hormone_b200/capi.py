@@ -301,3 +301,57 @@ class Context:
 
     def stream_ptr(self) -> int:
         return int(lib().hmn_stream(self.h) or 0)
+
+
+# ---------------------------------------------------------------------------
+# slab decomposition along z (hmn_set_slab and friends)
+
+def _bind_slab(L):
+    if getattr(L, "_hmn_slab_bound", False):
+        return L
+    L.hmn_slab_halo_bytes.argtypes = [_P]
+    L.hmn_slab_halo_bytes.restype = ctypes.c_size_t
+    L.hmn_set_slab.argtypes = [_P, _P, _P, _P, _P, _I, _I]
+    L.hmn_pack_halos.argtypes = [_P]
+    L.hmn_hydro_stage.argtypes = [_P, _I]
+    L.hmn_cfl_local.argtypes = [_P, _D, _D, _D]
+    L.hmn_cfl_partials.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]
+    L.hmn_cfl_finalize.argtypes = [_P, _DP, _DP]
+    for n in ("hmn_set_slab", "hmn_pack_halos", "hmn_hydro_stage", "hmn_cfl_local", "hmn_cfl_partials",
+              "hmn_cfl_finalize"):
+        getattr(L, n).restype = _I
+    L._hmn_slab_bound = True
+    return L
+
+
+class SlabContext(Context):
+    """A Context for one slab of a z-decomposed grid."""
+
+    def halo_bytes(self) -> int:
+        return int(_bind_slab(lib()).hmn_slab_halo_bytes(self.h))
+
+    def set_slab(self, send_lo, send_hi, recv_lo, recv_hi, wrap_lo=False, wrap_hi=False):
+        """Device addresses (ints, 0 for a physical face) of the halo buffers;
+        wrap_* mark the grid's periodic z boundary."""
+        L = _bind_slab(lib())
+        self._check(L.hmn_set_slab(self.h, send_lo or None, send_hi or None, recv_lo or None, recv_hi or None,
+                                   int(bool(wrap_lo)), int(bool(wrap_hi))), "hmn_set_slab")
+
+    def pack_halos(self):
+        self._check(_bind_slab(lib()).hmn_pack_halos(self.h), "hmn_pack_halos")
+
+    def hydro_stage(self, stage: int):
+        self._check(_bind_slab(lib()).hmn_hydro_stage(self.h, int(stage)), "hmn_hydro_stage")
+
+    def cfl_local(self, time, t_out, t_end):
+        self._check(_bind_slab(lib()).hmn_cfl_local(self.h, float(time), float(t_out), float(t_end)), "hmn_cfl_local")
+
+    def cfl_partials(self):
+        a, b = _P(), _P()
+        self._check(_bind_slab(lib()).hmn_cfl_partials(self.h, ctypes.byref(a), ctypes.byref(b)), "hmn_cfl_partials")
+        return int(a.value), int(b.value)
+
+    def cfl_finalize(self):
+        dt, ch = _D(), _D()
+        self._check(_bind_slab(lib()).hmn_cfl_finalize(self.h, ctypes.byref(dt), ctypes.byref(ch)), "hmn_cfl_finalize")
+        return dt.value, ch.value

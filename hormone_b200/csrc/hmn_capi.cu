@@ -50,6 +50,7 @@ struct hmn_ctx {
   int graph_steps;
   TmaMaps tmaps[2];          // tensor maps of pbuf[0], pbuf[1] for TMA staging of 3-D tiles
   int tma_ok;
+  double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
   double* spcorg;            // passive scalars times density at RK stage 1
   // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
   cudaStream_t cst;
@@ -201,6 +202,9 @@ static int to_host(hmn_ctx* ctx, double* dst, const double* src, int nplanes, si
         for (int i = 0; i < ctx->n[0]; i++) dst[q * dst_plane_stride + ghosted_index(ctx, i, j, k)] = ctx->stage_h[o++];
   return HMN_OK;
 }
+
+// a slab of a z-decomposed grid with at least one neighbouring slab
+static bool slab_exchanges(const hmn_ctx* ctx) { return ctx->G.zhalo[0] || ctx->G.zhalo[1]; }
 
 static int blocks_for(const hmn_ctx* ctx) {
   size_t b = (ctx->plane + 255) / 256;
@@ -498,6 +502,7 @@ static int enqueue_cfl(hmn_ctx* ctx) {
 
 extern "C" int hmn_timestep(hmn_ctx* ctx, double time, double t_out, double t_end, double* dt, double* ch) {
   if (!ctx) return HMN_EINVAL;
+  if (slab_exchanges(ctx)) return HMN_EBADCFG;  // dt is a reduction over all slabs
   int rc = push_times(ctx, time, t_out, t_end);
   if (rc) return rc;
   rc = enqueue_cfl(ctx);
@@ -522,12 +527,14 @@ static void rk_coeff(int iter, int type, double* faco, double* fact, double* fac
   }
 }
 
-static int enqueue_hydro(hmn_ctx* ctx) {
+// RK stage s (1..rktype) of the current step; the last stage also does the
+// step's buffer bookkeeping
+static int enqueue_stage(hmn_ctx* ctx, int s) {
   const int rk = ctx->par.rktype;
   double* A = ctx->buf[0];
   double* B = ctx->buf[1];
   double* C = ctx->buf[2];
-  for (int s = 1; s <= rk; s++) {
+  {
     StageArgs a;
     memset(&a, 0, sizeof(a));
     rk_coeff(s, rk, &a.faco, &a.fact, &a.facn);
@@ -569,19 +576,97 @@ static int enqueue_hydro(hmn_ctx* ctx) {
     ctx->launches += 1;
     ctx->pcur = 1 - ctx->pcur;
   }
-  if (rk == 1) {
-    double* t = ctx->buf[0];
-    ctx->buf[0] = ctx->buf[1];
-    ctx->buf[1] = t;
+  if (s == rk) {
+    if (rk == 1) {
+      double* t = ctx->buf[0];
+      ctx->buf[0] = ctx->buf[1];
+      ctx->buf[1] = t;
+    }
+    ctx->phifac = 1.0;
   }
-  ctx->phifac = 1.0;
+  return HMN_OK;
+}
+
+static int enqueue_hydro(hmn_ctx* ctx) {
+  for (int s = 1; s <= ctx->par.rktype; s++) {
+    int rc = enqueue_stage(ctx, s);
+    if (rc) return rc;
+  }
   return HMN_OK;
 }
 
 extern "C" int hmn_hydro_step(hmn_ctx* ctx) {
   if (!ctx) return HMN_EINVAL;
+  if (slab_exchanges(ctx)) return HMN_EBADCFG;  // the halos must be exchanged between stages
   ctx->graph_steps = 0;
   return enqueue_hydro(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// slab decomposition along z (mpi_domain.F90's role for this path)
+
+extern "C" size_t hmn_slab_halo_bytes(const hmn_ctx* ctx) {
+  if (!ctx) return 0;
+  return (size_t)(10 + ctx->par.nspc) * 2 * (size_t)ctx->n[0] * ctx->n[1] * sizeof(double);
+}
+
+extern "C" int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo,
+                            const double* recv_hi, int wrap_lo, int wrap_hi) {
+  if (!ctx) return HMN_EINVAL;
+  if (!ctx->solve[2] || ctx->n[2] < 2 || ctx->par.gravswitch != 0) return HMN_EBADCFG;
+  if ((recv_lo && !send_lo) || (recv_hi && !send_hi)) return HMN_EINVAL;
+  ctx->zsend[0] = send_lo;
+  ctx->zsend[1] = send_hi;
+  ctx->G.zhalo[0] = recv_lo;
+  ctx->G.zhalo[1] = recv_hi;
+  ctx->G.zwrap[0] = recv_lo && wrap_lo ? 1 : 0;
+  ctx->G.zwrap[1] = recv_hi && wrap_hi ? 1 : 0;
+  return HMN_OK;
+}
+
+extern "C" int hmn_pack_halos(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  if (!slab_exchanges(ctx)) return HMN_OK;  // a single slab has nothing to send
+  CK(launch_pack_zhalos(ctx->pbuf[ctx->pcur], ctx->n, 10 + ctx->par.nspc, ctx->zsend[0], ctx->zsend[1],
+                        blocks_for(ctx), ctx->st),
+     "pack halos");
+  ctx->launches += 1;
+  return HMN_OK;
+}
+
+extern "C" int hmn_hydro_stage(hmn_ctx* ctx, int stage) {
+  if (!ctx || stage < 1 || stage > ctx->par.rktype) return HMN_EINVAL;
+  ctx->graph_steps = 0;
+  return enqueue_stage(ctx, stage);
+}
+
+extern "C" int hmn_cfl_local(hmn_ctx* ctx, double time, double t_out, double t_end) {
+  if (!ctx) return HMN_EINVAL;
+  int rc = push_times(ctx, time, t_out, t_end);
+  if (rc) return rc;
+  CK(launch_cfl_cells(ctx->G, ctx->pbuf[ctx->pcur], ctx->plane, ctx->par.gamma, ctx->sc, ctx->mag,
+                      blocks_for(ctx), ctx->st),
+     "cfl");
+  ctx->launches += 1;
+  return HMN_OK;
+}
+
+extern "C" int hmn_cfl_partials(hmn_ctx* ctx, double** min_dti, double** cfmax) {
+  if (!ctx) return HMN_EINVAL;
+  static_assert(sizeof(unsigned long long) == sizeof(double), "bit patterns");
+  if (min_dti) *min_dti = reinterpret_cast<double*>(&ctx->sc->min_dti_bits);
+  if (cfmax) *cfmax = reinterpret_cast<double*>(&ctx->sc->cfmax_bits);
+  return HMN_OK;
+}
+
+extern "C" int hmn_cfl_finalize(hmn_ctx* ctx, double* dt, double* ch) {
+  if (!ctx) return HMN_EINVAL;
+  CK(launch_cfl_finalize(ctx->sc, ctx->st), "cfl");
+  ctx->launches += 1;
+  int rc = fetch_scalars(ctx);
+  if (dt) *dt = ctx->sc_h->dt;
+  if (ch) *ch = ctx->sc_h->ch;
+  return rc;
 }
 
 extern "C" int hmn_phidamp(hmn_ctx* ctx) {
@@ -863,6 +948,7 @@ static int enqueue_step(hmn_ctx* ctx) {
 
 extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, int* steps) {
   if (!ctx || !time) return HMN_EINVAL;
+  if (slab_exchanges(ctx)) return HMN_EBADCFG;
   if (ctx->par.gravswitch == 3) {
     // the sub-cycle count depends on each step's dt: step on the host clock
     int done = 0;

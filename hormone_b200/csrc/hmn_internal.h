@@ -38,6 +38,14 @@ struct GridDev {
   int solve[3];
   int bc[3][2][2];  // [axis][inner,outer][scalar,vector]
   AxisGeo g[3];
+  // slab decomposition along z: the two cell layers beyond the low / high z
+  // face come from the neighbouring slab (primitive planes x 2 layers x
+  // nx*ny, filled by the caller's exchange) instead of the boundary codes;
+  // nullptr on a physical face; zwrap[io] = 1 where the face is the grid's
+  // periodic z boundary, whose ghosts take the boundary condition's form
+  // (energies rebuilt from the pressure) rather than the interior values
+  const double* zhalo[2];
+  int zwrap[2];
 };
 
 // Device-resident scalars of one simulation: the CFL reduction slots, the
@@ -124,6 +132,13 @@ cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool gl
 // mixed precision (hmn_mixed.cu): FP32 Riemann solver, FP64 reconstruction and accumulation
 cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                                cudaStream_t st);
+// the two halves of launch_cfl: the per-cell reduction and the dt finalisation
+cudaError_t launch_cfl_cells(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc,
+                             bool mag, int nblocks, cudaStream_t st);
+cudaError_t launch_cfl_finalize(DevScalars* sc, cudaStream_t st);
+// the two boundary layers of each primitive plane next to the low / high z face
+cudaError_t launch_pack_zhalos(const double* P, const int n[3], int nplanes, double* send_lo, double* send_hi,
+                               int nblocks, cudaStream_t st);
 cudaError_t launch_cfl(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc, bool mag,
                        int nblocks, cudaStream_t st);
 cudaError_t launch_prim_init(double* P, size_t plane, bool mag, int nblocks, cudaStream_t st);

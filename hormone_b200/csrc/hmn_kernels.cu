@@ -665,6 +665,39 @@ cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool gl
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_cfl_cells(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc,
+                             bool mag, int nblocks, cudaStream_t st) {
+  if (mag)
+    cfl_kernel<true><<<nblocks, 256, 0, st>>>(G, P, plane, gamma, sc);
+  else
+    cfl_kernel<false><<<nblocks, 256, 0, st>>>(G, P, plane, gamma, sc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cfl_finalize(DevScalars* sc, cudaStream_t st) {
+  cfl_finalize_kernel<<<1, 32, 0, st>>>(sc);
+  return cudaGetLastError();
+}
+
+// send_lo[p][l][j][i] = P[p][k=l], send_hi[p][l][j][i] = P[p][k=nz-2+l]
+__global__ void pack_zhalos_kernel(const double* P, int nx, int ny, int nz, int nplanes, double* send_lo,
+                                   double* send_hi) {
+  const size_t hp = (size_t)nx * ny, plane = hp * nz;
+  const size_t total = (size_t)nplanes * 2 * hp;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = t / (2 * hp), r = t % (2 * hp);
+    const size_t l = r / hp, c = r % hp;
+    if (send_lo) send_lo[t] = P[p * plane + l * hp + c];
+    if (send_hi) send_hi[t] = P[p * plane + ((size_t)nz - 2 + l) * hp + c];
+  }
+}
+
+cudaError_t launch_pack_zhalos(const double* P, const int n[3], int nplanes, double* send_lo, double* send_hi,
+                               int nblocks, cudaStream_t st) {
+  pack_zhalos_kernel<<<nblocks, 256, 0, st>>>(P, n[0], n[1], n[2], nplanes, send_lo, send_hi);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_cfl(const GridDev& G, const double* P, size_t plane, double gamma, DevScalars* sc, bool mag,
                        int nblocks, cudaStream_t st) {
   if (mag)

@@ -129,6 +129,33 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
   const int s = c3[ax];
   const int io = s < 0 ? 0 : 1;
   const int gl = io == 0 ? s + 2 : s - n;  // ghost layer 0 or 1
+  if (ax == 2 && G.zhalo[io] != nullptr) {
+    // a neighbouring slab's interior cell: staged exactly as our own interior cells
+    const size_t hp = (size_t)G.n[0] * G.n[1];
+    const size_t h = (size_t)gl * hp + (size_t)i + (size_t)G.n[0] * j;
+    const double* H = G.zhalo[io];
+    const double d = H[h];
+    const double v1 = H[PV * 2 * hp + h], v2 = H[(PV + 1) * 2 * hp + h], v3 = H[(PV + 2) * 2 * hp + h];
+    const double b1 = MAG ? H[PB * 2 * hp + h] : 0.0, b2 = MAG ? H[(PB + 1) * 2 * hp + h] : 0.0;
+    const double b3 = MAG ? H[(PB + 2) * 2 * hp + h] : 0.0;
+    q[Q_D] = d;
+    q[Q_M + 0] = d * v1;
+    q[Q_M + 1] = d * v2;
+    q[Q_M + 2] = d * v3;
+    q[Q_B + 0] = b1;
+    q[Q_B + 1] = b2;
+    q[Q_B + 2] = b3;
+    q[Q_PHI] = GLM ? H[PPHI * 2 * hp + h] * A.phifac : 0.0;
+    if (G.zwrap[io]) {  // periodic ghost as the boundary condition forms it (see below)
+      const double eg = (A.gm1 * H[PEINT * 2 * hp + h]) / A.gm1;
+      q[Q_E] = eg + 0.5 * (d * (v1 * v1 + v2 * v2 + v3 * v3) + b1 * b1 + b2 * b2 + b3 * b3);
+      q[Q_EINT] = eg;
+    } else {
+      q[Q_E] = H[PE * 2 * hp + h];
+      q[Q_EINT] = H[PEINT * 2 * hp + h];
+    }
+    return;
+  }
   const int per = io == 0 ? n - 2 + gl : gl;
   const int refl = io == 0 ? 1 - gl : n - 1 - gl;
   const int edge = io == 0 ? 0 : n - 1;
@@ -263,8 +290,15 @@ __device__ __forceinline__ void stage_region(const GridDev& G, const StageArgs& 
 #pragma unroll
     for (int s = 0; s < NQ; s++) P[s][w] = q[s];
     if constexpr (TL::SP > 0) {
-      const size_t cs = scalar_image(G, gi, gj, gk);
-      for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = A.pin[(size_t)(NP + n) * A.plane + cs];
+      const int zio = gk < 0 ? 0 : 1;
+      if ((gk < 0 || gk >= G.n[2]) && G.zhalo[zio] != nullptr) {  // neighbouring slab
+        const size_t hp = (size_t)G.n[0] * G.n[1];
+        const size_t h = (size_t)(zio == 0 ? gk + 2 : gk - G.n[2]) * hp + (size_t)gi + (size_t)G.n[0] * gj;
+        for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = G.zhalo[zio][(size_t)(NP + n) * 2 * hp + h];
+      } else {
+        const size_t cs = scalar_image(G, gi, gj, gk);
+        for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = A.pin[(size_t)(NP + n) * A.plane + cs];
+      }
     }
   }
   __syncthreads();

@@ -1,0 +1,265 @@
+"""One grid decomposed into slabs along z, one slab per GPU.
+
+This is the role of the reference's MPI domain decomposition
+(src/main/mpi_domain.F90:256-339) for this path.  A rank owns the layers
+[k0, k1) of the global grid.  Before every RK stage it exchanges the two
+boundary layers of each primitive plane with its z neighbours; that is the
+only data exchange of the step.  The CFL timestep is the all-reduced
+minimum of the per-slab reductions (timestep.f90:56,87).  A slab's result is
+bit-identical to the same cells of the undecomposed run: every cell sees the
+same neighbours and the same operation order, and min/max reductions are
+exact.
+
+Two exchanges are provided:
+
+- ``TorchExchange``: one process per slab over ``torch.distributed``.  It
+  uses NCCL with CUDA tensors on GPUs and gloo with CPU tensors for the
+  host-side tests.
+- ``LocalExchange``: all slabs in one process, e.g. on one GPU, exchanging
+  by device copies.
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import capi, grid as gridmod, ic
+
+PRIMS = ("d", "v1", "v2", "v3", "e", "b1", "b2", "b3", "phi")
+
+
+def partition(nz: int, world: int) -> List[Tuple[int, int]]:
+    """Contiguous slabs [k0, k1) of as equal size as possible; each needs at
+    least 2 layers (the stencil's reach)."""
+    if world < 1 or nz < 2 * world:
+        raise ValueError(f"cannot split {nz} layers into {world} slabs of at least 2")
+    base, extra = divmod(nz, world)
+    out, k = [], 0
+    for r in range(world):
+        size = base + (1 if r < extra else 0)
+        out.append((k, k + size))
+        k += size
+    return out
+
+
+def neighbours(rank: int, world: int, periodic: bool) -> Tuple[Optional[int], Optional[int]]:
+    """Ranks of the lower and upper z neighbours (None at a physical face)."""
+    lo = rank - 1 if rank > 0 else (world - 1 if periodic and world > 1 else None)
+    hi = rank + 1 if rank < world - 1 else (0 if periodic and world > 1 else None)
+    return lo, hi
+
+
+def slab_config(cfg: dict, k0: int, k1: int) -> dict:
+    """The configuration of the slab [k0, k1): same settings, n[2] = k1 - k0."""
+    c = dict(cfg)
+    c["n"] = [cfg["n"][0], cfg["n"][1], k1 - k0]
+    c["ke"] = c["ks"] + (k1 - k0) - 1 if "ks" in c else k1 - k0
+    return c
+
+
+def slab_grid(grid, k0: int, k1: int):
+    """The global grid's z arrays restricted to the slab and its two ghost
+    layers on each side (they are the neighbours' cells)."""
+    out = [dict(grid[0]), dict(grid[1]), {}]
+    for key, arr in grid[2].items():
+        out[2][key] = np.ascontiguousarray(arr[k0:k1 + 4]) if isinstance(arr, np.ndarray) and arr.ndim == 1 else arr
+    return out
+
+
+class _DeviceArray:
+    """A device pointer exposed through __cuda_array_interface__ (for
+    torch.as_tensor views of memory the library owns)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str = "<f8"):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 2}
+
+
+class SlabSimulation:
+    """One rank's slab: the step of src/main/hormone.f90:126-155 split into the
+    phases that the exchange interleaves."""
+
+    def __init__(self, cfg: dict, prims_global: Dict[str, np.ndarray], k0: int, k1: int, precision: int = 0,
+                 halo_alloc=None, local: bool = False):
+        """prims_global: the global primitives (sliced here), or with
+        local=True the slab's own primitives."""
+        import torch
+
+        self.cfg_global = cfg
+        self.k0, self.k1 = k0, k1
+        self.cfg = slab_config(cfg, k0, k1)
+        self.grid = slab_grid(gridmod.make_grid(cfg), k0, k1)
+        if local:
+            local = prims_global
+        else:
+            local = {k: (v[..., k0:k1, :, :] if k == "spc" else v[k0:k1]) for k, v in prims_global.items()}
+        st = ic.to_state(self.cfg, local)
+        self.ctx = capi.SlabContext(self.cfg, self.grid, precision=precision)
+        self.ctx.upload(u=st["u"], prim=list(st["prim"]))
+        self.nspc = int(self.cfg.get("nspc", 0))
+        if self.nspc:
+            self.ctx.upload_scalars(st["spc"])
+        n = self.ctx.halo_bytes() // 8
+        alloc = halo_alloc or (lambda m: torch.zeros(m, dtype=torch.float64, device="cuda"))
+        self.send_lo, self.send_hi, self.recv_lo, self.recv_hi = (alloc(n) for _ in range(4))
+        self.time, self.tn = 0.0, 0
+        self.t_out, self.t_end = cfg["t_out"], cfg["t_end"]
+        self.dt = self.ch = 0.0
+        self.mag_glm = bool(cfg["mag_on"]) and cfg["dim"] > 1
+        pmin, pmax = self.ctx.cfl_partials()
+        self.cfl_min = torch.as_tensor(_DeviceArray(pmin, 1), device="cuda")
+        self.cfl_max = torch.as_tensor(_DeviceArray(pmax, 1), device="cuda")
+
+    def connect(self, has_lo: bool, has_hi: bool, wrap_lo: bool = False, wrap_hi: bool = False):
+        """Attach the halo buffers; wrap_* mark faces that are the grid's
+        periodic z boundary (first slab low, last slab high)."""
+        p = lambda t: t.data_ptr()  # noqa: E731
+        self.ctx.set_slab(p(self.send_lo) if has_lo else 0, p(self.send_hi) if has_hi else 0,
+                          p(self.recv_lo) if has_lo else 0, p(self.recv_hi) if has_hi else 0, wrap_lo, wrap_hi)
+
+    def stream(self):
+        import torch
+
+        return torch.cuda.ExternalStream(self.ctx.stream_ptr())
+
+    # phases of one step
+    def cfl_local(self):
+        self.ctx.cfl_local(self.time, self.t_out, self.t_end)
+
+    def cfl_finalize(self):
+        self.dt, self.ch = self.ctx.cfl_finalize()
+
+    def finish_step(self) -> bool:
+        if self.mag_glm:
+            self.ctx.phidamp()
+        self.time = self.time + self.dt
+        self.tn += 1
+        c = self.cfg
+        if c["endstyle"] == 1 and self.time >= self.t_end:
+            return True
+        if c["endstyle"] == 2 and self.tn >= c["tnlim"]:
+            return True
+        if c["outstyle"] == 1 and self.time >= self.t_out:
+            self.t_out = self.t_out + c["dt_out"]
+        return False
+
+    def state(self) -> Dict[str, np.ndarray]:
+        out = self.ctx.download()
+        if self.nspc:
+            out["spc"] = self.ctx.download_scalars()
+        return out
+
+    def close(self):
+        self.ctx.close()
+
+
+class LocalExchange:
+    """All slabs of a grid in one process (e.g. on one GPU): halos move by
+    device copies, the CFL partials by an in-process min/max."""
+
+    def __init__(self, cfg: dict, prims: Dict[str, np.ndarray], world: int, precision: int = 0):
+        self.periodic = int(cfg["bc"][2][0][0]) == 0
+        self.parts = partition(cfg["n"][2], world)
+        self.ranks = [SlabSimulation(cfg, prims, k0, k1, precision) for k0, k1 in self.parts]
+        self.nb = [neighbours(r, world, self.periodic) for r in range(world)]
+        for r, s in enumerate(self.ranks):
+            lo, hi = self.nb[r]
+            s.connect(lo is not None, hi is not None, wrap_lo=r == 0, wrap_hi=r == world - 1)
+
+    def _sync(self):
+        import torch
+
+        for s in self.ranks:
+            s.ctx.sync()
+        torch.cuda.synchronize()
+
+    def step(self) -> bool:
+        import torch
+
+        for s in self.ranks:
+            s.cfl_local()
+        self._sync()
+        gmin = torch.min(torch.cat([s.cfl_min for s in self.ranks]))
+        gmax = torch.max(torch.cat([s.cfl_max for s in self.ranks]))
+        for s in self.ranks:
+            s.cfl_min.copy_(gmin.reshape(1))
+            s.cfl_max.copy_(gmax.reshape(1))
+        torch.cuda.synchronize()
+        for s in self.ranks:
+            s.cfl_finalize()
+        for stage in range(1, self.cfg_rk() + 1):
+            for s in self.ranks:
+                s.ctx.pack_halos()
+            self._sync()
+            for r, s in enumerate(self.ranks):
+                lo, hi = self.nb[r]
+                if lo is not None:
+                    s.recv_lo.copy_(self.ranks[lo].send_hi)
+                if hi is not None:
+                    s.recv_hi.copy_(self.ranks[hi].send_lo)
+            torch.cuda.synchronize()
+            for s in self.ranks:
+                s.ctx.hydro_stage(stage)
+        ends = [s.finish_step() for s in self.ranks]
+        return ends[0]
+
+    def cfg_rk(self) -> int:
+        return int(self.ranks[0].cfg["rktype"])
+
+    def state(self) -> Dict[str, np.ndarray]:
+        """The global state assembled from the slabs (z is the slowest axis)."""
+        parts = [s.state() for s in self.ranks]
+        out = {}
+        for k in parts[0]:
+            axis = 1 if parts[0][k].ndim == 4 else 0
+            out[k] = np.concatenate([p[k] for p in parts], axis=axis)
+        return out
+
+    def close(self):
+        for s in self.ranks:
+            s.close()
+
+
+class TorchExchange:
+    """One slab per process over torch.distributed (NCCL on GPUs, gloo for
+    CPU tensors).  Every rank posts its sends high-then-low and its receives
+    low-then-high, so with two periodic ranks (both neighbours the same
+    peer) the messages still pair up face to face."""
+
+    def __init__(self, dist, rank: int, world: int, periodic: bool):
+        self.dist, self.rank, self.world = dist, rank, world
+        self.lo, self.hi = neighbours(rank, world, periodic)
+
+    def halos(self, send_lo, send_hi, recv_lo, recv_hi):
+        d = self.dist
+        ops = []
+        if self.hi is not None:
+            ops.append(d.P2POp(d.isend, send_hi, self.hi))
+        if self.lo is not None:
+            ops.append(d.P2POp(d.isend, send_lo, self.lo))
+        if self.lo is not None:
+            ops.append(d.P2POp(d.irecv, recv_lo, self.lo))
+        if self.hi is not None:
+            ops.append(d.P2POp(d.irecv, recv_hi, self.hi))
+        if ops:
+            for req in d.batch_isend_irecv(ops):
+                req.wait()
+
+    def cfl(self, tmin, tmax):
+        self.dist.all_reduce(tmin, op=self.dist.ReduceOp.MIN)
+        self.dist.all_reduce(tmax, op=self.dist.ReduceOp.MAX)
+
+
+def run_distributed_step(sim: SlabSimulation, ex: TorchExchange) -> bool:
+    """One step of one rank, the collectives ordered on the slab's stream."""
+    import torch
+
+    with torch.cuda.stream(sim.stream()):
+        sim.cfl_local()
+        ex.cfl(sim.cfl_min, sim.cfl_max)
+        sim.cfl_finalize()
+        for stage in range(1, int(sim.cfg["rktype"]) + 1):
+            sim.ctx.pack_halos()
+            ex.halos(sim.send_lo, sim.send_hi, sim.recv_lo, sim.recv_hi)
+            sim.ctx.hydro_stage(stage)
+    return sim.finish_step()

@@ -136,6 +136,38 @@ int hmn_checkpoint_begin(hmn_ctx* ctx, double* u, double* const prim[9], double*
                          double* spc);
 int hmn_checkpoint_wait(hmn_ctx* ctx);
 
+/* ---- slab decomposition along z -------------------------------------
+ * One grid split into slabs of whole x-y planes, one per context (one per
+ * GPU), as the reference's MPI domain decomposition (mpi_domain.F90:256-339,
+ * timestep.f90:56,87) splits it across processes.  Each context is created
+ * with its own slab: n[2] = the slab's layers (at least 2), the z coordinate
+ * arrays of the slab (with 2 ghost entries each side), and any boundary
+ * codes (those of an internal face are ignored).  hmn_set_slab hands it
+ * four device buffers of hmn_slab_halo_bytes each, owned by the caller:
+ * send_lo/send_hi receive the slab's two lowest/highest layers of every
+ * primitive plane (hmn_pack_halos), recv_lo/recv_hi must hold the lower /
+ * upper neighbour's send_hi / send_lo before each stage.  NULL recv/send
+ * pointers mark a physical face (boundary codes apply).  wrap_lo/wrap_hi = 1
+ * mark a face that is the grid's periodic z boundary (the first slab's low
+ * face, the last slab's high face): its ghosts are formed as the periodic
+ * boundary condition forms them (boundarycondition.f90:222-243 rebuilds
+ * their energies from the pressure).  A step is then:
+ *   hmn_cfl_local; all-reduce *min_dti (MIN) and *cfmax (MAX) from
+ *   hmn_cfl_partials over the slabs (two doubles in device memory, ordered
+ *   on hmn_stream); hmn_cfl_finalize -> dt, ch;
+ *   for each RK stage s: hmn_pack_halos; exchange; hmn_hydro_stage(s);
+ *   hmn_phidamp.
+ * hmn_timestep, hmn_hydro_step and hmn_run refuse a context with
+ * neighbours (HMN_EBADCFG); gravity is not decomposed. */
+size_t hmn_slab_halo_bytes(const hmn_ctx* ctx);
+int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo, const double* recv_hi,
+                 int wrap_lo, int wrap_hi);
+int hmn_pack_halos(hmn_ctx* ctx);
+int hmn_hydro_stage(hmn_ctx* ctx, int stage);
+int hmn_cfl_local(hmn_ctx* ctx, double time, double t_out, double t_end);
+int hmn_cfl_partials(hmn_ctx* ctx, double** min_dti, double** cfmax);
+int hmn_cfl_finalize(hmn_ctx* ctx, double* dt, double* ch);
+
 /* Advance whole steps on the device without host round trips: the loop of
  * hormone.f90:126-155 (timestep, gravity, hydro_step, phidamp, time += dt)
  * until time >= t_end or max_steps steps; the clamps use t_out = t_end.

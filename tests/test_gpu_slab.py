@@ -1,0 +1,98 @@
+"""Slab decomposition along z on one GPU: the slabs of one grid, each its
+own context, exchanging halos by device copies (hormone_b200.slab.
+LocalExchange), give bit for bit the undecomposed run's state and dt,
+periodic or not, with scalars, and in the mixed-precision form."""
+import numpy as np
+import pytest
+
+from hormone_b200 import slab
+from hormone_b200.sim import Simulation
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(cfg, prims, world, steps, precision=0):
+    ref = Simulation(cfg, prims, precision=precision)
+    dec = slab.LocalExchange(cfg, prims, world, precision=precision)
+    for n in range(steps):
+        ref.step()
+        dec.step()
+        for s in dec.ranks:
+            assert s.dt == ref.dt, (n, s.dt, ref.dt)
+    a, b = ref.state(), dec.state()
+    ref.close()
+    dec.close()
+    for k in a:
+        assert a[k].shape == b[k].shape, k
+        assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_orszag_tang_3d_periodic(world):
+    cfg, prims = cases.ot3d(16)
+    run_both(cfg, prims, world, 5)
+
+
+def test_blast_reflective_three_slabs():
+    cfg, prims = cases.blast3d(14, bc=1, mag=True)
+    run_both(cfg, prims, 3, 5)
+
+
+def test_riemann_with_scalars():
+    cfg, prims = cases.riemann3d(n=(12, 10, 8), bc=(3, 1, 0), nspc=2)
+    run_both(cfg, prims, 2, 5)
+
+
+def test_mixed_precision_slabs():
+    cfg, prims = cases.ot3d(16)
+    run_both(cfg, prims, 2, 4, precision=1)
+
+
+def test_decomposed_context_refuses_the_undecomposed_calls():
+    cfg, prims = cases.ot3d(16)
+    dec = slab.LocalExchange(cfg, prims, 2)
+    from hormone_b200 import capi
+
+    with pytest.raises(capi.HmnError):
+        dec.ranks[0].ctx.hydro_step()
+    with pytest.raises(capi.HmnError):
+        dec.ranks[0].ctx.timestep(0.0, 1.0, 1.0)
+    dec.close()
+
+
+def test_distributed_step_on_one_rank_over_nccl():
+    """The torch.distributed driver (NCCL all-reduce of the CFL partials
+    viewed in place, collectives ordered on the slab's stream) on a
+    one-rank group: the same bits as the undecomposed run."""
+    import datetime
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        cfg, prims = cases.blast3d(14, bc=2, mag=True)
+        ref = Simulation(cfg, prims)
+        sim = slab.SlabSimulation(cfg, prims, 0, cfg["n"][2])
+        ex = slab.TorchExchange(dist, 0, 1, periodic=False)
+        sim.connect(False, False)
+        for _ in range(4):
+            ref.step()
+            slab.run_distributed_step(sim, ex)
+            assert sim.dt == ref.dt
+        a, b = ref.state(), sim.state()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        ref.close()
+        sim.close()
+    finally:
+        dist.destroy_process_group()
