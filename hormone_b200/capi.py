@@ -83,6 +83,7 @@ def lib():
         L.hmn_gravity_clock.argtypes = [_P, _DP, _DP]
         L.hmn_checkpoint_begin.argtypes = [_P, _DP, _DPP, _DP, _DP, _DP]
         L.hmn_upload_scalars.argtypes = [_P, _DP]
+        L.hmn_set_dirichlet.argtypes = [_P, _I, _I, _DP]
         L.hmn_download_scalars.argtypes = [_P, _DP]
         L.hmn_checkpoint_wait.argtypes = [_P]
         L.hmn_stream.argtypes = [_P]
@@ -92,7 +93,7 @@ def lib():
         for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
                      "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait",
-                     "hmn_upload_scalars", "hmn_download_scalars"):
+                     "hmn_upload_scalars", "hmn_download_scalars", "hmn_set_dirichlet"):
             getattr(L, name).restype = _I
         _lib = L
     return _lib
@@ -246,6 +247,14 @@ class Context:
         if out is not None and spc is not None:
             out["spc"] = np.ascontiguousarray(np.moveaxis(spc, -1, 0))
         return out
+
+    def set_dirichlet(self, axis: int, side: int, vals: np.ndarray):
+        """Ghost values of a code-9 face: (8 + nspc, 2, n_slow, n_fast) for the
+        planes d, p, v1, v2, v3, b1, b2, b3, scalars."""
+        a = np.ascontiguousarray(vals, dtype=np.float64)
+        self._keep_dir = getattr(self, "_keep_dir", {})
+        self._keep_dir[(axis, side)] = a
+        self._check(lib().hmn_set_dirichlet(self.h, int(axis), int(side), _dp(a)), "hmn_set_dirichlet")
 
     def upload_scalars(self, spc: np.ndarray):
         """spc: (nspc, nz, ny, nx) mass fractions."""

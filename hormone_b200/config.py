@@ -223,7 +223,7 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     for a in range(3):
         if solve[a]:
             for code in bc[a].reshape(-1):
-                if code not in (0, 1, 2, 3):
+                if code not in (0, 1, 2, 3, 4, 5, 9):
                     raise ValueError(f"boundary code {code} on axis {a + 1} is not supported on this path")
     if float(cfg["courant"]) > 1.0:
         raise ValueError("courant number should be <= 1.0")

@@ -51,6 +51,7 @@ struct hmn_ctx {
   TmaMaps tmaps[2];          // tensor maps of pbuf[0], pbuf[1] for TMA staging of 3-D tiles
   int tma_ok;
   double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
+  double* dir[3][2];         // Dirichlet ghost values per face (device)
   double* spcorg;            // passive scalars times density at RK stage 1
   // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
   cudaStream_t cst;
@@ -242,7 +243,7 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     if (!ctx->solve[a]) continue;
     for (int io = 0; io < 2; io++)
       for (int sv = 0; sv < 2; sv++)
-        if (ctx->bc[a][io][sv] < 0 || ctx->bc[a][io][sv] > 3) {
+        if (!((ctx->bc[a][io][sv] >= 0 && ctx->bc[a][io][sv] <= 5) || ctx->bc[a][io][sv] == 9)) {
           delete ctx;
           return HMN_EBADCFG;
         }
@@ -414,6 +415,8 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
   for (int b = 0; b < 2; b++) cudaFree(ctx->pbuf[b]);
   cudaFree(ctx->spcorg);
+  for (int a = 0; a < 3; a++)
+    for (int io = 0; io < 2; io++) cudaFree(ctx->dir[a][io]);
   for (int b = 0; b < 2; b++) {
     cudaFree(ctx->gphi[b]);
     cudaFree(ctx->gpsi[b]);
@@ -531,6 +534,10 @@ static void rk_coeff(int iter, int type, double* faco, double* fact, double* fac
 // step's buffer bookkeeping
 static int enqueue_stage(hmn_ctx* ctx, int s) {
   const int rk = ctx->par.rktype;
+  for (int a = 0; a < 3; a++)
+    for (int io = 0; io < 2; io++)
+      if (ctx->solve[a] && (ctx->bc[a][io][0] == 9 || ctx->bc[a][io][1] == 9) && !ctx->G.dir[a][io])
+        return HMN_EBADCFG;  // code 9 needs hmn_set_dirichlet first
   double* A = ctx->buf[0];
   double* B = ctx->buf[1];
   double* C = ctx->buf[2];
@@ -600,6 +607,22 @@ extern "C" int hmn_hydro_step(hmn_ctx* ctx) {
   if (slab_exchanges(ctx)) return HMN_EBADCFG;  // the halos must be exchanged between stages
   ctx->graph_steps = 0;
   return enqueue_hydro(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// boundary code 9: ghost values given by the host (d0, p0, v10.., b10.., spc0
+// of module physval, boundarycondition.f90:104-115,196-212)
+
+extern "C" int hmn_set_dirichlet(hmn_ctx* ctx, int axis, int side, const double* vals) {
+  if (!ctx || !vals || axis < 0 || axis > 2 || side < 0 || side > 1) return HMN_EINVAL;
+  const int oa0 = axis == 0 ? 1 : 0, oa1 = axis == 2 ? 1 : 2;
+  const size_t m = (size_t)(8 + ctx->par.nspc) * 2 * (size_t)ctx->n[oa0] * ctx->n[oa1];
+  if (!ctx->dir[axis][side]) CK(cudaMalloc((void**)&ctx->dir[axis][side], m * sizeof(double)), "dirichlet");
+  CK(cudaMemcpyAsync(ctx->dir[axis][side], vals, m * sizeof(double), cudaMemcpyHostToDevice, ctx->st),
+     "dirichlet");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  ctx->G.dir[axis][side] = ctx->dir[axis][side];
+  return HMN_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -46,6 +46,11 @@ struct GridDev {
   // (energies rebuilt from the pressure) rather than the interior values
   const double* zhalo[2];
   int zwrap[2];
+  // boundary code 9 (Dirichlet): ghost values of face [axis][inner,outer],
+  // 8 + nspc planes (d, p, v1..3, b1..3, scalars) x 2 layers x face cells
+  // (layer l at coordinate -2+l inner, n+l outer; the other two axes in
+  // increasing order, the lower one fastest)
+  const double* dir[3][2];
 };
 
 // Device-resident scalars of one simulation: the CFL reduction slots, the

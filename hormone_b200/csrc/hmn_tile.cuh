@@ -161,30 +161,91 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
   const int edge = io == 0 ? 0 : n - 1;
   const int bs = G.bc[ax][io][0], bv = G.bc[ax][io][1];
   c3[ax] = bs == 0 ? per : (bs == 1 ? refl : edge);
-  const size_t cs = cidx(G, c3[0], c3[1], c3[2]);  // scalar image (d, p, phi)
+  const size_t cs = cidx(G, c3[0], c3[1], c3[2]);  // scalar image (d, p, phi); the edge cell for 4/5/9
   c3[ax] = bv == 0 ? per : (bv == 1 ? refl : edge);
-  const size_t cv = cidx(G, c3[0], c3[1], c3[2]);  // vector image (v, B)
-  const double dg = P[cs];
-  const double pg = A.gm1 * P[PEINT * pl + cs];  // pressure of the image cell (eos.f90:256)
-  const double phig = GLM ? P[PPHI * pl + cs] * A.phifac : 0.0;
-  double v[3] = {P[PV * pl + cv], P[(PV + 1) * pl + cv], P[(PV + 2) * pl + cv]};
-  double b[3] = {0.0, 0.0, 0.0};
-  if (MAG) {
-    b[0] = P[PB * pl + cv];
-    b[1] = P[(PB + 1) * pl + cv];
-    b[2] = P[(PB + 2) * pl + cv];
+  const size_t cv = cidx(G, c3[0], c3[1], c3[2]);  // vector image (v, B); the edge cell for 4/5/9
+  c3[ax] = io == 0 ? 1 : n - 2;
+  const size_t cin = cidx(G, c3[0], c3[1], c3[2]);  // the cell next to the edge cell, inward
+  // linear extrapolation from the edge cell (codes 4/5, boundarycondition.f90:302-327,419-468,963-985):
+  // both ghosts of the face, the near one from the interior and the far one from the near one
+  const bool far = io == 0 ? gl == 0 : gl == 1;
+  const double* dxa = G.g[ax].dx + 2;
+  auto linear = [&](double f0, double f1, double& g0, double& g1) {
+    if (io == 1) {
+      g0 = f0 + (f0 - f1) * dxa[n - 1] / dxa[n - 2];
+      g1 = g0 + (g0 - f0) * dxa[n] / dxa[n - 1];
+    } else {
+      g0 = f0 - (f1 - f0) * dxa[0] / dxa[1];
+      g1 = g0 - (f0 - g0) * dxa[-1] / dxa[0];
+    }
+  };
+  // Dirichlet values of this ghost (code 9): 8 + nspc planes x 2 layers x face cells
+  const double* D = G.dir[ax][io];
+  const int oa0 = ax == 0 ? 1 : 0, oa1 = ax == 2 ? 1 : 2;
+  const size_t area = (size_t)G.n[oa0] * G.n[oa1];
+  const size_t hd = (size_t)gl * area + (size_t)c3[oa0] + (size_t)G.n[oa0] * c3[oa1];
+  double dg, pg, phig;
+  if (bs == 4 || bs == 5) {
+    double g0, g1;
+    linear(P[cs], P[cin], g0, g1);
+    if (g1 <= 0.0) g0 = g1 = P[cs];
+    dg = far ? g1 : g0;
+    linear(A.gm1 * P[PEINT * pl + cs], A.gm1 * P[PEINT * pl + cin], g0, g1);
+    if (g1 <= 0.0) g0 = g1 = A.gm1 * P[PEINT * pl + cs];
+    pg = far ? g1 : g0;
+    phig = GLM ? P[PPHI * pl + cs] * A.phifac : 0.0;
+  } else if (bs == 9) {
+    dg = D[hd];
+    pg = D[2 * area + hd];
+    phig = 0.0;
+  } else {
+    dg = P[cs];
+    pg = A.gm1 * P[PEINT * pl + cs];  // pressure of the image cell (eos.f90:256)
+    phig = GLM ? P[PPHI * pl + cs] * A.phifac : 0.0;
   }
-  double vn = v[ax];
-  if (bv == 1) {
-    vn = -vn;
-    b[ax] = -b[ax];
-  } else if (bv == 2) {
-    if (io == 0)
-      vn = ax == 0 ? fmin2(0.0, vn) : vn * (0.5 - fsign(0.5, vn));  // :165 and the y/z plug form
-    else
-      vn = vn * (0.5 + fsign(0.5, vn));
+  double v[3], b[3] = {0.0, 0.0, 0.0};
+  if (bv == 4 || bv == 5) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double g0, g1;
+      linear(P[(PV + c) * pl + cv], P[(PV + c) * pl + cin], g0, g1);
+      v[c] = far ? g1 : g0;
+      if (MAG) {
+        linear(P[(PB + c) * pl + cv], P[(PB + c) * pl + cin], g0, g1);
+        b[c] = far ? g1 : g0;
+      }
+    }
+    if (bv == 5) {  // linear + outgoing: the normal velocity only flows out
+      const double vedge = P[(PV + ax) * pl + cv];
+      v[ax] = v[ax] * (io == 1 ? 0.5 + fsign(0.5, vedge) : 0.5 - fsign(0.5, vedge));
+    }
+  } else if (bv == 9) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      v[c] = D[(size_t)(2 + c) * 2 * area + hd];
+      if (MAG) b[c] = D[(size_t)(5 + c) * 2 * area + hd];
+    }
+  } else {
+    v[0] = P[PV * pl + cv];
+    v[1] = P[(PV + 1) * pl + cv];
+    v[2] = P[(PV + 2) * pl + cv];
+    if (MAG) {
+      b[0] = P[PB * pl + cv];
+      b[1] = P[(PB + 1) * pl + cv];
+      b[2] = P[(PB + 2) * pl + cv];
+    }
+    double vn = v[ax];
+    if (bv == 1) {
+      vn = -vn;
+      b[ax] = -b[ax];
+    } else if (bv == 2) {
+      if (io == 0)
+        vn = ax == 0 ? fmin2(0.0, vn) : vn * (0.5 - fsign(0.5, vn));  // :165 and the y/z plug form
+      else
+        vn = vn * (0.5 + fsign(0.5, vn));
+    }
+    v[ax] = vn;
   }
-  v[ax] = vn;
   const double eg = pg / A.gm1;  // eos.f90:287-289
   const double b1 = b[0], b2 = b[1], b3 = b[2];
   q[Q_D] = dg;
@@ -217,6 +278,32 @@ __device__ __forceinline__ size_t scalar_image(const GridDev& G, int i, int j, i
     c3[a] = bs == 0 ? per : (bs == 1 ? refl : edge);
   }
   return cidx(G, c3[0], c3[1], c3[2]);
+}
+
+// The Dirichlet values of a ghost cell's face (scalar code 9), or nullptr;
+// with the cell's index in that face's 2 x n1 x n2 layout and the face area.
+__device__ __forceinline__ int out_axis(const GridDev& G, int i, int j, int k) {
+  return (i < 0 || i >= G.n[0]) ? 0 : ((j < 0 || j >= G.n[1]) ? 1 : ((k < 0 || k >= G.n[2]) ? 2 : -1));
+}
+__device__ __forceinline__ const double* dirichlet_face(const GridDev& G, int i, int j, int k) {
+  const int ax = out_axis(G, i, j, k);
+  if (ax < 0) return nullptr;
+  const int c3[3] = {i, j, k};
+  const int io = c3[ax] < 0 ? 0 : 1;
+  return G.bc[ax][io][0] == 9 ? G.dir[ax][io] : nullptr;
+}
+__device__ __forceinline__ size_t dirichlet_area(const GridDev& G, int i, int j, int k) {
+  const int ax = out_axis(G, i, j, k);
+  const int oa0 = ax == 0 ? 1 : 0, oa1 = ax == 2 ? 1 : 2;
+  return (size_t)G.n[oa0] * G.n[oa1];
+}
+__device__ __forceinline__ size_t dirichlet_index(const GridDev& G, int i, int j, int k) {
+  const int ax = out_axis(G, i, j, k);
+  const int c3[3] = {i, j, k};
+  const int oa0 = ax == 0 ? 1 : 0, oa1 = ax == 2 ? 1 : 2;
+  const int s = c3[ax], n = G.n[ax];
+  const int gl = s < 0 ? s + 2 : s - n;
+  return (size_t)gl * G.n[oa0] * G.n[oa1] + (size_t)c3[oa0] + (size_t)G.n[oa0] * c3[oa1];
 }
 
 // Stage the tile's cross-shaped stencil region (tile origin t0, real extent
@@ -295,6 +382,10 @@ __device__ __forceinline__ void stage_region(const GridDev& G, const StageArgs& 
         const size_t hp = (size_t)G.n[0] * G.n[1];
         const size_t h = (size_t)(zio == 0 ? gk + 2 : gk - G.n[2]) * hp + (size_t)gi + (size_t)G.n[0] * gj;
         for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = G.zhalo[zio][(size_t)(NP + n) * 2 * hp + h];
+      } else if (const double* D = dirichlet_face(G, gi, gj, gk)) {
+        const size_t hd = dirichlet_index(G, gi, gj, gk);
+        const size_t two_area = 2 * dirichlet_area(G, gi, gj, gk);
+        for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = D[(size_t)(8 + n) * two_area + hd];
       } else {
         const size_t cs = scalar_image(G, gi, gj, gk);
         for (int n = 0; n < A.nspc; n++) P[NQ + n][w] = A.pin[(size_t)(NP + n) * A.plane + cs];

@@ -42,7 +42,8 @@ typedef struct hmn_ctx hmn_ctx;
 typedef struct {
   int n[3];           /* ie-is+1, je-js+1, ke-ks+1 */
   int ghost;          /* ghost layers of the caller's 3-D arrays (0 or 2) */
-  int bc[3][2][2];    /* boundary codes [axis][inner,outer][scalar,vector], after checksetup.f90:109-128 */
+  int bc[3][2][2];    /* boundary codes [axis][inner,outer][scalar,vector], after checksetup.f90:109-128:
+                       0 periodic, 1 reflective, 2 outgoing, 3 free, 4/5 linear, 9 Dirichlet */
   const double* x[3];
   const double* xi[3];
   const double* dx[3];
@@ -100,6 +101,17 @@ int hmn_phidamp(hmn_ctx* ctx);
  * rungekutta.f90:205-229 and phidamp leave them, and the potential.  NULL
  * pointers are skipped. */
 int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi, double* grvpsi);
+
+/* Boundary code 9 (Dirichlet, boundarycondition.f90:104-115,196-212): the
+ * ghost values of face (axis 0-2, side 0 inner / 1 outer), i.e. the d0, p0,
+ * v10, v20, v30, b10, b20, b30 (and spc0) of module physval there: 8 + nspc
+ * planes, each 2 layers x the face's cells (layer l is the ghost at
+ * coordinate -2+l on the inner side, n+l on the outer side; the other two
+ * axes in increasing order, the lower one fastest).  Call again whenever
+ * the values change.  Codes 4 and 5 (linear extrapolation, and linear with
+ * outflow-only normal velocity) need no data; code 10 (the wind-tunnel flux
+ * boundary, fluxboundary.f90) is not on this path. */
+int hmn_set_dirichlet(hmn_ctx* ctx, int axis, int side, const double* vals);
 
 /* Passive scalars (compswitch 2: module physval's spc(1:spn,i,j,k), species
  * fastest, then i, j, k with the grid's ghost layers): upload the mass

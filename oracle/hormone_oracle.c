@@ -24,7 +24,9 @@
  *   EOS (ideal)     src/main/eos.f90:195-274,351-365,742-866
  *   source          src/main/source.f90:14-85,177-228
  *   RK + primitive  src/main/rungekutta.f90:16-232
- *   boundaries      src/main/boundarycondition.f90:14-1442 (codes 0-3)
+ *   boundaries      src/main/boundarycondition.f90:14-1442 (codes 0-3; 4/5
+ *                   linear extrapolation as :302-327,419-468; 9 Dirichlet
+ *                   as :104-115,196-212 from per-face ghost values)
  *   timestep        src/main/timestep.f90:15-183
  *   phidamp         src/main/source.f90:239-260
  *   hyperbolic grav src/main/gravity_hyperbolic.f90:19-125,230-280 with a
@@ -76,6 +78,9 @@ typedef struct {
   /* passive scalars (compswitch 2): mass fractions, ghosted */
   int spn;
   double *spc[MAXSPC], *spcorg[MAXSPC], *dspc[3][MAXSPC], *spcflx[3][MAXSPC];
+  /* Dirichlet ghost values per face: 8 + spn planes (d, p, v1..3, b1..3,
+     spc) x 2 layers x face cells, layer l at coordinate -2+l (inner) or n+l */
+  double *dir[3][2];
   /* scalars */
   double dt, ch, time, t_out, t_end, dt_out, cfmax;
   double cgrav, cgrav_old, dtgrav, dtg_unit, grvtime;
@@ -151,6 +156,7 @@ void hmo_destroy(Oracle *o) {
     for (int a = 0; a < 3; a++) free(o->flux[a][q]);
   }
   free(o->grvphi); free(o->grvpsi); free(o->gorg1); free(o->gorg2); free(o->lapphi); free(o->hgsrc); free(o->gsrc);
+  for (int a = 0; a < 3; a++) { free(o->dir[a][0]); free(o->dir[a][1]); }
   for (int n = 0; n < o->spn; n++) {
     free(o->spc[n]); free(o->spcorg[n]);
     for (int a = 0; a < 3; a++) { free(o->dspc[a][n]); free(o->spcflx[a][n]); }
@@ -166,6 +172,16 @@ int hmo_set_species(Oracle *o, int spn) {
     o->spc[n] = zalloc(o->ncell); o->spcorg[n] = zalloc(o->ncell);
     for (int a = 0; a < 3; a++) { o->dspc[a][n] = zalloc(o->ncell); o->spcflx[a][n] = zalloc(o->ncell); }
   }
+  return HMO_OK;
+}
+
+/* Dirichlet ghost values of face (a, io): 8 + spn planes of 2 x n1 x n2 */
+int hmo_set_dirichlet(Oracle *o, int a, int io, const double *vals) {
+  int oa[2], q = 0;
+  for (int b = 0; b < 3; b++) if (b != a) oa[q++] = b;
+  size_t m = (size_t)(8 + o->spn) * 2 * o->n[oa[0]] * o->n[oa[1]];
+  if (!o->dir[a][io]) o->dir[a][io] = zalloc(m);
+  memcpy(o->dir[a][io], vals, m * sizeof(double));
   return HMO_OK;
 }
 
@@ -314,57 +330,128 @@ static void ghost_energy(Oracle *o, size_t g) {
   o->e[g] = o->eint[g] + 0.5 * (o->d[g] * (v1 * v1 + v2 * v2 + v3 * v3) + b1 * b1 + b2 * b2 + b3 * b3);
 }
 
+/* linear extrapolation into the two ghosts beyond the edge cell (code 4/5):
+   outer  q(n)   = q(n-1) + (q(n-1)-q(n-2))*dx(n-1)/dx(n-2),
+          q(n+1) = q(n)   + (q(n)-q(n-1))*dx(n)/dx(n-1)        (:302-327)
+   inner  q(-1)  = q(0)   - (q(1)-q(0))*dx(0)/dx(1),
+          q(-2)  = q(-1)  - (q(0)-q(-1))*dx(-1)/dx(0)           (:963-985) */
+static void linear_ghosts(const Oracle *o, int a, int io, const double *f, size_t e0, size_t e1, double *g0,
+                          double *g1) {
+  /* e0: edge cell, e1: the next one inward; g0: near ghost, g1: far ghost */
+  const double *DX = o->dx[a] + 2;
+  int n = o->n[a];
+  if (io == 1) {
+    *g0 = f[e0] + (f[e0] - f[e1]) * DX[n - 1] / DX[n - 2];
+    *g1 = *g0 + (*g0 - f[e0]) * DX[n] / DX[n - 1];
+  } else {
+    *g0 = f[e0] - (f[e1] - f[e0]) * DX[0] / DX[1];
+    *g1 = *g0 - (f[e0] - *g0) * DX[-1] / DX[0];
+  }
+}
+
 static void bc_axis(Oracle *o, int a) {
   int n = o->n[a];
   int oa[2], q = 0;
   for (int b = 0; b < 3; b++) if (b != a) oa[q++] = b;
   int n1 = o->n[oa[0]], n2 = o->n[oa[1]];
+  size_t area = (size_t)n1 * n2;
   for (int io = 0; io < 2; io++) {
     int bs = o->bc[a][io][0], bv = o->bc[a][io][1];
     for (int t2 = 0; t2 < n2; t2++)
       for (int t1 = 0; t1 < n1; t1++) {
+        int edge = io == 0 ? 0 : n - 1;
+        size_t ce0 = IXa(o, a, edge, t1, t2), ce1 = IXa(o, a, io == 0 ? 1 : n - 2, t1, t2);
+        size_t cnear = IXa(o, a, io == 0 ? -1 : n, t1, t2), cfar = IXa(o, a, io == 0 ? -2 : n + 1, t1, t2);
+        size_t fidx = (size_t)t1 + (size_t)n1 * t2;
+        if (bs == 4 || bs == 5) {
+          double g0, g1;
+          linear_ghosts(o, a, io, o->d, ce0, ce1, &g0, &g1);
+          if (g1 <= 0.0) g0 = g1 = o->d[ce0];
+          o->d[cnear] = g0; o->d[cfar] = g1;
+          linear_ghosts(o, a, io, o->p, ce0, ce1, &g0, &g1);
+          if (g1 <= 0.0) g0 = g1 = o->p[ce0];
+          o->p[cnear] = g0; o->p[cfar] = g1;
+          if (o->mag_on) { o->phi[cnear] = o->phi[ce0]; o->phi[cfar] = o->phi[ce0]; }
+          for (int ns = 0; ns < o->spn; ns++) { o->spc[ns][cnear] = o->spc[ns][ce0]; o->spc[ns][cfar] = o->spc[ns][ce0]; }
+        }
+        if (bv == 4 || bv == 5) {
+          for (int c = 0; c < 3; c++) {
+            double g0, g1;
+            linear_ghosts(o, a, io, o->v[c], ce0, ce1, &g0, &g1);
+            if (bv == 5 && c == a) {
+              /* linear + outgoing: the normal velocity only flows out (:441-468) */
+              double plug = io == 1 ? 0.5 + fsign(0.5, o->v[a][ce0]) : 0.5 - fsign(0.5, o->v[a][ce0]);
+              g0 = g0 * plug; g1 = g1 * plug;
+            }
+            o->v[c][cnear] = g0; o->v[c][cfar] = g1;
+            if (o->mag_on) {
+              linear_ghosts(o, a, io, o->b[c], ce0, ce1, &g0, &g1);
+              o->b[c][cnear] = g0; o->b[c][cfar] = g1;
+            }
+          }
+        }
         for (int gl = 0; gl < 2; gl++) {
           /* ghost coordinate and its source cells */
           int g = io == 0 ? -2 + gl : n + gl;       /* is-2,is-1 | ie+1,ie+2 */
-          int edge = io == 0 ? 0 : n - 1;
           int per = io == 0 ? n - 2 + gl : gl;       /* periodic image */
           int refl = io == 0 ? 1 - gl : n - 1 - gl;  /* reflective image: is+1,is | ie,ie-1 */
           size_t cg = IXa(o, a, g, t1, t2);
-          int ss;
+          const double *D = o->dir[a][io];
+          size_t h = (size_t)gl * area + fidx;
+          int ss = -1;
           switch (bs) {
             case 0: ss = per; break;
             case 1: ss = refl; break;
             case 2: case 3: ss = edge; break;
+            case 4: case 5: break;
+            case 9:
+              if (!D) { set_err(o, HMO_EBADCFG, a, io, 0); return; }
+              o->d[cg] = D[0 * 2 * area + h]; o->p[cg] = D[1 * 2 * area + h];
+              if (o->mag_on) o->phi[cg] = 0.0;
+              for (int ns = 0; ns < o->spn; ns++) o->spc[ns][cg] = D[(size_t)(8 + ns) * 2 * area + h];
+              break;
             default: set_err(o, HMO_EBADCFG, a, io, 0); return;
           }
-          size_t cs_ = IXa(o, a, ss, t1, t2);
-          o->d[cg] = o->d[cs_]; o->p[cg] = o->p[cs_];
-          for (int ns = 0; ns < o->spn; ns++) o->spc[ns][cg] = o->spc[ns][cs_];
-          if (o->mag_on) o->phi[cg] = o->phi[cs_];
-          int sv;
+          if (ss >= 0) {
+            size_t cs_ = IXa(o, a, ss, t1, t2);
+            o->d[cg] = o->d[cs_]; o->p[cg] = o->p[cs_];
+            for (int ns = 0; ns < o->spn; ns++) o->spc[ns][cg] = o->spc[ns][cs_];
+            if (o->mag_on) o->phi[cg] = o->phi[cs_];
+          }
+          int sv = -1;
           switch (bv) {
             case 0: sv = per; break;
             case 1: sv = refl; break;
             case 2: case 3: sv = edge; break;
+            case 4: case 5: break;
+            case 9:
+              if (!D) { set_err(o, HMO_EBADCFG, a, io, 1); return; }
+              for (int c = 0; c < 3; c++) {
+                o->v[c][cg] = D[(size_t)(2 + c) * 2 * area + h];
+                if (o->mag_on) o->b[c][cg] = D[(size_t)(5 + c) * 2 * area + h];
+              }
+              break;
             default: set_err(o, HMO_EBADCFG, a, io, 1); return;
           }
-          size_t cv = IXa(o, a, sv, t1, t2);
-          for (int c = 0; c < 3; c++) {
-            double vv = o->v[c][cv];
-            if (c == a && bv == 1) vv = -vv;
-            if (c == a && bv == 2) {
-              if (io == 0) {
-                if (a == 0) vv = fmin2(0.0, vv);                 /* :165 */
-                else vv = vv * (0.5 - fsign(0.5, vv));           /* y/z inner plug */
-              } else {
-                vv = vv * (0.5 + fsign(0.5, vv));                /* :388-390 */
+          if (sv >= 0) {
+            size_t cv = IXa(o, a, sv, t1, t2);
+            for (int c = 0; c < 3; c++) {
+              double vv = o->v[c][cv];
+              if (c == a && bv == 1) vv = -vv;
+              if (c == a && bv == 2) {
+                if (io == 0) {
+                  if (a == 0) vv = fmin2(0.0, vv);                 /* :165 */
+                  else vv = vv * (0.5 - fsign(0.5, vv));           /* y/z inner plug */
+                } else {
+                  vv = vv * (0.5 + fsign(0.5, vv));                /* :388-390 */
+                }
               }
-            }
-            o->v[c][cg] = vv;
-            if (o->mag_on) {
-              double bb = o->b[c][cv];
-              if (c == a && bv == 1) bb = -bb;
-              o->b[c][cg] = bb;
+              o->v[c][cg] = vv;
+              if (o->mag_on) {
+                double bb = o->b[c][cv];
+                if (c == a && bv == 1) bb = -bb;
+                o->b[c][cg] = bb;
+              }
             }
           }
         }

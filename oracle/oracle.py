@@ -55,6 +55,8 @@ def lib():
         L.hmo_set_species.argtypes = [_P, _I]
         L.hmo_set_species.restype = _I
         L.hmo_set_spc.argtypes = [_P, _I, _DP]
+        L.hmo_set_dirichlet.argtypes = [_P, _I, _I, _DP]
+        L.hmo_set_dirichlet.restype = _I
         L.hmo_gravity_setup.argtypes = [_P, _D]
         L.hmo_start.argtypes = [_P]
         L.hmo_start.restype = _I
@@ -137,6 +139,13 @@ class Oracle:
             for n in range(self.nspc):
                 lib().hmo_set_spc(self.h, n, _dp(spc[n].reshape(-1)))
         lib().hmo_set_prims(self.h, *[_dp(f[k]) for k in ["d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi"]])
+
+    def set_dirichlet(self, axis: int, side: int, vals):
+        """Ghost values of a code-9 face, laid out as for hmn_set_dirichlet."""
+        a = np.ascontiguousarray(vals, dtype=np.float64)
+        self._keep_dir = getattr(self, "_keep_dir", {})
+        self._keep_dir[(axis, side)] = a
+        lib().hmo_set_dirichlet(self.h, int(axis), int(side), _dp(a.reshape(-1)))
 
     def set_gravity_state(self, grvphi, grvpsi=None, cgrav_old=0.0):
         a = np.ascontiguousarray(grvphi, dtype=np.float64).reshape(-1)

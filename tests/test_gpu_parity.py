@@ -33,13 +33,17 @@ def compare(o, s, where):
         assert np.array_equal(st["spc"][n], o.get(f"spc{n}")), f"{where}: scalar {n} differs"
 
 
-def run_pair(cfg, prims, nsteps, grvphi=None, cgrav_old=0.0, check_every=1):
+def run_pair(cfg, prims, nsteps, grvphi=None, cgrav_old=0.0, check_every=1, dirichlet=None):
     o = Oracle(cfg)
+    for (axis, side), vals in (dirichlet or {}).items():
+        o.set_dirichlet(axis, side, vals)
     o.set_prims(prims)
     if grvphi is not None:
         o.set_gravity_state(grvphi, None, cgrav_old)
     o.start()
     s = Simulation(cfg, prims, grvphi=grvphi, cgrav_old=cgrav_old)
+    for (axis, side), vals in (dirichlet or {}).items():
+        s.ctx.set_dirichlet(axis, side, vals)
     compare(o, s, "initial state")
     assert s.dt == o.scalars()["dt"] and s.ch == o.scalars()["ch"]
     for n in range(nsteps):
@@ -138,3 +142,41 @@ def test_passive_scalars(make):
     reflective, free and periodic boundaries, MHD and hydro."""
     cfg, prims = make()
     run_pair(cfg, prims, 6)
+
+
+def _edge_dirichlet(cfg, prims, axis, side, scale=1.0):
+    """Ghost values of a code-9 face: the edge cells' state, density and
+    pressure times `scale`, on both ghost layers."""
+    p = {k: np.asarray(v) for k, v in prims.items()}
+    idx = [slice(None)] * 3
+    idx[2 - axis] = 0 if side == 0 else -1
+    planes = [p["d"][tuple(idx)] * scale, p["p"][tuple(idx)] * scale] + \
+             [p[k][tuple(idx)] for k in ("v1", "v2", "v3", "b1", "b2", "b3")]
+    if cfg.get("nspc", 0):
+        planes += [p["spc"][n][tuple(idx)] for n in range(cfg["nspc"])]
+    return np.ascontiguousarray(np.stack([np.stack([pl, pl]) for pl in planes]))
+
+
+@pytest.mark.parametrize("nspc", [0, 2])
+def test_linear_and_dirichlet_boundaries(nspc):
+    """Codes 4 and 5 (linear extrapolation; with outflow-only normal
+    velocity) and 9 (Dirichlet ghost values from the host) on every axis,
+    against the oracle, with and without passive scalars."""
+    from hormone_b200 import config, grid as G, ic
+
+    ov = dict(ie=12, je=10, ke=8, mag_on=True, gamma=1.4, t_end=0.1, dt_out=0.1, courant=0.6,
+              bc1is=3, bc1iv=3, bc1os=4, bc1ov=4, bc2is=5, bc2iv=5, bc2os=9, bc2ov=9,
+              bc3is=4, bc3iv=5, bc3os=9, bc3ov=4)
+    if nspc:
+        ov.update(compswitch=2, spn=nspc)
+    cfg = config.resolve("riemann", overrides=ov)
+    rng = np.random.default_rng(5)
+    st = [dict(d=10 ** rng.uniform(-0.5, 0.3), p=10 ** rng.uniform(-0.5, 0.3), v1=rng.uniform(-0.5, 0.5),
+               v2=rng.uniform(-0.5, 0.5), v3=rng.uniform(-0.5, 0.5), b1=0.3, b2=rng.uniform(-0.5, 0.5),
+               b3=rng.uniform(-0.5, 0.5)) for _ in range(2)]
+    prims = ic.riemann(cfg, 0, st[0], st[1])
+    prims["d"] *= 1.0 + 0.1 * np.sin(np.arange(10))[None, :, None] * np.cos(np.arange(8))[:, None, None]
+    if nspc:
+        prims = cases.add_scalars(cfg, prims)
+    dirichlet = {(1, 1): _edge_dirichlet(cfg, prims, 1, 1, 1.05), (2, 1): _edge_dirichlet(cfg, prims, 2, 1, 0.95)}
+    run_pair(cfg, prims, 8, dirichlet=dirichlet)
