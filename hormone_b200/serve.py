@@ -98,10 +98,12 @@ class ServeStats:
     latencies: List[float] = field(default_factory=list)
     max_live: int = 0
     batch_steps: int = 0
+    failures: List[tuple] = field(default_factory=list)  # (request id, kind, cells, error code, steps)
 
     def summary(self) -> dict:
         lat = np.array(self.latencies) if self.latencies else np.zeros(1)
-        return {"completed": self.completed, "failed": self.failed, "wall_s": self.wall_s,
+        return {"completed": self.completed, "failed": self.failed, "failures": self.failures[:20],
+                "wall_s": self.wall_s,
                 "zone_updates_per_s": self.zone_updates / max(self.wall_s, 1e-12),
                 "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                 "max_concurrent": self.max_live, "batch_steps": self.batch_steps}
@@ -131,6 +133,7 @@ def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], fl
                 r.error = -5
                 r.t_done = clock() - t0
                 stats.failed += 1
+                stats.failures.append((r.rid, r.kind, r.cells, r.error, 0))
                 continue
             slot = batch.add(r.cfg, r.prims)
             if slot is None:
@@ -158,6 +161,7 @@ def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], fl
             batch.remove(slot)
             if r.error:
                 stats.failed += 1
+                stats.failures.append((r.rid, r.kind, r.cells, r.error, r.steps))
             else:
                 stats.completed += 1
                 stats.latencies.append(r.latency)
