@@ -99,7 +99,7 @@ def parse_namelists(text: str) -> Dict[str, Dict[str, Any]]:
 
 BASE: Dict[str, Any] = dict(
     xi1s=0.0, xi1e=1.0, xi2s=0.0, xi2e=1.0, xi3s=0.0, xi3e=1.0,
-    is_=1, ie=10, js=1, je=1, ks=1, ke=1, imesh=0, jmesh=0, kmesh=0,
+    is_=1, ie=10, js=1, je=1, ks=1, ke=1, imesh=0, jmesh=0, kmesh=0, x1min=0.0, x2min=0.0, x3min=0.0,
     outstyle=1, endstyle=1, tnlim=0, t_end=0.0, dt_out=1.0, tn_out=1, dt_unit="s",
     eostype=0, compswitch=0, muconst=0.62, spn=0, gamma=1.6666666666666667,
     crdnt=0, courant=0.9, rktype=3, mag_on=False, flux_limiter="modified_mc", alpha9wave=0.1,

@@ -211,12 +211,12 @@ void hmo_set_gravity(Oracle *o, int gravswitch, double HGfac, double hgcfl, doub
 /* gridset.f90:46-80 for a uniform Cartesian axis; with gravity the spacing
    arrays are reset to dxi and the two ghost layers are re-accumulated
    (gridset.f90:71-81). */
-void hmo_make_uniform_axis(Oracle *o, int a, double xis, double xie) {
+/* gridset.f90:46-81 from the cell widths dxi(is-2:ie+2) of any Cartesian mesh */
+void hmo_make_axis(Oracle *o, int a, double xis, const double *widths) {
   int n = o->n[a];
   double *x = o->x[a], *xi = o->xi[a], *dx = o->dx[a], *dxi = o->dxi[a], *idx = o->idx[a], *idxi = o->idxi[a];
 #define G2(arr, i) arr[(i) + 2]
-  double h = (xie - xis) / (double)n;
-  for (int i = -2; i <= n + 1; i++) G2(dxi, i) = h;
+  for (int i = -2; i <= n + 1; i++) G2(dxi, i) = widths[i + 2];
   for (int i = -1; i <= n + 1; i++) {
     G2(dx, i) = 0.5 * (G2(dxi, i - 1) + G2(dxi, i));
     G2(idxi, i) = 1.0 / G2(dxi, i);
@@ -246,6 +246,44 @@ void hmo_make_uniform_axis(Oracle *o, int a, double xis, double xie) {
     }
   }
 #undef G2
+}
+
+/* geometrical-series mesh (imesh=1): utils.f90:351-404 */
+int hmo_make_geometric_axis(Oracle *o, int a, double xis, double xie, double xmin) {
+  int n = o->n[a];
+  const double xrmax = 1.05, maxerr = 1e-10;
+  double xr = 1.01, xrng = xie - xis, irng = (double)n;
+  if (xrng / irng < xmin) return HMO_EBADCFG;
+  for (long it = 0; it < 10000000; it++) {
+    double fx = (xr - 1.0) * xrng - xmin * (pow(xr, irng) - 1.0);
+    double dfx = xrng - irng * xmin * pow(xr, irng - 1.0);
+    double xrnew = xr - fx / dfx;
+    if (fabs((xrnew - xr) / xr) < maxerr) { xr = xrnew; break; }
+    if (xrnew < 1.0) xrnew = 2.0;
+    xr = xrnew;
+  }
+  if (xr > xrmax) return HMO_EBADCFG;
+  double *w = zalloc((size_t)n + 4);
+  w[2] = xmin;
+  for (int i = 1; i < n; i++) w[i + 2] = w[i + 1] * xr;
+  w[1] = w[2];
+  w[0] = w[3];
+  w[n + 2] = w[n + 1] * xr;
+  w[n + 3] = w[n + 1] * xr * xr;
+  if (xr - 1.0 < maxerr)
+    for (int i = 0; i < n + 4; i++) w[i] = xrng / irng;
+  hmo_make_axis(o, a, xis, w);
+  free(w);
+  return HMO_OK;
+}
+
+void hmo_make_uniform_axis(Oracle *o, int a, double xis, double xie) {
+  int n = o->n[a];
+  double h = (xie - xis) / (double)n;
+  double *w = zalloc((size_t)n + 4);
+  for (int i = 0; i < n + 4; i++) w[i] = h;
+  hmo_make_axis(o, a, xis, w);
+  free(w);
 }
 
 void hmo_get_axis(Oracle *o, int a, double *x, double *xi, double *dx, double *dxi, double *idx, double *idxi) {

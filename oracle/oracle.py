@@ -49,6 +49,9 @@ def lib():
         L.hmo_set_test_mode.argtypes = [_P]
         L.hmo_set_gravity.argtypes = [_P, _I, _D, _D, _D, _D, _I, _I]
         L.hmo_make_uniform_axis.argtypes = [_P, _I, _D, _D]
+        L.hmo_make_axis.argtypes = [_P, _I, _D, _DP]
+        L.hmo_make_geometric_axis.argtypes = [_P, _I, _D, _D, _D]
+        L.hmo_make_geometric_axis.restype = _I
         L.hmo_get_axis.argtypes = [_P, _I] + [_DP] * 6
         L.hmo_set_prims.argtypes = [_P] + [_DP] * 9
         L.hmo_set_grvphi.argtypes = [_P, _DP, _DP]
@@ -106,8 +109,14 @@ class Oracle:
         if cfg.get("gravswitch", 0):
             L.hmo_set_gravity(self.h, int(cfg["gravswitch"]), float(cfg["HGfac"]), float(cfg["hgcfl"]),
                               float(cfg["alphagrv"]), float(cfg["G"]), int(cfg["grktype"]), int(cfg["maxtngrv"]))
+        mesh_keys = ("imesh", "jmesh", "kmesh")
         for a, (lo, hi) in enumerate(cfg["extent"]):
-            L.hmo_make_uniform_axis(self.h, a, float(lo), float(hi))
+            if cfg["n"][a] > 1 and int(cfg.get(mesh_keys[a], 0)) == 1:
+                xmin = float(cfg[("x1min", "x2min", "x3min")[a]])
+                if L.hmo_make_geometric_axis(self.h, a, float(lo), float(hi), xmin) != 0:
+                    raise ValueError("geometrical series mesh: bad xmin")
+            else:
+                L.hmo_make_uniform_axis(self.h, a, float(lo), float(hi))
         L.hmo_set_times(self.h, 0.0, float(cfg["t_end"]), float(cfg["dt_out"]), int(cfg["outstyle"]),
                         int(cfg["endstyle"]), int(cfg["tnlim"]))
         if cfg.get("is_test", False):

@@ -79,3 +79,25 @@ def test_golden_fixture_format_matches_reference_dump():
     data = binio.readbin(ref, cfg["n"], cfg["mag_on"])
     again = binio.writebin(None, data["tn"], data["time"], data, mag_on=True)
     assert again == open(ref, "rb").read()
+
+
+def test_geometric_mesh_matches_the_oracle_restatement():
+    """imesh=1 (utils.f90:351-404): the host grid and the oracle's C
+    restatement build the same arrays, and the widths grow by one ratio."""
+    import numpy as np
+
+    from hormone_b200 import config, grid as G
+    from oracle.oracle import Oracle
+
+    cfg = config.resolve("riemann", overrides=dict(ie=40, je=24, ke=1, imesh=1, x1min=0.01, jmesh=1, x2min=0.03,
+                                                    xi1s=0.0, xi1e=1.0, xi2s=-0.5, xi2e=0.5))
+    grid = G.make_grid(cfg)
+    o = Oracle(cfg)
+    for a in range(2):
+        ax = o.axis(a)
+        for k in G.AXIS_KEYS:
+            assert np.array_equal(ax[k], grid[a][k]), (a, k)
+    w = grid[0]["dxi"][2:-2]
+    r = w[1:] / w[:-1]
+    assert w[0] == 0.01 and np.allclose(r, r[0]) and r[0] > 1.0
+    assert abs(grid[0]["xi"][-3] - 1.0) < 1e-9  # the last face lands on xi1e

@@ -180,3 +180,16 @@ def test_linear_and_dirichlet_boundaries(nspc):
         prims = cases.add_scalars(cfg, prims)
     dirichlet = {(1, 1): _edge_dirichlet(cfg, prims, 1, 1, 1.05), (2, 1): _edge_dirichlet(cfg, prims, 2, 1, 0.95)}
     run_pair(cfg, prims, 8, dirichlet=dirichlet)
+
+
+def test_geometric_series_mesh():
+    """Stretched cells on two axes (imesh=jmesh=1): the modified-MC factors,
+    face offsets and divergence widths that vary per cell."""
+    from hormone_b200 import config, grid as G, ic
+
+    cfg = config.resolve("kh", overrides=dict(ie=40, je=32, ke=1, mag_on=True, gamma=1.6666666666666667,
+                                              imesh=1, x1min=0.015, jmesh=1, x2min=0.02, t_end=2.0, dt_out=2.0,
+                                              xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5,
+                                              bc2is=3, bc2os=3, bc2iv=3, bc2ov=3))
+    prims = ic.kelvin_helmholtz(cfg, G.make_grid(cfg), 2.0, 0.05)
+    run_pair(cfg, prims, 10)
