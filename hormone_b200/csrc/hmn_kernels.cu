@@ -638,30 +638,30 @@ cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool gl
                          cudaStream_t st) {
   const int* t = A.tile;
   if (A.nspc > 0) {  // tiles with room for up to 4 passive scalars
-    using S3 = Tile<8, 8, 4, 256, 2, 4>;
+    using S3 = Tile<8, 8, 4, 384, 2, 4>;
     if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<S3>(G, A, mag, glm, nullptr, st);
     if (t[0] == 16 && t[1] == 16 && t[2] == 1)
-      return launch_stage_tl<Tile<16, 16, 1, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+      return launch_stage_tl<Tile<16, 16, 1, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
     if (t[0] == 16 && t[1] == 1 && t[2] == 16)
-      return launch_stage_tl<Tile<16, 1, 16, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+      return launch_stage_tl<Tile<16, 1, 16, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
     if (t[0] == 1 && t[1] == 16 && t[2] == 16)
-      return launch_stage_tl<Tile<1, 16, 16, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+      return launch_stage_tl<Tile<1, 16, 16, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
     if (t[0] == 256 && t[1] == 1 && t[2] == 1)
-      return launch_stage_tl<Tile<256, 1, 1, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+      return launch_stage_tl<Tile<256, 1, 1, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
     if (t[0] == 1 && t[1] == 256 && t[2] == 1)
-      return launch_stage_tl<Tile<1, 256, 1, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+      return launch_stage_tl<Tile<1, 256, 1, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
     if (t[0] == 1 && t[1] == 1 && t[2] == 256)
-      return launch_stage_tl<Tile<1, 1, 256, 256, 2, 4>>(G, A, mag, glm, nullptr, st);
+      return launch_stage_tl<Tile<1, 1, 256, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
     return cudaErrorInvalidValue;
   }
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
-  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4>>(G, A, mag, glm, tm, st);
-  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, tm, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256, 288, 2>>(G, A, mag, glm, nullptr, st);
   return cudaErrorInvalidValue;
 }
 
@@ -747,10 +747,10 @@ cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
 // in its descriptor, so a batch step equals one hormone.f90 step per grid.
 
 using T3D = Tile<8, 8, 8, 640, 1>;
-using T3D4 = Tile<8, 8, 4>;
-using T2D = Tile<16, 16, 1>;
-using T2D8 = Tile<32, 8, 1>;
-using T1D = Tile<256, 1, 1>;
+using T3D4 = Tile<8, 8, 4, 384, 2>;
+using T2D = Tile<16, 16, 1, 288, 2>;
+using T2D8 = Tile<32, 8, 1, 320, 2>;
+using T1D = Tile<256, 1, 1, 288, 2>;
 
 // tile ids: 0 3-D 8x8x8 (640 threads), 1 3-D 8x8x4 (256 threads, 2 CTAs/SM),
 // 2 2-D 16x16, 3 2-D 32x8, 4 1-D 256.  batch_tile_kind gives the grid's

@@ -39,7 +39,10 @@ template <int TX_, int TY_, int TZ_, int NT_ = 256, int MINB_ = 2, int SP_ = 0>
 struct Tile {
   static constexpr int TX = TX_, TY = TY_, TZ = TZ_;
   static constexpr int SP = SP_;      // passive scalars the shared-memory layout has room for
-  static constexpr int NT = NT_;      // threads per CTA (at least the tile's cell count)
+  // threads per CTA: at least the tile's cell count, and best the size of the
+  // largest per-axis slope box, so that every phase of an axis pass takes one
+  // round (16x16 -> 288, 256 -> 288, 32x8 -> 320, 8x8x4 -> 384, 8x8x8 -> 640)
+  static constexpr int NT = NT_;
   static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget is sized for
   static constexpr int NC = TX * TY * TZ;
   static constexpr int HX = TX > 1 ? 2 : 0, HY = TY > 1 ? 2 : 0, HZ = TZ > 1 ? 2 : 0;
