@@ -967,12 +967,13 @@ __device__ __forceinline__ double rdist(const GridDev& G, int i, int j, int k) {
   return sqrt(x * x + y * y + z * z);
 }
 
-__global__ void __launch_bounds__(256) hg_stage_kernel(const GridDev G, const HGArgs A) {
-  const size_t plane = A.plane;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(c % G.n[0]);
-    const int j = (int)((c / G.n[0]) % G.n[1]);
-    const int k = (int)(c / ((size_t)G.n[0] * G.n[1]));
+// one thread per cell of an x row segment; rows by (blockIdx.y, blockIdx.z)
+// = (j, k), so no index division
+__global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HGArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i < G.n[0]) {
+    const size_t c = cidx(G, i, j, k);
     const AxisGeo &gx = G.g[0], &gy = G.g[1], &gz = G.g[2];
     double c0 = -((gx.idx[i + 2] + gx.idx[i + 3]) * gy.dxi[j + 2] * gz.dxi[k + 2] +
                   (gy.idx[j + 2] + gy.idx[j + 3]) * gx.dxi[i + 2] * gz.dxi[k + 2] +
@@ -1040,7 +1041,10 @@ __global__ void __launch_bounds__(256) hg_stage_kernel(const GridDev G, const HG
 }
 
 cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cudaStream_t st) {
-  hg_stage_kernel<<<nblocks, 256, 0, st>>>(G, A);
+  (void)nblocks;
+  const int bx = G.n[0] < 128 ? ((G.n[0] + 31) / 32) * 32 : 128;
+  const dim3 grid((G.n[0] + bx - 1) / bx, G.n[1], G.n[2]);
+  hg_stage_kernel<<<grid, bx, 0, st>>>(G, A);
   return cudaGetLastError();
 }
 
