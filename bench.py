@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope"], default="ot3d",
+    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope", "briowu"], default="ot3d",
                     help="ot3d: the headline (3-D Orszag-Tang 256^3); kh-batch: 512 uneven 2-D KH boxes batched vs "
                          "one at a time; serve: a Poisson request stream through the continuous-batching server; "
                          "polytrope: 192^3 self-gravitating polytrope with hyperbolic gravity")
@@ -624,6 +624,66 @@ def run_polytrope(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_briowu(args, rank=0, world=1, local_rank=0):
+    """The Brio-Wu shock tube of the benchmark list (1024 cells on [0,1],
+    gamma=2, Bx=0.75, minmod, CFL 0.4, to t=0.1): time to solution of the
+    whole run on the device clock (hmn_run), FP64 and mixed, against the
+    oracle's CPU run of the same case.  A parity case: ~2000 steps of 1024
+    cells are launch-bound on a GPU."""
+    import numpy as np
+    import torch
+
+    from hormone_b200 import config, grid as G, ic
+    from hormone_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    cfg = config.resolve("briowushock_x test", overrides=dict(ie=1024, t_end=100.0, dt_out=100.0, courant=0.4,
+                                                              flux_limiter="minmod"))
+    prims = ic.make(cfg, G.make_grid(cfg))
+    out = {}
+    for prec in (0, 1):
+        runs = []
+        for rep in range(max(1, args.warmup) + 1):
+            s = Simulation(cfg, prims, precision=prec)
+            stream = torch.cuda.ExternalStream(s.ctx.stream_ptr())
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            s.run_device()
+            e1.record(stream)
+            e1.synchronize()
+            runs.append((e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3, s.tn, s.ctx.launches()))
+            st = s.state()
+            s.close()
+        ms, wall, tn, launches = runs[-1]
+        out[prec] = dict(ms=ms, wall_ms=wall, steps=tn, launches=launches, d=st["d"])
+    l1 = float(np.sum(np.abs(out[1]["d"] - out[0]["d"])) / np.sum(np.abs(out[0]["d"])))
+    cpu = None
+    if not args.no_cpu:
+        from oracle.oracle import Oracle
+
+        o = Oracle(cfg)
+        o.set_prims(prims)
+        t0 = time.perf_counter()
+        o.start()
+        o.run()
+        el = time.perf_counter() - t0
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": 1024 * o.scalars()["tn"] / el, "unit": METRIC, "cores": cores, "kind": "port",
+               "sample": f"the whole run ({o.scalars()['tn']} steps, {el:.2f} s) of the CPU restatement"}
+    cells = 1024
+    r0 = out[0]
+    line = {"metric": METRIC, "value": cells * r0["steps"] / (r0["ms"] * 1e-3), "unit": METRIC, "n_gpus": 1,
+            "steps": r0["steps"], "warmup": max(1, args.warmup), "ms_per_step": r0["ms"] / r0["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "brio-wu-1024-cells-t0.1", "gamma": 2.0, "limiter": "minmod", "courant": 0.4,
+                       "l2": "inputs far smaller than L2 (a launch-bound parity case)"},
+            "time_to_solution_ms": {"fp64": r0["ms"], "mixed": out[1]["ms"], "fp64_wall": r0["wall_ms"]},
+            "mixed_l1_rho_vs_fp64": l1, "gpu_launches": r0["launches"], "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args, rank=0, world=1, local_rank=0):
     """The serving stream through the continuous-batching server.  With N
     ranks every request goes to one rank (split by cells, in arrival order
@@ -693,6 +753,8 @@ def main():
             run_serve(args, rank, world, local_rank)
         elif args.workload == "polytrope":
             run_polytrope(args, rank, world, local_rank)
+        elif args.workload == "briowu":
+            run_briowu(args, rank, world, local_rank)
         elif args.decomp == "slab" and world > 1:
             run_slab(args, rank, world, local_rank)
         else:
