@@ -46,8 +46,6 @@ struct hmn_ctx {
   double grvtime, cgrav_old;
   double dtg_unit;
   int nsm;
-  cudaGraphExec_t graph;
-  int graph_steps;
   TmaMaps tmaps[2];          // tensor maps of pbuf[0], pbuf[1] for TMA staging of 3-D tiles
   int tma_ok;
   double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
@@ -411,7 +409,6 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   if (ctx->ck_done) cudaEventDestroy(ctx->ck_done);
   cudaFree(ctx->ck_dev);
   if (ctx->ck_h) cudaFreeHost(ctx->ck_h);
-  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
   for (int b = 0; b < 2; b++) cudaFree(ctx->pbuf[b]);
   cudaFree(ctx->spcorg);
@@ -470,7 +467,6 @@ extern "C" int hmn_upload(hmn_ctx* ctx, const double* u, const double* const pri
     rc = to_device(ctx, ctx->gpsi[ctx->gcur], grvpsi, 1, gp);
     if (rc) return rc;
   }
-  ctx->graph_steps = 0;
   CK(cudaStreamSynchronize(ctx->st), "sync");
   return HMN_OK;
 }
@@ -605,7 +601,6 @@ static int enqueue_hydro(hmn_ctx* ctx) {
 extern "C" int hmn_hydro_step(hmn_ctx* ctx) {
   if (!ctx) return HMN_EINVAL;
   if (slab_exchanges(ctx)) return HMN_EBADCFG;  // the halos must be exchanged between stages
-  ctx->graph_steps = 0;
   return enqueue_hydro(ctx);
 }
 
@@ -659,7 +654,6 @@ extern "C" int hmn_pack_halos(hmn_ctx* ctx) {
 
 extern "C" int hmn_hydro_stage(hmn_ctx* ctx, int stage) {
   if (!ctx || stage < 1 || stage > ctx->par.rktype) return HMN_EINVAL;
-  ctx->graph_steps = 0;
   return enqueue_stage(ctx, stage);
 }
 
