@@ -133,18 +133,21 @@ def params_struct(cfg: dict, precision: int = 0) -> HmnParams:
 class Context:
     """One simulation resident on the GPU (a thin owner of an ``hmn_ctx*``)."""
 
-    def __init__(self, cfg: dict, grid, precision: int = 0):
+    def __init__(self, cfg: dict, grid, precision: int = 0, ghost: int = 0):
+        """ghost = 2 makes every host array carry HORMONE's two ghost layers
+        per side (the Fortran module arrays' layout); 0 is packed."""
         L = lib()
         self.cfg = cfg
         n = cfg["n"]
-        self.shape = (n[2], n[1], n[0])
+        self.ghost = ghost
+        self.shape = (n[2] + 2 * ghost, n[1] + 2 * ghost, n[0] + 2 * ghost)
         self.nvar = cfg["nvar"]
         self.nspc = int(cfg.get("nspc", 0))
         self._grid_arrays = []
         g = HmnGrid()
         for a in range(3):
             g.n[a] = n[a]
-        g.ghost = 0
+        g.ghost = ghost
         bc = np.asarray(cfg["bc"], dtype=np.int32).reshape(-1)
         for q in range(12):
             g.bc[q] = int(bc[q])
@@ -203,15 +206,17 @@ class Context:
 
     def download(self, prims=True, u=True, gravity=False) -> Dict[str, np.ndarray]:
         out: Dict[str, np.ndarray] = {}
-        U = np.empty((self.nvar,) + self.shape) if u else None
+        # ghosted layouts: the ghost layers are never written, leave them NaN
+        new = (lambda shape: np.full(shape, np.nan)) if self.ghost else np.empty
+        U = new((self.nvar,) + self.shape) if u else None
         pp = None
         if prims:
-            P = np.empty((9,) + self.shape)
+            P = new((9,) + self.shape)
             pp = (_DP * 9)()
             for q in range(9):
                 pp[q] = _dp(P[q])
-        gphi = np.empty(self.shape) if gravity else None
-        gpsi = np.empty(self.shape) if gravity else None
+        gphi = new(self.shape) if gravity else None
+        gpsi = new(self.shape) if gravity else None
         self._check(lib().hmn_download(self.h, _dp(U), pp, _dp(gphi), _dp(gpsi)), "hmn_download")
         if u:
             out["u"] = U
