@@ -14,6 +14,7 @@ HORMONE-format parameter files can be given instead and then takes over.
 """
 from __future__ import annotations
 
+import math
 import os
 import re
 from typing import Any, Dict, Optional
@@ -106,7 +107,7 @@ BASE: Dict[str, Any] = dict(
     bc1is=0, bc1os=0, bc2is=0, bc2os=0, bc3is=0, bc3os=0,
     bc1iv=0, bc1ov=0, bc2iv=0, bc2ov=0, bc3iv=0, bc3ov=0,
     gravswitch=0, HGfac=5.0, hgcfl=0.9, maxtngrv=-1, gbtype=0, grktype=2, alphagrv=0.1,
-    G=6.67430e-8, fixed_dt=-1.0,
+    G=6.67430e-8, fixed_dt=-1.0, eq_sym=False,
     test_tol=1e-15, Mach_tol=1e-5,
 )
 
@@ -128,6 +129,11 @@ SIMTYPES: Dict[str, Dict[str, Any]] = {
                           dt_out=500.0, tn_out=1, dt_unit="ms", test_tol=7e-15),
     "orszagtang_xz": dict(ie=128, ke=128, mag_on=True, outstyle=1, endstyle=1, tnlim=100000, t_end=500.0,
                           dt_out=500.0, tn_out=1, dt_unit="ms", test_tol=7e-15),
+    # para/parameters_sedov_default (spherical, 1-D radial) with
+    # para/extras_sedov (gamma=1.4, damb=1, Eexp=1; read by sedov.f90:30-38)
+    "sedov_default": dict(xi1s=0.0, xi1e=1.0, ie=500, outstyle=1, endstyle=1, tnlim=100000, t_end=300.0,
+                          dt_out=300.0, tn_out=1, dt_unit="ms", eostype=0, crdnt=2, flux_limiter="modified_mc",
+                          bc1is=1, bc1os=2, bc1iv=1, bc1ov=2, test_tol=2e-14, gamma=1.4, damb=1.0, Eexp=1.0),
     # para/parameters_KHinstability (two passive scalars)
     "KHinstability": dict(xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5, ie=128, je=128, outstyle=1, endstyle=1,
                           tnlim=100000, t_end=1000.0, dt_out=100.0, tn_out=1, dt_unit="ms", compswitch=2, spn=2),
@@ -197,8 +203,9 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     dim = sum(solve)
     if dim == 0:
         raise ValueError("Error from gridset: no direction to solve")
-    if int(cfg.get("crdnt", 0)) != 0:
-        raise ValueError("only Cartesian coordinates (crdnt=0) are on this path")
+    crdnt = int(cfg.get("crdnt", 0))
+    if crdnt not in (0, 2):
+        raise ValueError("Cartesian (crdnt=0) and spherical (crdnt=2) coordinates are on this path")
     if int(cfg.get("eostype", 0)) != 0:
         raise ValueError("only the ideal-gas EOS (eostype=0) is on this path")
     mag_on = bool(cfg["mag_on"])
@@ -214,6 +221,9 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
             x, y = bc[a, 0, sv], bc[a, 1, sv]
             if x * y == 0 and x + y != 0:
                 raise ValueError(f"boundary condition axis {a + 1}: both sides must be periodic")
+    if crdnt == 2:  # polar boundaries (checksetup.f90:112-115, :134-137)
+        bc[1] = 1
+        bc[2] = 0
     if not solve[0]:
         bc[0] = 2
     if not solve[1]:
@@ -246,15 +256,24 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     nspc = int(cfg.get("spn", 0)) if comp == 2 else 0
     if nspc < 0 or nspc > 4:
         raise ValueError("at most 4 passive scalars are on this path")
+    if crdnt == 2 and nspc:
+        raise ValueError("passive scalars on spherical grids are not on this path")
     grav = int(cfg.get("gravswitch", 0))
+    if crdnt == 2 and grav:
+        raise ValueError("self-gravity on spherical grids is not on this path")
     if grav not in (0, 3):
         raise ValueError("only gravswitch 0 (off) or 3 (hyperbolic) is on this path")
     if grav == 3 and dim != 3:
         raise ValueError("the Cartesian hyperbolic gravity solver needs a 3-D grid")
+    extent = [(float(cfg["xi1s"]), float(cfg["xi1e"])), (float(cfg["xi2s"]), float(cfg["xi2e"])),
+              (float(cfg["xi3s"]), float(cfg["xi3e"]))]
+    if crdnt == 2:  # gridset.f90:295-296
+        half = n[1] == 1 or bool(cfg.get("eq_sym", False))
+        extent[1] = (0.0, math.pi * 0.5 if half else math.pi)
+        extent[2] = (-math.pi, math.pi)
     cfg.update(
-        n=n, solve=solve, dim=dim, mag_on=mag_on, glm=glm, nvar=nvar, bc=bc,
-        extent=[(float(cfg["xi1s"]), float(cfg["xi1e"])), (float(cfg["xi2s"]), float(cfg["xi2e"])),
-                (float(cfg["xi3s"]), float(cfg["xi3e"]))],
+        n=n, solve=solve, dim=dim, mag_on=mag_on, glm=glm, nvar=nvar, bc=bc, crdnt=crdnt,
+        extent=extent,
         t_end=t_end, dt_out=dt_out, t_out=t_out, tn_out=tn_out, limiter_code=_LIMITERS[lim],
         rktype=int(cfg["rktype"]), gamma=float(cfg["gamma"]), courant=float(cfg["courant"]),
         alpha9wave=float(cfg["alpha9wave"]), outstyle=int(cfg["outstyle"]), endstyle=int(cfg["endstyle"]),

@@ -1,5 +1,6 @@
-"""Cartesian grid arrays, built as HORMONE's gridset builds them (uniform
-or geometrical-series meshes).
+"""Grid arrays, built as HORMONE's gridset builds them: Cartesian axes
+(uniform or geometrical-series meshes) and spherical polar axes (r, theta,
+phi) with their metric factors.
 
 Each axis holds six arrays over Fortran indices ``is-2 .. ie+2`` (stored at
 offset +2, length n+4): cell centres ``x``, right faces ``xi``, centre
@@ -12,7 +13,9 @@ and the ghost layers re-accumulated (gridset.f90:71-81).
 """
 from __future__ import annotations
 
-from typing import Dict, List
+import math
+from decimal import Decimal, localcontext
+from typing import Dict, List, Tuple
 
 import numpy as np
 
@@ -99,9 +102,103 @@ def axis_from_widths(widths, xis: float, gravity: bool = False) -> Dict[str, np.
 MESH_KEYS = (("imesh", "x1min"), ("jmesh", "x2min"), ("kmesh", "x3min"))
 
 
+def quad_sin_cos(x: float) -> Tuple[float, float]:
+    """sin and cos of a binary64 value, summed as Taylor series to 60
+    digits and rounded once to binary64.  The reference takes them in quad
+    precision and rounds to double (gridset.f90:376-382); both are the
+    correctly rounded values except in double-rounding cases far rarer than
+    any grid here."""
+    with localcontext() as ctx:
+        ctx.prec = 60
+        t = Decimal(x)  # exact
+        t2 = t * t
+        s, c = Decimal(0), Decimal(0)
+        ts, tc = t, Decimal(1)
+        n = 0
+        eps = Decimal(10) ** -58
+        while abs(ts) > eps or abs(tc) > eps:
+            s += ts
+            c += tc
+            ts = -ts * t2 / ((2 * n + 2) * (2 * n + 3))
+            tc = -tc * t2 / ((2 * n + 1) * (2 * n + 2))
+            n += 1
+        return float(s), float(c)
+
+
+def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
+    """Spherical polar axes (crdnt=2) as gridset.f90:294-423 builds them
+    without gravity, and the 1-D metric factors of metric.f90:102-151.
+
+    r runs over [xi1s, xi1e] (uniform, or a geometrical series with imesh=1)
+    with volumetric cell centres; theta over [0, pi] ([0, pi/2] for one
+    theta cell or eq_sym), uniform, with volumetric centres; phi over
+    [-pi, pi], uniform (one cell stands for a quarter turn).  Extra keys:
+    axis 0 ``detg`` (xi1**2), ``idetg`` and ``sx`` (over is-1..ie+1);
+    axis 1 ``sini``/``cosi`` (is-2..ie+2) and ``scot`` (js-1..je+1)."""
+    n1, n2, n3 = (int(v) for v in cfg["n"])
+    if int(cfg.get("gravswitch", 0)) != 0:
+        raise ValueError("self-gravity on spherical grids is not on this path")
+    if 1 < n3 < 4:
+        raise ValueError(f"Error from ke {n3}: a spherical grid needs one or at least four phi cells")
+    if int(cfg.get("jmesh", 0)) != 0 or int(cfg.get("kmesh", 0)) != 0:
+        raise ValueError("spherical grids take uniform theta and phi meshes (jmesh=kmesh=0) on this path")
+    lo, hi = (float(v) for v in cfg["extent"][0])
+    imesh = int(cfg.get("imesh", 0)) if n1 > 1 else 0
+    if imesh == 0:
+        widths = [(hi - lo) / float(n1)] * (n1 + 4)
+    elif imesh == 1:
+        widths = geometric_widths(n1, lo, hi, float(cfg["x1min"]))
+    else:
+        raise ValueError(f"imesh={imesh}: only uniform (0) and geometrical-series (1) meshes are on this path")
+    r = axis_from_widths(widths, lo)
+    x, xi, dx, idx = (r[k].tolist() for k in ("x", "xi", "dx", "idx"))
+    for s in range(1, n1 + 4):  # Fortran is-1 .. ie+2 (:323-329)
+        a, b = xi[s], xi[s - 1]
+        x[s] = 0.75 * (a + b) * (a * a + b * b) / (a * a + a * b + b * b)
+        if s == 2:
+            x[1] = -x[2]
+        dx[s] = x[s] - x[s - 1]
+        idx[s] = 1.0 / dx[s]
+    r.update(x=np.array(x), dx=np.array(dx), idx=np.array(idx))
+
+    pi = math.pi  # acos(-1d0)
+    xi2e = pi * 0.5 if (n2 == 1 or bool(cfg.get("eq_sym", False))) else pi
+    th = axis_from_widths([xi2e / float(1 if n2 == 1 else n2)] * (n2 + 4), 0.0)
+    x, xi, dx, idx = (th[k].tolist() for k in ("x", "xi", "dx", "idx"))
+    sc = [quad_sin_cos(v) for v in xi]
+    si, ci = [v[0] for v in sc], [v[1] for v in sc]
+    for s in range(1, n2 + 4):  # js-1 .. je+2 (:385-392)
+        x[s] = (xi[s - 1] * ci[s - 1] - xi[s] * ci[s] + si[s] - si[s - 1]) / (ci[s - 1] - ci[s])
+        if s == 2:
+            x[1] = -x[2]
+        dx[s] = x[s] - x[s - 1]
+        idx[s] = 1.0 / dx[s]
+    th.update(x=np.array(x), dx=np.array(dx), idx=np.array(idx))
+
+    ketmp = 4 if n3 == 1 else n3
+    ph = axis_from_widths([(pi - -pi) / float(ketmp)] * (n3 + 4), -pi)
+
+    # metric.f90:102-151 (1-D factors; the 2-D/3-D ones are their products)
+    xi, dxi = r["xi"].tolist(), r["dxi"].tolist()
+    detg, idetg, sx = [0.0] * (n1 + 4), [0.0] * (n1 + 4), [0.0] * (n1 + 4)
+    for s in range(1, n1 + 3):
+        a, b = xi[s], xi[s - 1]
+        detg[s] = a * a
+        idetg[s] = 3.0 / (dxi[s] * (a * a + a * b + b * b))
+        sx[s] = 1.5 * (a + b) / (a * a + a * b + b * b)
+    scot = [0.0] * (n2 + 4)
+    for s in range(1, n2 + 3):
+        scot[s] = (si[s] - si[s - 1]) / (ci[s - 1] - ci[s])
+    r.update(detg=np.array(detg), idetg=np.array(idetg), sx=np.array(sx))
+    th.update(sini=np.array(si), cosi=np.array(ci), scot=np.array(scot))
+    return [r, th, ph]
+
+
 def make_grid(cfg) -> List[Dict[str, np.ndarray]]:
     """The three axes of gridset.f90: uniform (mesh 0) or geometrical series
-    (mesh 1, first cell x?min wide)."""
+    (mesh 1, first cell x?min wide); spherical polar with crdnt=2."""
+    if int(cfg.get("crdnt", 0)) == 2:
+        return spherical_grid(cfg)
     grav = int(cfg.get("gravswitch", 0)) != 0
     out = []
     for a in range(3):
@@ -120,3 +217,28 @@ def make_grid(cfg) -> List[Dict[str, np.ndarray]]:
 def centres(grid, a: int) -> np.ndarray:
     """Interior cell centres of axis a."""
     return grid[a]["x"][2:-2]
+
+
+def spherical_dvol(grid, n) -> np.ndarray:
+    """Cell volumes dvol(i,j,k) of a spherical grid, (nz, ny, nx), in the
+    operation order of metric.f90:122-123:
+    (xi1(i)**3-xi1(i-1)**3)/3 * (cosi(j-1)-cosi(j)) * dxi3(k) * fac_j * fac_k."""
+    n1, n2, n3 = (int(v) for v in n)
+    xi = grid[0]["xi"]
+    a, b = xi[2:n1 + 2], xi[1:n1 + 1]
+    vr = (a * a * a - b * b * b) / 3.0
+    ci = grid[1]["cosi"]
+    cd = ci[1:n2 + 1] - ci[2:n2 + 2]
+    dxi3 = grid[2]["dxi"][2:n3 + 2]
+    fac_j = 2.0 if n2 == 1 else 1.0
+    fac_k = 4.0 if n3 == 1 else 1.0
+    return vr[None, None, :] * cd[None, :, None] * dxi3[:, None, None] * fac_j * fac_k
+
+
+def fortran_sum(a: np.ndarray) -> float:
+    """Fortran SUM of an array section: one running sum in storage order
+    (i fastest), no reassociation."""
+    t = 0.0
+    for v in np.ascontiguousarray(a).reshape(-1).tolist():
+        t = t + v
+    return t

@@ -220,6 +220,28 @@ def sedov(cfg, grid, energy: float = 1.0, radius: float = 0.05, rho0: float = 1.
     return out
 
 
+def sedov_spherical(cfg, grid) -> Dict[str, np.ndarray]:
+    """Spherical Sedov-Taylor blast of src/init/sedov.f90:14-64: density
+    damb everywhere; the energy Eexp as pressure (gamma-1)*Eexp/vol_inj in
+    the first ten radial cells (vol_inj their volume), and the ambient
+    pressure 1e-3*Eexp/vol_tot elsewhere; at rest."""
+    from .grid import fortran_sum, spherical_dvol
+
+    out = _blank(cfg)
+    i_inj = 10
+    damb, eexp = float(cfg.get("damb", 1.0)), float(cfg.get("Eexp", 1.0))
+    dvol = spherical_dvol(grid, cfg["n"])
+    vol_inj = fortran_sum(dvol[:, :, :i_inj])
+    ein = eexp / vol_inj
+    pin = (cfg["gamma"] - 1.0) * ein  # eos_p, eostype 0 (eos.f90:254-256)
+    vol_tot = fortran_sum(dvol)
+    pamb = 1e-3 * eexp / vol_tot
+    out["d"][:] = damb
+    out["p"][:] = pamb
+    out["p"][:, :, :i_inj] = pin
+    return out
+
+
 def to_state(cfg, prims: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
     """Total energy and conserved variables from the initial primitives.
 
@@ -278,4 +300,6 @@ def make(cfg, grid, **kw):
         return shocktube(cfg, grid)
     if st.startswith("orszagtang"):
         return orszagtang(cfg, grid)
+    if st == "sedov_default":
+        return sedov_spherical(cfg, grid)
     raise ValueError(f"no initial condition for simtype {st}")

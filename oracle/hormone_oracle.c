@@ -15,14 +15,16 @@
  * tests/orszagtang_{xy,yz,xz}[_flat].bin with the norms of
  * src/main/tests.f90:46-292.
  *
- *   grid            src/main/gridset.f90:40-80 (uniform Cartesian)
- *   metric          src/main/metric.f90:26-51
+ *   grid            src/main/gridset.f90:40-80 (uniform Cartesian),
+ *                   :294-423 (spherical polar r, theta, phi)
+ *   metric          src/main/metric.f90:26-51 (Cartesian), :102-151 (spherical)
  *   limiters        src/main/fluxlimiter.f90:94-129
  *   slopes          src/main/interpolation.f90:49-484
  *   face fluxes     src/main/numflux.f90:46-563
  *   HLLD + GLM      src/main/hlldflux.f90:19-179
  *   EOS (ideal)     src/main/eos.f90:195-274,351-365,742-866
- *   source          src/main/source.f90:14-85,177-228
+ *   source          src/main/source.f90:14-85,177-228; spherical geometric
+ *                   terms :113-143, pinned by tests/sedov_default[_flat].bin
  *   RK + primitive  src/main/rungekutta.f90:16-232
  *   boundaries      src/main/boundarycondition.f90:14-1442 (codes 0-3; 4/5
  *                   linear extrapolation as :302-327,419-468; 9 Dirichlet
@@ -43,6 +45,7 @@
  * operation, as in the reference built without optimisation.
  */
 #include <math.h>
+#include <quadmath.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -81,6 +84,12 @@ typedef struct {
   /* Dirichlet ghost values per face: 8 + spn planes (d, p, v1..3, b1..3,
      spc) x 2 layers x face cells, layer l at coordinate -2+l (inner) or n+l */
   double *dir[3][2];
+  /* coordinate system: 0 Cartesian, 2 spherical polar (r, theta, phi) with
+     the metric factors of metric.f90:102-151 (offset +2 like the axes) */
+  int crdnt;
+  double *detg1, *idetg1, *sx1;   /* r faces / cells */
+  double *sini, *cosi, *scot;     /* theta faces / cells */
+  double fac_j, fac_k;
   /* scalars */
   double dt, ch, time, t_out, t_end, dt_out, cfmax;
   double cgrav, cgrav_old, dtgrav, dtg_unit, grvtime;
@@ -140,6 +149,9 @@ Oracle *hmo_create(int nx, int ny, int nz, int mag_on, int limiter, int rktype, 
   for (size_t c = 0; c < N; c++) { o->d[c] = 1.0; o->p[c] = 1.0; o->e[c] = 1.0; o->eint[c] = 1.0; o->cs[c] = 1.0; o->ptot[c] = 1.0; }
   o->grvphi = zalloc(N); o->grvpsi = zalloc(N); o->gorg1 = zalloc(N); o->gorg2 = zalloc(N);
   o->lapphi = zalloc(N); o->hgsrc = zalloc(N); o->gsrc = zalloc(N);
+  o->detg1 = zalloc((size_t)nx + 4); o->idetg1 = zalloc((size_t)nx + 4); o->sx1 = zalloc((size_t)nx + 4);
+  o->sini = zalloc((size_t)ny + 4); o->cosi = zalloc((size_t)ny + 4); o->scot = zalloc((size_t)ny + 4);
+  o->fac_j = 1.0; o->fac_k = 1.0;
   return o;
 }
 
@@ -157,6 +169,7 @@ void hmo_destroy(Oracle *o) {
   }
   free(o->grvphi); free(o->grvpsi); free(o->gorg1); free(o->gorg2); free(o->lapphi); free(o->hgsrc); free(o->gsrc);
   for (int a = 0; a < 3; a++) { free(o->dir[a][0]); free(o->dir[a][1]); }
+  free(o->detg1); free(o->idetg1); free(o->sx1); free(o->sini); free(o->cosi); free(o->scot);
   for (int n = 0; n < o->spn; n++) {
     free(o->spc[n]); free(o->spcorg[n]);
     for (int a = 0; a < 3; a++) { free(o->dspc[a][n]); free(o->spcflx[a][n]); }
@@ -248,9 +261,9 @@ void hmo_make_axis(Oracle *o, int a, double xis, const double *widths) {
 #undef G2
 }
 
-/* geometrical-series mesh (imesh=1): utils.f90:351-404 */
-int hmo_make_geometric_axis(Oracle *o, int a, double xis, double xie, double xmin) {
-  int n = o->n[a];
+/* cell widths dxi(is-2:ie+2) of a geometrical-series mesh (imesh=1):
+   utils.f90:351-404 */
+static int geometric_widths(int n, double xis, double xie, double xmin, double *w) {
   const double xrmax = 1.05, maxerr = 1e-10;
   double xr = 1.01, xrng = xie - xis, irng = (double)n;
   if (xrng / irng < xmin) return HMO_EBADCFG;
@@ -263,7 +276,6 @@ int hmo_make_geometric_axis(Oracle *o, int a, double xis, double xie, double xmi
     xr = xrnew;
   }
   if (xr > xrmax) return HMO_EBADCFG;
-  double *w = zalloc((size_t)n + 4);
   w[2] = xmin;
   for (int i = 1; i < n; i++) w[i + 2] = w[i + 1] * xr;
   w[1] = w[2];
@@ -272,9 +284,99 @@ int hmo_make_geometric_axis(Oracle *o, int a, double xis, double xie, double xmi
   w[n + 3] = w[n + 1] * xr * xr;
   if (xr - 1.0 < maxerr)
     for (int i = 0; i < n + 4; i++) w[i] = xrng / irng;
-  hmo_make_axis(o, a, xis, w);
-  free(w);
   return HMO_OK;
+}
+
+int hmo_make_geometric_axis(Oracle *o, int a, double xis, double xie, double xmin) {
+  double *w = zalloc((size_t)o->n[a] + 4);
+  int rc = geometric_widths(o->n[a], xis, xie, xmin, w);
+  if (rc == HMO_OK) hmo_make_axis(o, a, xis, w);
+  free(w);
+  return rc;
+}
+
+/* sin and cos evaluated in quad precision and rounded to double, as
+   gridset.f90:376-382 forms sini/cosi with real(..., kind=16) */
+static double qsin(double x) { return (double)sinq((__float128)x); }
+static double qcos(double x) { return (double)cosq((__float128)x); }
+
+/* Spherical polar grid (crdnt=2) without gravity: r from xi1s to xi1e
+   (uniform, or a geometrical series with first width x1min when imesh=1),
+   theta over [0, pi] ([0, pi/2] for one theta cell or eq_sym), phi over
+   [-pi, pi) (a quarter turn for one phi cell), with the volumetric centres
+   of r and theta; gridset.f90:294-423.  Then the metric factors of
+   metric.f90:102-151. */
+int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1min, int eq_sym) {
+  const int n1 = o->n[0], n2 = o->n[1], n3 = o->n[2];
+  if (o->gravswitch != 0 || (n3 > 1 && n3 < 4)) return HMO_EBADCFG;
+  const double pi = acos(-1.0);
+  double *w = zalloc((size_t)(n1 > n2 ? (n1 > n3 ? n1 : n3) : (n2 > n3 ? n2 : n3)) + 4);
+  /* r */
+  if (imesh == 1) {
+    int rc = geometric_widths(n1, xi1s, xi1e, x1min, w);
+    if (rc) { free(w); return rc; }
+  } else {
+    for (int i = 0; i < n1 + 4; i++) w[i] = (xi1e - xi1s) / (double)n1;
+  }
+  hmo_make_axis(o, 0, xi1s, w);
+  {
+    double *x = o->x[0] + 2, *xi = o->xi[0] + 2, *dx = o->dx[0] + 2, *idx = o->idx[0] + 2;
+    for (int i = -1; i <= n1 + 1; i++) { /* :323-329 */
+      x[i] = 0.75 * (xi[i] + xi[i - 1]) * (xi[i] * xi[i] + xi[i - 1] * xi[i - 1]) /
+             (xi[i] * xi[i] + xi[i] * xi[i - 1] + xi[i - 1] * xi[i - 1]);
+      if (i == 0) x[i - 1] = -x[i];
+      dx[i] = x[i] - x[i - 1];
+      idx[i] = 1.0 / dx[i];
+    }
+  }
+  /* theta */
+  double xi2e = (n2 == 1 || eq_sym) ? pi * 0.5 : pi;
+  int jetmp = n2 == 1 ? 1 : n2;
+  for (int j = 0; j < n2 + 4; j++) w[j] = xi2e / (double)jetmp;
+  hmo_make_axis(o, 1, 0.0, w);
+  {
+    double *x = o->x[1] + 2, *xi = o->xi[1] + 2, *dx = o->dx[1] + 2, *idx = o->idx[1] + 2;
+    double *si = o->sini + 2, *ci = o->cosi + 2;
+    for (int j = -2; j <= n2 + 1; j++) { si[j] = qsin(xi[j]); ci[j] = qcos(xi[j]); }
+    for (int j = -1; j <= n2 + 1; j++) { /* :385-392 */
+      x[j] = (xi[j - 1] * ci[j - 1] - xi[j] * ci[j] + si[j] - si[j - 1]) / (ci[j - 1] - ci[j]);
+      if (j == 0) x[j - 1] = -x[j];
+      dx[j] = x[j] - x[j - 1];
+      idx[j] = 1.0 / dx[j];
+    }
+  }
+  /* phi */
+  int ketmp = n3 == 1 ? 4 : n3;
+  for (int k = 0; k < n3 + 4; k++) w[k] = (pi - -pi) / (double)ketmp;
+  hmo_make_axis(o, 2, -pi, w);
+  free(w);
+  /* metric.f90:102-151 */
+  {
+    const double *xi = o->xi[0] + 2, *dxi = o->dxi[0] + 2;
+    double *g1 = o->detg1 + 2, *ig1 = o->idetg1 + 2, *s1 = o->sx1 + 2;
+    for (int i = -1; i <= n1; i++) {
+      g1[i] = xi[i] * xi[i];
+      ig1[i] = 3.0 / (dxi[i] * (xi[i] * xi[i] + xi[i] * xi[i - 1] + xi[i - 1] * xi[i - 1]));
+      s1[i] = 1.5 * (xi[i] + xi[i - 1]) / (xi[i] * xi[i] + xi[i] * xi[i - 1] + xi[i - 1] * xi[i - 1]);
+    }
+    const double *si = o->sini + 2, *ci = o->cosi + 2;
+    double *sc = o->scot + 2;
+    for (int j = -1; j <= n2; j++) sc[j] = (si[j] - si[j - 1]) / (ci[j - 1] - ci[j]);
+  }
+  o->fac_k = n3 == 1 ? 4.0 : 1.0;
+  o->fac_j = n2 == 1 ? 2.0 : 1.0;
+  o->crdnt = 2;
+  return HMO_OK;
+}
+
+/* metric arrays of a spherical grid: 0 detg1, 1 idetg1, 2 sx1 (n0+4 each),
+   3 sini, 4 cosi, 5 scot (n1+4 each) */
+int hmo_get_metric(Oracle *o, int which, double *out) {
+  const double *src[6] = {o->detg1, o->idetg1, o->sx1, o->sini, o->cosi, o->scot};
+  if (which < 0 || which > 5) return -1;
+  size_t L = (size_t)o->n[which < 3 ? 0 : 1] + 4;
+  memcpy(out, src[which], L * sizeof(double));
+  return 0;
 }
 
 void hmo_make_uniform_axis(Oracle *o, int a, double xis, double xie) {
@@ -803,6 +905,23 @@ static void source(Oracle *o) {
       for (int i = 0; i < nx; i++) {
         size_t c = IX(o, i, j, k);
         for (int q = 0; q < 9; q++) o->src[q][c] = 0.0;
+        if (o->crdnt == 2) {
+          /* spherical geometric terms (source.f90:113-143; no gravity here) */
+          const double d = o->d[c], v1 = o->v[0][c], v2 = o->v[1][c], v3 = o->v[2][c], pt = o->ptot[c];
+          const double s1 = o->sx1[i + 2], sc = o->scot[j + 2];
+          o->src[IMO1][c] = (d * (v2 * v2 + v3 * v3) + 2.0 * pt) * s1;
+          o->src[IMO2][c] = ny > 1 ? (-(d * v1 * v2) + (d * (v3 * v3) + pt) * sc) * s1 : 0.0;
+          o->src[IMO3][c] = (-(d * v1 * v3) - d * v2 * v3 * sc) * s1;
+          if (o->mag_on) {
+            const double b1 = o->b[0][c], b2 = o->b[1][c], b3 = o->b[2][c];
+            o->src[IMO1][c] = o->src[IMO1][c] - (b2 * b2 + b3 * b3) * s1;
+            o->src[IMO2][c] = o->src[IMO2][c] + (b1 * b2 - b3 * b3 * sc) * s1;
+            o->src[IMO3][c] = o->src[IMO3][c] + (b1 * b3 + b2 * b3 * sc) * s1;
+            o->src[IMG2][c] = (b2 * v1 - b1 * v2) * s1;
+            o->src[IMG3][c] = ((v2 * b3 - b2 * v3) * sc - (b1 * v3 - b3 * v1)) * s1;
+          }
+          continue;
+        }
         if (grav) {
           o->src[IMO1][c] = o->grv[0][c];
           o->src[IMO2][c] = o->grv[1][c];
@@ -863,6 +982,19 @@ static void rungekutta(Oracle *o) {
         for (int i = 0; i < nx; i++) {
           size_t c = IX(o, i, j, k);
           if (o->rungen == 1) UO[c] = U[c];
+          if (o->crdnt == 2) {
+            /* idetg1, idetg2 = sx1/(cos(theta_-)-cos(theta_+)), idetg3 (metric.f90:105-130) */
+            const double *g1 = o->detg1 + 2, *si = o->sini + 2, *ci = o->cosi + 2, *s1 = o->sx1 + 2;
+            const double *dxi2 = o->dxi[1] + 2;
+            double id2 = 1.0 / (-ci[j] + ci[j - 1]) * s1[i];
+            double id3 = id2 * dxi2[j] * idxi3[k] / o->fac_k;
+            U[c] = faco * UO[c] + facn * U[c] +
+                   fact * dt *
+                       (o->idetg1[i + 2] * (g1[i - 1] * F1[IX(o, i - 1, j, k)] - g1[i] * F1[c]) +
+                        id2 * (si[j - 1] * F2[IX(o, i, j - 1, k)] - si[j] * F2[c]) +
+                        id3 * (F3[IX(o, i, j, k - 1)] - F3[c]) + S[c]);
+            continue;
+          }
           U[c] = faco * UO[c] + facn * U[c] +
                  fact * dt *
                      (idxi1[i] * (1.0 * F1[IX(o, i - 1, j, k)] - 1.0 * F1[c]) +
@@ -939,6 +1071,18 @@ int hmo_timestep(Oracle *o) {
         double sa1m = dxi2[j] * dxi3[k], sa1p = dxi2[j] * dxi3[k];
         double sa2m = dxi1[i] * dxi3[k], sa2p = dxi1[i] * dxi3[k];
         double sa3m = dxi1[i] * dxi2[j], sa3p = dxi1[i] * dxi2[j];
+        if (o->crdnt == 2) { /* metric.f90:117-130 */
+          const double *xi = o->xi[0] + 2, *si = o->sini + 2, *ci = o->cosi + 2;
+          const double fj = o->fac_j, fk = o->fac_k;
+          const double a = xi[i], b = xi[i - 1];
+          dvol = (a * a * a - b * b * b) / 3.0 * (ci[j - 1] - ci[j]) * dxi3[k] * fj * fk;
+          sa1p = 0.5 * (a * a) * (ci[j - 1] - ci[j]) * dxi3[k] * fj * fk;
+          sa1m = 0.5 * (b * b) * (ci[j - 1] - ci[j]) * dxi3[k] * fj * fk;
+          sa2p = 0.5 * si[j] * (a * a - b * b) * dxi3[k] * fk;
+          sa2m = 0.5 * si[j - 1] * (a * a - b * b) * dxi3[k] * fk;
+          sa3p = 0.5 * (a * a - b * b) * dxi2[j] * fj;
+          sa3m = sa3p;
+        }
         double dti = dvol / (cf1 * off[0] * (sa1m + sa1p) + cf2 * off[1] * (sa2m + sa2p) + cf3 * off[2] * (sa3m + sa3p));
         double cm = fmax2(fmax2(cf1, cf2), cf3);
         cfmax = fmax2(cfmax, cm);

@@ -52,6 +52,10 @@ def lib():
         L.hmo_make_axis.argtypes = [_P, _I, _D, _DP]
         L.hmo_make_geometric_axis.argtypes = [_P, _I, _D, _D, _D]
         L.hmo_make_geometric_axis.restype = _I
+        L.hmo_make_spherical.argtypes = [_P, _I, _D, _D, _D, _I]
+        L.hmo_make_spherical.restype = _I
+        L.hmo_get_metric.argtypes = [_P, _I, _DP]
+        L.hmo_get_metric.restype = _I
         L.hmo_get_axis.argtypes = [_P, _I] + [_DP] * 6
         L.hmo_set_prims.argtypes = [_P] + [_DP] * 9
         L.hmo_set_grvphi.argtypes = [_P, _DP, _DP]
@@ -110,7 +114,15 @@ class Oracle:
             L.hmo_set_gravity(self.h, int(cfg["gravswitch"]), float(cfg["HGfac"]), float(cfg["hgcfl"]),
                               float(cfg["alphagrv"]), float(cfg["G"]), int(cfg["grktype"]), int(cfg["maxtngrv"]))
         mesh_keys = ("imesh", "jmesh", "kmesh")
+        if int(cfg.get("crdnt", 0)) == 2:
+            imesh = int(cfg.get("imesh", 0)) if n[0] > 1 else 0
+            lo, hi = cfg["extent"][0]
+            if L.hmo_make_spherical(self.h, imesh, float(lo), float(hi), float(cfg.get("x1min", 0.0)),
+                                    int(bool(cfg.get("eq_sym", False)))) != 0:
+                raise ValueError("spherical grid: bad settings")
         for a, (lo, hi) in enumerate(cfg["extent"]):
+            if int(cfg.get("crdnt", 0)) == 2:
+                break
             if cfg["n"][a] > 1 and int(cfg.get(mesh_keys[a], 0)) == 1:
                 xmin = float(cfg[("x1min", "x2min", "x3min")[a]])
                 if L.hmo_make_geometric_axis(self.h, a, float(lo), float(hi), xmin) != 0:
@@ -137,6 +149,16 @@ class Oracle:
         arrs = [np.zeros(n) for _ in range(6)]
         lib().hmo_get_axis(self.h, a, *[_dp(x) for x in arrs])
         return dict(zip(["x", "xi", "dx", "dxi", "idx", "idxi"], arrs))
+
+    def metric(self) -> dict:
+        """Spherical metric factors: detg1, idetg1, sx1 (n0+4) and sini,
+        cosi, scot (n1+4)."""
+        out = {}
+        for w, name in enumerate(("detg1", "idetg1", "sx1", "sini", "cosi", "scot")):
+            a = np.zeros(self.cfg["n"][0 if w < 3 else 1] + 4)
+            lib().hmo_get_metric(self.h, w, _dp(a))
+            out[name] = a
+        return out
 
     def set_prims(self, prims: dict):
         f = {k: (np.ascontiguousarray(prims[k], dtype=np.float64).reshape(-1) if prims.get(k) is not None else None)

@@ -18,7 +18,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from hormone_b200 import binio, config  # noqa: E402
 
 CASES = [f"{k}_{d}" for k in ("sodshock", "briowushock") for d in "xyz"] + \
-        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability"]
+        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability", "sedov_default"]
 
 
 def main(ref_root):
