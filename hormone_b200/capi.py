@@ -84,6 +84,7 @@ def lib():
         L.hmn_checkpoint_begin.argtypes = [_P, _DP, _DPP, _DP, _DP, _DP]
         L.hmn_upload_scalars.argtypes = [_P, _DP]
         L.hmn_set_dirichlet.argtypes = [_P, _I, _I, _DP]
+        L.hmn_set_metric.argtypes = [_P, _I] + [_DP] * 6
         L.hmn_download_scalars.argtypes = [_P, _DP]
         L.hmn_checkpoint_wait.argtypes = [_P]
         L.hmn_stream.argtypes = [_P]
@@ -93,7 +94,7 @@ def lib():
         for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
                      "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait",
-                     "hmn_upload_scalars", "hmn_download_scalars", "hmn_set_dirichlet"):
+                     "hmn_upload_scalars", "hmn_download_scalars", "hmn_set_dirichlet", "hmn_set_metric"):
             getattr(L, name).restype = _I
         _lib = L
     return _lib
@@ -163,6 +164,15 @@ class Context:
         if rc != 0:
             raise HmnError(rc, "hmn_create")
         self.h = h
+        if int(cfg.get("crdnt", 0)) == 2:
+            self.set_metric(grid)
+
+    def set_metric(self, grid):
+        """Spherical metric factors (metric.f90:102-151) from the grid's
+        ``detg``/``idetg``/``sx`` (r) and ``sini``/``cosi``/``scot`` (theta)."""
+        arrs = [np.ascontiguousarray(grid[a][k], dtype=np.float64)
+                for a, k in ((0, "detg"), (0, "idetg"), (0, "sx"), (1, "sini"), (1, "cosi"), (1, "scot"))]
+        self._check(lib().hmn_set_metric(self.h, 2, *[_dp(v) for v in arrs]), "hmn_set_metric")
 
     def close(self):
         if getattr(self, "h", None):

@@ -51,6 +51,8 @@ struct hmn_ctx {
   double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
   double* dir[3][2];         // Dirichlet ghost values per face (device)
   double* spcorg;            // passive scalars times density at RK stage 1
+  double* xi1_h;             // host copy of the r faces xi1(is-2..ie+2) for the metric
+  double* sphbuf;            // spherical metric factors (SphGeo arrays)
   // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
   cudaStream_t cst;
   cudaEvent_t ck_snap, ck_done;
@@ -301,6 +303,13 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     }
     off += (size_t)kA * L;
   }
+  ctx->xi1_h = (double*)malloc((size_t)(ctx->n[0] + 4) * sizeof(double));
+  if (!ctx->xi1_h) {
+    cudaStreamDestroy(ctx->st);
+    delete ctx;
+    return HMN_ENOMEM;
+  }
+  memcpy(ctx->xi1_h, grid->xi[0], (size_t)(ctx->n[0] + 4) * sizeof(double));
   size_t bytes = ctx->plane * sizeof(double);
   int nplanes = 9;  // every RK buffer can also hold the 9 primitive planes
   e = cudaMalloc((void**)&ctx->geo, geo_len * sizeof(double));
@@ -420,12 +429,73 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
     cudaFree(ctx->gorg[b]);
   }
   cudaFree(ctx->geo);
+  cudaFree(ctx->sphbuf);
+  free(ctx->xi1_h);
   cudaFree(ctx->prim_out);
   cudaFree(ctx->sc);
   if (ctx->sc_h) cudaFreeHost(ctx->sc_h);
   if (ctx->stage_h) cudaFreeHost(ctx->stage_h);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
+  return HMN_OK;
+}
+
+// metric.f90:102-151 for spherical polar coordinates: the caller's 1-D
+// factors plus the radial and polar products the kernels form the 2-D and
+// 3-D factors from (same single IEEE operations as the reference).
+extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, const double* idetg1, const double* sx1,
+                              const double* sini, const double* cosi, const double* scot) {
+  if (!ctx) return HMN_EINVAL;
+  if (crdnt == 0) {
+    ctx->G.sph = SphGeo{};
+    return HMN_OK;
+  }
+  if (crdnt != 2) return HMN_EBADCFG;
+  if (!detg1 || !idetg1 || !sx1 || !sini || !cosi || !scot) return HMN_EINVAL;
+  // the FP64 form of single grids without gravity or passive scalars; r solved
+  if (ctx->par.precision != 0 || ctx->par.gravswitch != 0 || ctx->par.nspc != 0 || !ctx->solve[0])
+    return HMN_EBADCFG;
+  const int L1 = ctx->n[0] + 4, L2 = ctx->n[1] + 4;
+  std::vector<double> h((size_t)6 * L1 + (size_t)4 * L2, 0.0);
+  double *g1 = h.data(), *ig1 = g1 + L1, *s1 = ig1 + L1, *vr = s1 + L1, *hr2 = vr + L1, *ar2 = hr2 + L1;
+  double *si = ar2 + L1, *ra2 = si + L2, *cd = ra2 + L2, *sc = cd + L2;
+  const double* xi = ctx->xi1_h;
+  for (int s = 0; s < L1; s++) {
+    g1[s] = detg1[s];
+    ig1[s] = idetg1[s];
+    s1[s] = sx1[s];
+    hr2[s] = 0.5 * (xi[s] * xi[s]);
+    if (s > 0) {
+      vr[s] = (xi[s] * xi[s] * xi[s] - xi[s - 1] * xi[s - 1] * xi[s - 1]) / 3.0;
+      ar2[s] = xi[s] * xi[s] - xi[s - 1] * xi[s - 1];
+    }
+  }
+  for (int s = 0; s < L2; s++) {
+    si[s] = sini[s];
+    sc[s] = scot[s];
+    if (s > 0) {
+      ra2[s] = 1.0 / (-cosi[s] + cosi[s - 1]);
+      cd[s] = cosi[s - 1] - cosi[s];
+    }
+  }
+  if (!ctx->sphbuf) CK(cudaMalloc((void**)&ctx->sphbuf, h.size() * sizeof(double)), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->sphbuf, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st), "metric");
+  CK(cudaStreamSynchronize(ctx->st), "metric");
+  SphGeo& M = ctx->G.sph;
+  const double* b = ctx->sphbuf;
+  M.detg1 = b;
+  M.idetg1 = b + L1;
+  M.sx1 = b + 2 * L1;
+  M.vr = b + 3 * L1;
+  M.hr2 = b + 4 * L1;
+  M.ar2 = b + 5 * L1;
+  M.sini = b + 6 * L1;
+  M.ra2 = M.sini + L2;
+  M.cd = M.sini + 2 * L2;
+  M.scot = M.sini + 3 * L2;
+  M.fac_j = ctx->n[1] == 1 ? 2.0 : 1.0;
+  M.fac_k = ctx->n[2] == 1 ? 4.0 : 1.0;
+  M.on = 1;
   return HMN_OK;
 }
 

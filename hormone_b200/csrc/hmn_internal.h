@@ -33,6 +33,26 @@ struct AxisGeo {
 };
 constexpr int kGeoArrays = 15;
 
+// Spherical polar coordinates (r, theta, phi as axes 1-3): the 1-D factors
+// of the metric (metric.f90:102-151), each at offset +2 like the axis
+// arrays.  The 2-D and 3-D factors of the reference (idetg2, idetg3, dvol,
+// sa1..3) are formed from them per cell in the reference's operation order.
+// on = 0 for Cartesian grids.
+struct SphGeo {
+  int on;
+  double fac_j, fac_k;   // 2 for a single theta cell, 4 for a single phi cell, else 1
+  const double* detg1;   // xi1(i)^2: weight of the r flux through the high face of cell i
+  const double* idetg1;  // 3 / (dxi1 (xi1(i)^2 + xi1(i) xi1(i-1) + xi1(i-1)^2))
+  const double* sx1;     // 1.5 (xi1(i) + xi1(i-1)) / (same sum of squares)
+  const double* vr;      // (xi1(i)^3 - xi1(i-1)^3) / 3: radial factor of dvol
+  const double* hr2;     // 0.5 xi1(i)^2: radial factor of sa1
+  const double* ar2;     // xi1(i)^2 - xi1(i-1)^2: radial factor of sa2, sa3
+  const double* sini;    // sin(theta) at the high face of cell j (detg2)
+  const double* ra2;     // 1 / (cos(theta)(j-1) - cos(theta)(j)): theta factor of idetg2
+  const double* cd;      // cos(theta)(j-1) - cos(theta)(j): theta factor of dvol, sa1
+  const double* scot;    // (sin(j) - sin(j-1)) / (cos(j-1) - cos(j))
+};
+
 struct GridDev {
   int n[3];
   int solve[3];
@@ -51,6 +71,7 @@ struct GridDev {
   // (layer l at coordinate -2+l inner, n+l outer; the other two axes in
   // increasing order, the lower one fastest)
   const double* dir[3][2];
+  SphGeo sph;
 };
 
 // Device-resident scalars of one simulation: the CFL reduction slots, the

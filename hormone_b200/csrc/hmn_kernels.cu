@@ -46,7 +46,7 @@ struct SmemT {
 
 // One axis of the fused stage: slopes, face fluxes, flux divergence of the
 // thread's own cell added to acc[].
-template <int AX, bool MAG, bool GLM, class TL>
+template <int AX, bool MAG, bool GLM, class TL, bool SPH = false>
 __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, const int t0[3],
                                           const int T[3], double acc[9], double accs[], double ch) {
   constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ;
@@ -239,11 +239,33 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
     if (cx < T[0] && cy < T[1] && cz < T[2]) {
       const int wm = cx + FBX * (cy + FBY * cz);  // face on the low side
       const int wp = wm + FSTR;
-      const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
       constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
+      if constexpr (SPH) {
+        // idetg1 (detg1 F)(i-1) - ..., idetg2 (sin F)(j-1) - ..., idetg3 (F(k-1) - F(k))
+        // with idetg2 = sx1 / (cos(j-1) - cos(j)) and idetg3 = idetg2 dxi2 / dxi3 / fac_k
+        // (rungekutta.f90:42-53, metric.f90:105-125)
+        const SphGeo& M = G.sph;
+        const int i = cx + t0[0], j = cy + t0[1], k = cz + t0[2];
+        if constexpr (AX == 0) {
+          const double cw = M.idetg1[i + 2], fm = M.detg1[i + 1], fp = M.detg1[i + 2];
 #pragma unroll
-      for (int q = 0; q < nv; q++) acc[q] = acc[q] + idxi * (sm.F[q][wm] - sm.F[q][wp]);
-      if constexpr (TL::SP > 0) {
+          for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (fm * sm.F[q][wm] - fp * sm.F[q][wp]);
+        } else if constexpr (AX == 1) {
+          const double cw = M.ra2[j + 2] * M.sx1[i + 2], fm = M.sini[j + 1], fp = M.sini[j + 2];
+#pragma unroll
+          for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (fm * sm.F[q][wm] - fp * sm.F[q][wp]);
+        } else {
+          const double cw = M.ra2[j + 2] * M.sx1[i + 2] * G.g[1].dxi[j + 2] * G.g[2].idxi[k + 2] / M.fac_k;
+#pragma unroll
+          for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (sm.F[q][wm] - sm.F[q][wp]);
+        }
+      } else {
+        const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
+#pragma unroll
+        for (int q = 0; q < nv; q++) acc[q] = acc[q] + idxi * (sm.F[q][wm] - sm.F[q][wp]);
+      }
+      if constexpr (TL::SP > 0 && !SPH) {
+        const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
 #pragma unroll
         for (int n = 0; n < TL::SP; n++)
           if (n < A.nspc) accs[n] = accs[n] + idxi * (sm.F[9 + n][wm] - sm.F[9 + n][wp]);
@@ -255,7 +277,7 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
 
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
 // (x fastest).  Shared by the single-grid and the batched kernels.
-template <bool MAG, bool GLM, class TL>
+template <bool MAG, bool GLM, class TL, bool SPH = false>
 __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, int tile_id,
                                                  const TmaMaps* tm) {
   const int tid = threadIdx.x;
@@ -284,9 +306,9 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
 #pragma unroll
   for (int n = 0; n < (TL::SP > 0 ? TL::SP : 1); n++) accs[n] = 0.0;
   const double ch = A.sc->ch;
-  if (TL::TX > 1 && G.solve[0]) axis_pass<0, MAG, GLM, TL>(G, A, sm, t0, T, acc, accs, ch);
-  if (TL::TY > 1 && G.solve[1]) axis_pass<1, MAG, GLM, TL>(G, A, sm, t0, T, acc, accs, ch);
-  if (TL::TZ > 1 && G.solve[2]) axis_pass<2, MAG, GLM, TL>(G, A, sm, t0, T, acc, accs, ch);
+  if (TL::TX > 1 && G.solve[0]) axis_pass<0, MAG, GLM, TL, SPH>(G, A, sm, t0, T, acc, accs, ch);
+  if (TL::TY > 1 && G.solve[1]) axis_pass<1, MAG, GLM, TL, SPH>(G, A, sm, t0, T, acc, accs, ch);
+  if (TL::TZ > 1 && G.solve[2]) axis_pass<2, MAG, GLM, TL, SPH>(G, A, sm, t0, T, acc, accs, ch);
 
   // ---- RK combination (rungekutta.f90:35-59) + source (source.f90:70-85) -------
   if (tid >= TL::NC) return;
@@ -332,6 +354,35 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
     acc[3] = acc[3] + frc[2];
     acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
   }
+  if constexpr (SPH) {
+    // spherical geometric source terms (source.f90:113-143) from the stage's
+    // input primitives; ptot = p + B^2/2 as pressure (eos.f90:758-768)
+    const SphGeo& M = G.sph;
+    const double d = A.pin[c];
+    const double v1 = A.pin[PV * pl + c], v2 = A.pin[(PV + 1) * pl + c], v3 = A.pin[(PV + 2) * pl + c];
+    double pt = A.gm1 * A.pin[PEINT * pl + c];
+    double b1 = 0.0, b2 = 0.0, b3 = 0.0;
+    if (MAG) {
+      b1 = A.pin[PB * pl + c];
+      b2 = A.pin[(PB + 1) * pl + c];
+      b3 = A.pin[(PB + 2) * pl + c];
+      pt = pt + 0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
+    }
+    const double s1 = M.sx1[i + 2], sc = M.scot[j + 2];
+    double r1 = (d * (v2 * v2 + v3 * v3) + 2.0 * pt) * s1;
+    double r2 = G.solve[1] ? (-(d * v1 * v2) + (d * (v3 * v3) + pt) * sc) * s1 : 0.0;
+    double r3 = (-(d * v1 * v3) - d * v2 * v3 * sc) * s1;
+    if (MAG) {
+      r1 = r1 - (b2 * b2 + b3 * b3) * s1;
+      r2 = r2 + (b1 * b2 - b3 * b3 * sc) * s1;
+      r3 = r3 + (b1 * b3 + b2 * b3 * sc) * s1;
+      acc[6] = acc[6] + (b2 * v1 - b1 * v2) * s1;
+      acc[7] = acc[7] + ((v2 * b3 - b2 * v3) * sc - (b1 * v3 - b3 * v1)) * s1;
+    }
+    acc[1] = acc[1] + r1;
+    acc[2] = acc[2] + r2;
+    acc[3] = acc[3] + r3;
+  }
   const double dtf = A.fact * A.sc->dt;
   double un[9];
 #pragma unroll
@@ -375,12 +426,12 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
   }
 }
 
-template <bool MAG, bool GLM, class TL>
+template <bool MAG, bool GLM, class TL, bool SPH = false>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G, const StageArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
   if (A.sc->done) return;
-  stage_tile_exact<MAG, GLM, TL>(G, A, sm, blockIdx.x, nullptr);
+  stage_tile_exact<MAG, GLM, TL, SPH>(G, A, sm, blockIdx.x, nullptr);
 }
 
 // the same stage with the stencil region staged by TMA (3-D tiles)
@@ -463,9 +514,19 @@ __device__ __forceinline__ bool cfl_cell(const GridDev& G, const double* P, size
     cf3 = cs + fabs(v3);
   }
   const double dxi1 = G.g[0].dxi[i + 2], dxi2 = G.g[1].dxi[j + 2], dxi3 = G.g[2].dxi[k + 2];
-  const double dvol = dxi1 * dxi2 * dxi3;  // metric.f90:45-48
-  const double sa1 = dxi2 * dxi3, sa2 = dxi1 * dxi3, sa3 = dxi1 * dxi2;
-  dti = dvol / (cf1 * off0 * (sa1 + sa1) + cf2 * off1 * (sa2 + sa2) + cf3 * off2 * (sa3 + sa3));
+  if (G.sph.on) {  // metric.f90:117-130
+    const SphGeo& M = G.sph;
+    const double cd = M.cd[j + 2], fj = M.fac_j, fk = M.fac_k, ar = M.ar2[i + 2];
+    const double dvol = M.vr[i + 2] * cd * dxi3 * fj * fk;
+    const double sa1m = M.hr2[i + 1] * cd * dxi3 * fj * fk, sa1p = M.hr2[i + 2] * cd * dxi3 * fj * fk;
+    const double sa2m = 0.5 * M.sini[j + 1] * ar * dxi3 * fk, sa2p = 0.5 * M.sini[j + 2] * ar * dxi3 * fk;
+    const double sa3 = 0.5 * ar * dxi2 * fj;
+    dti = dvol / (cf1 * off0 * (sa1m + sa1p) + cf2 * off1 * (sa2m + sa2p) + cf3 * off2 * (sa3 + sa3));
+  } else {
+    const double dvol = dxi1 * dxi2 * dxi3;  // metric.f90:45-48
+    const double sa1 = dxi2 * dxi3, sa2 = dxi1 * dxi3, sa3 = dxi1 * dxi2;
+    dti = dvol / (cf1 * off0 * (sa1 + sa1) + cf2 * off1 * (sa2 + sa2) + cf3 * off2 * (sa3 + sa3));
+  }
   cfm = fmax2(fmax2(cf1, cf2), cf3);
   return true;
 }
@@ -575,6 +636,42 @@ __global__ void advance_kernel(DevScalars* sc) {
 // ---------------------------------------------------------------------------
 // host-side launchers (called from hmn_capi.cu)
 
+// spherical grids: the plain (non-TMA) FP64 kernel with the metric factors
+template <bool MAG, bool GLM, class TL>
+static cudaError_t launch_stage_sph(const GridDev& G, const StageArgs& A, cudaStream_t st) {
+  constexpr int smem = (int)sizeof(SmemT<TL>);
+  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e =
+        cudaFuncSetAttribute(stage_kernel<MAG, GLM, TL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  stage_kernel<MAG, GLM, TL, true><<<blocks, TL::NT, smem, st>>>(G, A);
+  return cudaGetLastError();
+}
+
+// r always solved; 1-D grids carry no GLM wave, 2-D and 3-D MHD grids do
+template <class TL>
+static cudaError_t launch_stage_sph_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  constexpr bool multi = (TL::TY > 1) || (TL::TZ > 1);
+  if (mag && glm != multi) return cudaErrorInvalidValue;
+  if (!mag) return launch_stage_sph<false, false, TL>(G, A, st);
+  return launch_stage_sph<true, multi, TL>(G, A, st);
+}
+
+static cudaError_t launch_stage_spherical(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  const int* t = A.tile;
+  if (A.nspc > 0) return cudaErrorInvalidValue;
+  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_sph_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_sph_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_sph_tl<Tile<16, 16, 1, 288, 2>>(G, A, mag, glm, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_sph_tl<Tile<16, 1, 16, 288, 2>>(G, A, mag, glm, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_sph_tl<Tile<256, 1, 1, 288, 2>>(G, A, mag, glm, st);
+  return cudaErrorInvalidValue;
+}
+
 template <bool MAG, bool GLM, class TL>
 static cudaError_t launch_stage_t(const GridDev& G, const StageArgs& A, const TmaMaps* tm, cudaStream_t st) {
   constexpr int smem = (int)sizeof(SmemT<TL>);
@@ -636,6 +733,7 @@ void stage_tile(const int solve[3], int precision, int nspc, int tile[3]) {
 
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st) {
+  if (G.sph.on) return launch_stage_spherical(G, A, mag, glm, st);
   const int* t = A.tile;
   if (A.nspc > 0) {  // tiles with room for up to 4 passive scalars
     using S3 = Tile<8, 8, 4, 384, 2, 4>;

@@ -87,3 +87,38 @@ def polytrope(n=16):
     cfg = config.resolve("polytrope_cart", overrides=ov)
     prims, phi = ic.polytrope_n1(cfg, G.make_grid(cfg))
     return cfg, prims, phi
+
+
+def cell_volumes(cfg, grid):
+    """dvol of metric.f90 (norm weights of tests.f90)."""
+    if cfg.get("crdnt", 0) == 2:
+        return G.spherical_dvol(grid, cfg["n"])
+    n = cfg["n"]
+    return np.full((n[2], n[1], n[0]), grid[0]["dxi"][2] * grid[1]["dxi"][2] * grid[2]["dxi"][2])
+
+
+def spherical(n=(24, 16, 1), mag=True, seed=5, xi1s=0.0, imesh=0, limiter="modified_mc", bc_r=(1, 2)):
+    """A spherical polar grid (crdnt=2: r, theta, phi) holding a seeded,
+    perturbed over-pressured core with small random velocities and a
+    uniform field along the polar axis; the azimuthal components vanish on
+    the axis like sin(theta)."""
+    rng = np.random.default_rng(seed)
+    ov = dict(ie=n[0], je=n[1], ke=n[2], crdnt=2, mag_on=mag, gamma=1.6666666666666667, xi1s=xi1s, xi1e=1.0,
+              imesh=imesh, x1min=0.03, flux_limiter=limiter, t_end=1.0, dt_out=1.0, courant=0.8,
+              bc1is=bc_r[0], bc1iv=bc_r[0], bc1os=bc_r[1], bc1ov=bc_r[1])
+    cfg = config.resolve("spherical", overrides=ov)
+    grid = G.make_grid(cfg)
+    r = G.centres(grid, 0)[None, None, :]
+    th = G.centres(grid, 1)[None, :, None]
+    shape = (n[2], n[1], n[0])
+    prims = {k: np.zeros(shape) for k in ("d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi")}
+    prims["d"][:] = 1.0 + 0.2 * rng.random(shape)
+    prims["p"][:] = np.where(r < 0.3, 2.0, 0.5) * (1.0 + 0.1 * rng.random(shape))
+    prims["v1"][:] = 0.1 * rng.uniform(-1.0, 1.0, shape)
+    prims["v2"][:] = 0.1 * rng.uniform(-1.0, 1.0, shape)
+    prims["v3"][:] = 0.1 * np.sin(th) * rng.uniform(-1.0, 1.0, shape)
+    if mag:
+        prims["b1"][:] = 0.2 * np.cos(th) + 0.02 * rng.uniform(-1.0, 1.0, shape)
+        prims["b2"][:] = -0.2 * np.sin(th) + 0.02 * rng.uniform(-1.0, 1.0, shape)
+        prims["b3"][:] = 0.02 * np.sin(th) * rng.uniform(-1.0, 1.0, shape)
+    return cfg, prims

@@ -17,7 +17,7 @@ import norms
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 NAMES = [f"{k}_{d}" for k in ("sodshock", "briowushock") for d in "xyz"] + \
-        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability"]
+        [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability", "sedov_default"]
 NAMES = NAMES + [n + "_flat" for n in NAMES]
 
 
@@ -32,7 +32,7 @@ def test_gpu_matches_golden(name):
     s.close()
     for n in range(cfg["nspc"]):
         st[f"spc{n}"] = st["spc"][n]
-    res = norms.compare(st, gold, cfg)
+    res = norms.compare(st, gold, cfg, dvol=cases.cell_volumes(cfg, G.make_grid(cfg)))
     assert max(r["L2"] for r in res.values()) < cfg["test_tol"], res
     for lab, r in res.items():
         assert r["identical"], (lab, r)

@@ -193,3 +193,17 @@ def test_geometric_series_mesh():
                                               bc2is=3, bc2os=3, bc2iv=3, bc2ov=3))
     prims = ic.kelvin_helmholtz(cfg, G.make_grid(cfg), 2.0, 0.05)
     run_pair(cfg, prims, 10)
+
+
+@pytest.mark.parametrize("make", [lambda: cases.spherical((40, 1, 1), mag=True),
+                                  lambda: cases.spherical((24, 16, 1), mag=True),
+                                  lambda: cases.spherical((16, 12, 8), mag=False),
+                                  lambda: cases.spherical((20, 1, 8), mag=True, xi1s=0.1, imesh=1, bc_r=(3, 3)),
+                                  lambda: cases.spherical((21, 10, 4), mag=True, xi1s=0.2, limiter="minmod")],
+                         ids=["radial-mhd", "r-theta-mhd", "r-theta-phi", "r-phi-stretched", "shell-3d-minmod"])
+def test_spherical_coordinates(make):
+    """crdnt=2: metric-weighted flux divergence (rungekutta.f90:42-53),
+    geometric source terms (source.f90:113-143) and the spherical CFL
+    (timestep.f90:175-178 with metric.f90:117-130), bitwise vs the oracle."""
+    cfg, prims = make()
+    run_pair(cfg, prims, 12)

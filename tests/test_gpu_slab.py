@@ -40,6 +40,13 @@ def test_blast_reflective_three_slabs():
     run_both(cfg, prims, 3, 5)
 
 
+def test_spherical_phi_wedges():
+    """A spherical polar grid (crdnt=2) split along phi into two wedges: the
+    metric factors ride with the r and theta axes of every slab."""
+    cfg, prims = cases.spherical((16, 12, 8), mag=True, xi1s=0.2)
+    run_both(cfg, prims, 2, 5)
+
+
 def test_riemann_with_scalars():
     cfg, prims = cases.riemann3d(n=(12, 10, 8), bc=(3, 1, 0), nspc=2)
     run_both(cfg, prims, 2, 5)

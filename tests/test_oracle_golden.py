@@ -14,6 +14,7 @@ import pytest
 
 from hormone_b200 import config, grid as G, ic
 from oracle.oracle import Oracle
+import cases
 import norms
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -21,13 +22,6 @@ CASES = [f"{k}_{d}" for k in ("sodshock", "briowushock") for d in "xyz"] + \
         [f"orszagtang_{p}" for p in ("xy", "yz", "xz")] + ["KHinstability", "sedov_default"]
 CASES = CASES + [c + "_flat" for c in CASES]
 
-
-def cell_volumes(cfg, grid):
-    """dvol of metric.f90 for the norm weights."""
-    if cfg.get("crdnt", 0) == 2:
-        return G.spherical_dvol(grid, cfg["n"])
-    n = cfg["n"]
-    return np.full((n[2], n[1], n[0]), grid[0]["dxi"][2] * grid[1]["dxi"][2] * grid[2]["dxi"][2])
 
 
 def run_case(name):
@@ -61,7 +55,7 @@ def test_oracle_matches_golden(name):
     sim = {k: o.get(k) for k in ("d", "e", "v1", "v2", "v3", "b1", "b2", "b3", "phi")}
     for n in range(cfg["nspc"]):
         sim[f"spc{n}"] = o.get(f"spc{n}")
-    res = norms.compare(sim, gold, cfg, dvol=cell_volumes(cfg, G.make_grid(cfg)))
+    res = norms.compare(sim, gold, cfg, dvol=cases.cell_volumes(cfg, G.make_grid(cfg)))
     worst = max(r["L2"] for r in res.values())
     assert worst < cfg["test_tol"], res  # the reference's own criterion (tests.f90:170)
     for lab, r in res.items():
