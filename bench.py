@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope", "briowu"], default="ot3d",
+    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope", "briowu", "sedov"], default="ot3d",
                     help="ot3d: the headline (3-D Orszag-Tang 256^3); kh-batch: 512 uneven 2-D KH boxes batched vs "
                          "one at a time; serve: a Poisson request stream through the continuous-batching server; "
                          "polytrope: 192^3 self-gravitating polytrope with hyperbolic gravity")
@@ -684,6 +684,57 @@ def run_briowu(args, rank=0, world=1, local_rank=0):
     print(json.dumps(line), flush=True)
 
 
+def run_sedov(args, rank=0, world=1, local_rank=0):
+    """HORMONE's own spherical Sedov-Taylor test (sedov_default: 500 radial
+    cells of a spherical polar grid, gamma=1.4, modified MC, to t=0.3):
+    time to solution of the whole run on the device clock (hmn_run, FP64,
+    the form spherical grids run in) against the oracle's CPU run of the
+    same case.  Launch-bound like the Brio-Wu case."""
+    import torch
+
+    from hormone_b200 import config, grid as G, ic
+    from hormone_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    cfg = config.resolve("sedov_default test")
+    prims = ic.make(cfg, G.make_grid(cfg))
+    runs = []
+    for rep in range(max(1, args.warmup) + 1):
+        s = Simulation(cfg, prims)
+        stream = torch.cuda.ExternalStream(s.ctx.stream_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        s.run_device()
+        e1.record(stream)
+        e1.synchronize()
+        runs.append((e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3, s.tn, s.ctx.launches()))
+        s.close()
+    ms, wall, tn, launches = runs[-1]
+    cells = cfg["n"][0]
+    cpu = None
+    if not args.no_cpu:
+        from oracle.oracle import Oracle
+
+        o = Oracle(cfg)
+        o.set_prims(prims)
+        t0 = time.perf_counter()
+        o.start()
+        o.run()
+        el = time.perf_counter() - t0
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": cells * o.scalars()["tn"] / el, "unit": METRIC, "cores": cores, "kind": "port",
+               "sample": f"the whole run ({o.scalars()['tn']} steps, {el:.2f} s) of the CPU restatement"}
+    line = {"metric": METRIC, "value": cells * tn / (ms * 1e-3), "unit": METRIC, "n_gpus": 1, "steps": tn,
+            "warmup": max(1, args.warmup), "ms_per_step": ms / tn, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "sedov-spherical-500-cells-t0.3", "crdnt": 2, "gamma": 1.4,
+                       "limiter": "modified_mc", "l2": "inputs far smaller than L2 (a launch-bound parity case)"},
+            "time_to_solution_ms": {"fp64": ms, "fp64_wall": wall}, "gpu_launches": launches, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args, rank=0, world=1, local_rank=0):
     """The serving stream through the continuous-batching server.  With N
     ranks every request goes to one rank (split by cells, in arrival order
@@ -755,6 +806,8 @@ def main():
             run_polytrope(args, rank, world, local_rank)
         elif args.workload == "briowu":
             run_briowu(args, rank, world, local_rank)
+        elif args.workload == "sedov":
+            run_sedov(args, rank, world, local_rank)
         elif args.decomp == "slab" and world > 1:
             run_slab(args, rank, world, local_rank)
         else:
