@@ -18,6 +18,8 @@
 
 using namespace hmn;
 
+constexpr int kRunGraphSteps = 16;
+
 struct hmn_ctx {
   int n[3];
   int solve[3];
@@ -52,6 +54,12 @@ struct hmn_ctx {
   double* dir[3][2];         // Dirichlet ghost values per face (device)
   double* spcorg;            // passive scalars times density at RK stage 1
   double* xi1_h;             // host copy of the r faces xi1(is-2..ie+2) for the metric
+  // hmn_run's device loop as a CUDA graph of kRunGraphSteps steps, valid for
+  // the primitive-buffer parity and phidamp factor it was captured with
+  cudaGraphExec_t run_exec;
+  int run_pcur;
+  double run_phifac;
+  long long run_launches;    // kernel launches one replay makes
   double* sphbuf;            // spherical metric factors (SphGeo arrays)
   // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
   cudaStream_t cst;
@@ -428,6 +436,7 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
     cudaFree(ctx->gpsi[b]);
     cudaFree(ctx->gorg[b]);
   }
+  if (ctx->run_exec) cudaGraphExecDestroy(ctx->run_exec);
   cudaFree(ctx->geo);
   cudaFree(ctx->sphbuf);
   free(ctx->xi1_h);
@@ -440,12 +449,20 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   return HMN_OK;
 }
 
+// the captured device loop bakes in the grid description: drop it whenever
+// that changes
+static void drop_run_graph(hmn_ctx* ctx) {
+  if (ctx->run_exec) cudaGraphExecDestroy(ctx->run_exec);
+  ctx->run_exec = nullptr;
+}
+
 // metric.f90:102-151 for spherical polar coordinates: the caller's 1-D
 // factors plus the radial and polar products the kernels form the 2-D and
 // 3-D factors from (same single IEEE operations as the reference).
 extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, const double* idetg1, const double* sx1,
                               const double* sini, const double* cosi, const double* scot) {
   if (!ctx) return HMN_EINVAL;
+  drop_run_graph(ctx);
   if (crdnt == 0) {
     ctx->G.sph = SphGeo{};
     return HMN_OK;
@@ -686,6 +703,7 @@ extern "C" int hmn_set_dirichlet(hmn_ctx* ctx, int axis, int side, const double*
   CK(cudaMemcpyAsync(ctx->dir[axis][side], vals, m * sizeof(double), cudaMemcpyHostToDevice, ctx->st),
      "dirichlet");
   CK(cudaStreamSynchronize(ctx->st), "sync");
+  drop_run_graph(ctx);
   ctx->G.dir[axis][side] = ctx->dir[axis][side];
   return HMN_OK;
 }
@@ -705,6 +723,7 @@ extern "C" int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, cons
   if ((recv_lo && !send_lo) || (recv_hi && !send_hi)) return HMN_EINVAL;
   ctx->zsend[0] = send_lo;
   ctx->zsend[1] = send_hi;
+  drop_run_graph(ctx);
   ctx->G.zhalo[0] = recv_lo;
   ctx->G.zhalo[1] = recv_hi;
   ctx->G.zwrap[0] = recv_lo && wrap_lo ? 1 : 0;
@@ -1033,6 +1052,43 @@ static int enqueue_step(hmn_ctx* ctx) {
   return HMN_OK;
 }
 
+// kRunGraphSteps steps of the device loop as one graph launch.  Steps are
+// launch-bound on small grids (a few microseconds of work per kernel); the
+// graph removes the per-launch host cost.  The step count is even so that
+// an RK3 graph ends on the primitive buffer it starts on.
+static int run_graph_steps(hmn_ctx* ctx) {
+  if (!ctx->run_exec || ctx->run_pcur != ctx->pcur || ctx->run_phifac != ctx->phifac) {
+    drop_run_graph(ctx);
+    const int pcur = ctx->pcur;
+    const double phifac = ctx->phifac;
+    const long long launches = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal), "graph capture");
+    int rc = HMN_OK;
+    for (int s = 0; s < kRunGraphSteps && rc == HMN_OK; s++) rc = enqueue_step(ctx);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+    if (rc == HMN_OK && e == cudaSuccess && ctx->pcur == pcur && ctx->phifac == phifac)
+      e = cudaGraphInstantiate(&ctx->run_exec, g, 0);
+    else if (rc == HMN_OK)
+      rc = HMN_ECUDA;
+    if (g) cudaGraphDestroy(g);
+    ctx->run_launches = ctx->launches - launches;
+    ctx->launches = launches;
+    ctx->pcur = pcur;
+    ctx->phifac = phifac;
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+      ctx->run_exec = nullptr;
+      return cuda_fail(ctx, e, "graph instantiate");
+    }
+    ctx->run_pcur = pcur;
+    ctx->run_phifac = phifac;
+  }
+  CK(cudaGraphLaunch(ctx->run_exec, ctx->st), "graph launch");
+  ctx->launches += ctx->run_launches;
+  return HMN_OK;
+}
+
 extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, int* steps) {
   if (!ctx || !time) return HMN_EINVAL;
   if (slab_exchanges(ctx)) return HMN_EBADCFG;
@@ -1063,12 +1119,21 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
   const int tn0 = ctx->sc_h->tn;
   const int pcur0 = ctx->pcur;
   int done = 0;
-  const int chunk = ctx->par.rktype == 1 ? 1 : 8;  // rktype 1 swaps buffers on the host after each step
+  const bool graphs = ctx->par.rktype != 1;  // rktype 1 swaps buffers on the host after each step
+  const int chunk = graphs ? kRunGraphSteps : 1;
   while (done < max_steps) {
     int n = max_steps - done < chunk ? max_steps - done : chunk;
-    for (int s = 0; s < n; s++) {
-      rc = enqueue_step(ctx);
+    // the first step of a call runs plain: it settles the phidamp factor
+    // the later steps share
+    if (graphs && done > 0 && n == kRunGraphSteps) {
+      rc = run_graph_steps(ctx);
       if (rc) return rc;
+    } else {
+      if (done == 0 && graphs) n = 1;
+      for (int s = 0; s < n; s++) {
+        rc = enqueue_step(ctx);
+        if (rc) return rc;
+      }
     }
     done += n;
     rc = fetch_scalars(ctx);
