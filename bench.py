@@ -682,9 +682,10 @@ def run_briowu(args, rank=0, world=1, local_rank=0):
 def run_sedov(args, rank=0, world=1, local_rank=0):
     """HORMONE's own spherical Sedov-Taylor test (sedov_default: 500 radial
     cells of a spherical polar grid, gamma=1.4, modified MC, to t=0.3):
-    time to solution of the whole run on the device clock (hmn_run, FP64,
-    the form spherical grids run in) against the oracle's CPU run of the
-    same case.  Launch-bound like the Brio-Wu case."""
+    time to solution of the whole run on the device clock (hmn_run), FP64
+    and mixed, against the oracle's CPU run of the same case.  Launch-bound
+    like the Brio-Wu case."""
+    import numpy as np
     import torch
 
     from hormone_b200 import config, grid as G, ic
@@ -693,20 +694,25 @@ def run_sedov(args, rank=0, world=1, local_rank=0):
     torch.cuda.set_device(local_rank)
     cfg = config.resolve("sedov_default test")
     prims = ic.make(cfg, G.make_grid(cfg))
-    runs = []
-    for rep in range(max(1, args.warmup) + 1):
-        s = Simulation(cfg, prims)
-        stream = torch.cuda.ExternalStream(s.ctx.stream_ptr())
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0 = time.perf_counter()
-        e0.record(stream)
-        s.run_device()
-        e1.record(stream)
-        e1.synchronize()
-        runs.append((e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3, s.tn, s.ctx.launches()))
-        s.close()
-    ms, wall, tn, launches = runs[-1]
+    out = {}
+    for prec in (0, 1):
+        runs = []
+        for rep in range(max(1, args.warmup) + 1):
+            s = Simulation(cfg, prims, precision=prec)
+            stream = torch.cuda.ExternalStream(s.ctx.stream_ptr())
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            s.run_device()
+            e1.record(stream)
+            e1.synchronize()
+            runs.append((e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3, s.tn, s.ctx.launches()))
+            d = s.state()["d"]
+            s.close()
+        out[prec] = runs[-1] + (d,)
+    ms, wall, tn, launches, d0 = out[0]
+    l1 = float(np.sum(np.abs(out[1][4] - d0)) / np.sum(np.abs(d0)))
     cells = cfg["n"][0]
     cpu = None
     if not args.no_cpu:
@@ -726,7 +732,8 @@ def run_sedov(args, rank=0, world=1, local_rank=0):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "sedov-spherical-500-cells-t0.3", "crdnt": 2, "gamma": 1.4,
                        "limiter": "modified_mc", "l2": "inputs far smaller than L2 (a launch-bound parity case)"},
-            "time_to_solution_ms": {"fp64": ms, "fp64_wall": wall}, "gpu_launches": launches, "cpu_baseline": cpu}
+            "time_to_solution_ms": {"fp64": ms, "mixed": out[1][0], "fp64_wall": wall},
+            "mixed_l1_rho_vs_fp64": l1, "gpu_launches": launches, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
 
 

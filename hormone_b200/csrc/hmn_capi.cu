@@ -469,9 +469,8 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, cons
   }
   if (crdnt != 2) return HMN_EBADCFG;
   if (!detg1 || !idetg1 || !sx1 || !sini || !cosi || !scot) return HMN_EINVAL;
-  // the FP64 form of single grids without gravity or passive scalars; r solved
-  if (ctx->par.precision != 0 || ctx->par.gravswitch != 0 || ctx->par.nspc != 0 || !ctx->solve[0])
-    return HMN_EBADCFG;
+  // single grids without gravity or passive scalars (either precision); r solved
+  if (ctx->par.gravswitch != 0 || ctx->par.nspc != 0 || !ctx->solve[0]) return HMN_EBADCFG;
   const int L1 = ctx->n[0] + 4, L2 = ctx->n[1] + 4;
   std::vector<double> h((size_t)6 * L1 + (size_t)4 * L2, 0.0);
   double *g1 = h.data(), *ig1 = g1 + L1, *s1 = ig1 + L1, *vr = s1 + L1, *hr2 = vr + L1, *ar2 = hr2 + L1;

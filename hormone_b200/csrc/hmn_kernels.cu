@@ -241,24 +241,10 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
       const int wp = wm + FSTR;
       constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
       if constexpr (SPH) {
-        // idetg1 (detg1 F)(i-1) - ..., idetg2 (sin F)(j-1) - ..., idetg3 (F(k-1) - F(k))
-        // with idetg2 = sx1 / (cos(j-1) - cos(j)) and idetg3 = idetg2 dxi2 / dxi3 / fac_k
-        // (rungekutta.f90:42-53, metric.f90:105-125)
-        const SphGeo& M = G.sph;
-        const int i = cx + t0[0], j = cy + t0[1], k = cz + t0[2];
-        if constexpr (AX == 0) {
-          const double cw = M.idetg1[i + 2], fm = M.detg1[i + 1], fp = M.detg1[i + 2];
+        double cw, fm, fp;
+        sph_div_weights<AX>(G, cx + t0[0], cy + t0[1], cz + t0[2], cw, fm, fp);
 #pragma unroll
-          for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (fm * sm.F[q][wm] - fp * sm.F[q][wp]);
-        } else if constexpr (AX == 1) {
-          const double cw = M.ra2[j + 2] * M.sx1[i + 2], fm = M.sini[j + 1], fp = M.sini[j + 2];
-#pragma unroll
-          for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (fm * sm.F[q][wm] - fp * sm.F[q][wp]);
-        } else {
-          const double cw = M.ra2[j + 2] * M.sx1[i + 2] * G.g[1].dxi[j + 2] * G.g[2].idxi[k + 2] / M.fac_k;
-#pragma unroll
-          for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (sm.F[q][wm] - sm.F[q][wp]);
-        }
+        for (int q = 0; q < nv; q++) acc[q] = acc[q] + cw * (fm * sm.F[q][wm] - fp * sm.F[q][wp]);
       } else {
         const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
 #pragma unroll
@@ -354,35 +340,7 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
     acc[3] = acc[3] + frc[2];
     acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
   }
-  if constexpr (SPH) {
-    // spherical geometric source terms (source.f90:113-143) from the stage's
-    // input primitives; ptot = p + B^2/2 as pressure (eos.f90:758-768)
-    const SphGeo& M = G.sph;
-    const double d = A.pin[c];
-    const double v1 = A.pin[PV * pl + c], v2 = A.pin[(PV + 1) * pl + c], v3 = A.pin[(PV + 2) * pl + c];
-    double pt = A.gm1 * A.pin[PEINT * pl + c];
-    double b1 = 0.0, b2 = 0.0, b3 = 0.0;
-    if (MAG) {
-      b1 = A.pin[PB * pl + c];
-      b2 = A.pin[(PB + 1) * pl + c];
-      b3 = A.pin[(PB + 2) * pl + c];
-      pt = pt + 0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
-    }
-    const double s1 = M.sx1[i + 2], sc = M.scot[j + 2];
-    double r1 = (d * (v2 * v2 + v3 * v3) + 2.0 * pt) * s1;
-    double r2 = G.solve[1] ? (-(d * v1 * v2) + (d * (v3 * v3) + pt) * sc) * s1 : 0.0;
-    double r3 = (-(d * v1 * v3) - d * v2 * v3 * sc) * s1;
-    if (MAG) {
-      r1 = r1 - (b2 * b2 + b3 * b3) * s1;
-      r2 = r2 + (b1 * b2 - b3 * b3 * sc) * s1;
-      r3 = r3 + (b1 * b3 + b2 * b3 * sc) * s1;
-      acc[6] = acc[6] + (b2 * v1 - b1 * v2) * s1;
-      acc[7] = acc[7] + ((v2 * b3 - b2 * v3) * sc - (b1 * v3 - b3 * v1)) * s1;
-    }
-    acc[1] = acc[1] + r1;
-    acc[2] = acc[2] + r2;
-    acc[3] = acc[3] + r3;
-  }
+  if constexpr (SPH) sph_sources<MAG>(G, A, c, i, j, acc);
   const double dtf = A.fact * A.sc->dt;
   double un[9];
 #pragma unroll

@@ -65,7 +65,7 @@ __device__ __forceinline__ double minmod_fast(double u0, double u1, double u2, d
   return s * fmax2(0.0, m);
 }
 
-template <int AX, bool MAG, bool GLM, class TL>
+template <int AX, bool MAG, bool GLM, class TL, bool SPH = false>
 __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArgs& A, SmemMixed<TL>& sm,
                                                 const int t0[3], const int T[3], double acc[9], float ch) {
   constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ;
@@ -224,10 +224,18 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
     if (cx < T[0] && cy < T[1] && cz < T[2]) {
       const int wm = cx + FBX * (cy + FBY * cz);
       const int wp = wm + FSTR;
-      const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
       constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
+      if constexpr (SPH) {  // FP64 metric weights on the FP32 fluxes
+        double cw, fm, fp;
+        sph_div_weights<AX>(G, cx + t0[0], cy + t0[1], cz + t0[2], cw, fm, fp);
 #pragma unroll
-      for (int q = 0; q < nv; q++) acc[q] = acc[q] + idxi * ((double)sm.F[q][wm] - (double)sm.F[q][wp]);
+        for (int q = 0; q < nv; q++)
+          acc[q] = acc[q] + cw * (fm * (double)sm.F[q][wm] - fp * (double)sm.F[q][wp]);
+      } else {
+        const double idxi = g.idxi[cc[AX] + t0[AX] + 2];
+#pragma unroll
+        for (int q = 0; q < nv; q++) acc[q] = acc[q] + idxi * ((double)sm.F[q][wm] - (double)sm.F[q][wp]);
+      }
     }
   }
   __syncthreads();
@@ -235,7 +243,7 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
 
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
 // (x fastest).  Shared by the single-grid and the batched kernels.
-template <bool MAG, bool GLM, class TL>
+template <bool MAG, bool GLM, class TL, bool SPH = false>
 __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageArgs& A, SmemMixed<TL>& sm, int tile_id,
                                                  const TmaMaps* tm) {
   const int tid = threadIdx.x;
@@ -254,9 +262,9 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
 #pragma unroll
   for (int q = 0; q < 9; q++) acc[q] = 0.0;
   const float ch = (float)A.sc->ch;
-  if (TL::TX > 1 && G.solve[0]) axis_pass_mixed<0, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
-  if (TL::TY > 1 && G.solve[1]) axis_pass_mixed<1, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
-  if (TL::TZ > 1 && G.solve[2]) axis_pass_mixed<2, MAG, GLM, TL>(G, A, sm, t0, T, acc, ch);
+  if (TL::TX > 1 && G.solve[0]) axis_pass_mixed<0, MAG, GLM, TL, SPH>(G, A, sm, t0, T, acc, ch);
+  if (TL::TY > 1 && G.solve[1]) axis_pass_mixed<1, MAG, GLM, TL, SPH>(G, A, sm, t0, T, acc, ch);
+  if (TL::TZ > 1 && G.solve[2]) axis_pass_mixed<2, MAG, GLM, TL, SPH>(G, A, sm, t0, T, acc, ch);
 
   if (tid >= TL::NC) return;
   const int cx = tid % TL::TX, cy = (tid / TL::TX) % TL::TY, cz = tid / (TL::TX * TL::TY);
@@ -299,6 +307,7 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
     acc[3] = acc[3] + frc[2];
     acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
   }
+  if constexpr (SPH) sph_sources<MAG>(G, A, c, i, j, acc);  // geometric sources in FP64
   const double dtf = A.fact * A.sc->dt;
   double un[9];
 #pragma unroll
@@ -335,12 +344,12 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
   }
 }
 
-template <bool MAG, bool GLM, class TL>
+template <bool MAG, bool GLM, class TL, bool SPH = false>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel_mixed(const GridDev G, const StageArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
   if (A.sc->done) return;
-  stage_tile_mixed<MAG, GLM, TL>(G, A, sm, blockIdx.x, nullptr);
+  stage_tile_mixed<MAG, GLM, TL, SPH>(G, A, sm, blockIdx.x, nullptr);
 }
 
 // the same stage with the stencil region staged by TMA (3-D tiles)
@@ -390,8 +399,44 @@ static cudaError_t launch_mixed_tl(const GridDev& G, const StageArgs& A, bool ma
   return launch_mixed_t<false, false, TL>(G, A, tm, st);
 }
 
+// spherical grids: the plain (non-TMA) mixed kernel with the metric factors
+template <bool MAG, bool GLM, class TL>
+static cudaError_t launch_mixed_sph(const GridDev& G, const StageArgs& A, cudaStream_t st) {
+  constexpr int smem = (int)sizeof(SmemMixed<TL>);
+  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel_mixed<MAG, GLM, TL, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  stage_kernel_mixed<MAG, GLM, TL, true><<<blocks, TL::NT, smem, st>>>(G, A);
+  return cudaGetLastError();
+}
+
+// r always solved; 1-D grids carry no GLM wave, 2-D and 3-D MHD grids do
+template <class TL>
+static cudaError_t launch_mixed_sph_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  constexpr bool multi = (TL::TY > 1) || (TL::TZ > 1);
+  if (mag && glm != multi) return cudaErrorInvalidValue;
+  if (!mag) return launch_mixed_sph<false, false, TL>(G, A, st);
+  return launch_mixed_sph<true, multi, TL>(G, A, st);
+}
+
+static cudaError_t launch_mixed_spherical(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  const int* t = A.tile;
+  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_mixed_sph_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_mixed_sph_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_mixed_sph_tl<Tile<16, 16, 1, 288, 2>>(G, A, mag, glm, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_mixed_sph_tl<Tile<16, 1, 16, 288, 2>>(G, A, mag, glm, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_mixed_sph_tl<Tile<256, 1, 1, 288, 2>>(G, A, mag, glm, st);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                                cudaStream_t st) {
+  if (G.sph.on) return launch_mixed_spherical(G, A, mag, glm, st);
   const int* t = A.tile;
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_mixed_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
   if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_mixed_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, tm, st);

@@ -466,4 +466,61 @@ __device__ __forceinline__ StageArgs batch_stage_args(SimDesc& S, int stage, int
 // 2 = 1-D x 256
 constexpr int kBatchKinds = 3;
 
+// Spherical metric weights of the flux divergence of cell (i,j,k) along AX
+// (rungekutta.f90:42-53 with metric.f90:105-125): the cell adds
+// cw (fm F(low face) - fp F(high face)).  Along phi the reference has no face
+// factor; fm = fp = 1 there, and multiplying by one is exact.
+template <int AX>
+__device__ __forceinline__ void sph_div_weights(const GridDev& G, int i, int j, int k, double& cw, double& fm,
+                                                double& fp) {
+  const SphGeo& M = G.sph;
+  if constexpr (AX == 0) {  // idetg1, detg1 = xi1^2
+    cw = M.idetg1[i + 2];
+    fm = M.detg1[i + 1];
+    fp = M.detg1[i + 2];
+  } else if constexpr (AX == 1) {  // idetg2 = 1/(cos(j-1) - cos(j)) * sx1, detg2 = sin
+    cw = M.ra2[j + 2] * M.sx1[i + 2];
+    fm = M.sini[j + 1];
+    fp = M.sini[j + 2];
+  } else {  // idetg3 = idetg2 * dxi2 * idxi3 / fac_k
+    cw = M.ra2[j + 2] * M.sx1[i + 2] * G.g[1].dxi[j + 2] * G.g[2].idxi[k + 2] / M.fac_k;
+    fm = 1.0;
+    fp = 1.0;
+  }
+}
+
+// Spherical geometric source terms (source.f90:113-143) of cell c, from the
+// stage's input primitives with ptot = p + B^2/2 as `pressure` forms it
+// (eos.f90:758-768), added to the flux divergence in acc[].
+template <bool MAG>
+__device__ __forceinline__ void sph_sources(const GridDev& G, const StageArgs& A, size_t c, int i, int j,
+                                            double acc[9]) {
+  const SphGeo& M = G.sph;
+  const size_t pl = A.plane;
+  const double d = A.pin[c];
+  const double v1 = A.pin[PV * pl + c], v2 = A.pin[(PV + 1) * pl + c], v3 = A.pin[(PV + 2) * pl + c];
+  double pt = A.gm1 * A.pin[PEINT * pl + c];
+  double b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  if (MAG) {
+    b1 = A.pin[PB * pl + c];
+    b2 = A.pin[(PB + 1) * pl + c];
+    b3 = A.pin[(PB + 2) * pl + c];
+    pt = pt + 0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
+  }
+  const double s1 = M.sx1[i + 2], sc = M.scot[j + 2];
+  double r1 = (d * (v2 * v2 + v3 * v3) + 2.0 * pt) * s1;
+  double r2 = G.solve[1] ? (-(d * v1 * v2) + (d * (v3 * v3) + pt) * sc) * s1 : 0.0;
+  double r3 = (-(d * v1 * v3) - d * v2 * v3 * sc) * s1;
+  if (MAG) {
+    r1 = r1 - (b2 * b2 + b3 * b3) * s1;
+    r2 = r2 + (b1 * b2 - b3 * b3 * sc) * s1;
+    r3 = r3 + (b1 * b3 + b2 * b3 * sc) * s1;
+    acc[6] = acc[6] + (b2 * v1 - b1 * v2) * s1;
+    acc[7] = acc[7] + ((v2 * b3 - b2 * v3) * sc - (b1 * v3 - b3 * v1)) * s1;
+  }
+  acc[1] = acc[1] + r1;
+  acc[2] = acc[2] + r2;
+  acc[3] = acc[3] + r3;
+}
+
 }  // namespace hmn

@@ -75,8 +75,8 @@ int hmn_create(const hmn_grid* grid, const hmn_params* params, hmn_ctx** out);
  * detg1, idetg1, sx1 cover is-2..ie+2 and sini, cosi, scot js-2..je+2, as
  * module `grid` holds them after `metric`; the kernels form idetg2, idetg3,
  * dvol and sa1..3 from them in the reference's operation order.  crdnt 0
- * (Cartesian, the default) takes no arrays.  Spherical grids run on the FP64
- * form of single grids with r solved and without gravity or passive
+ * (Cartesian, the default) takes no arrays.  Spherical grids run as single
+ * grids (either precision) with r solved and without gravity or passive
  * scalars (HMN_EBADCFG otherwise).  Call before the first step. */
 int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, const double* idetg1, const double* sx1,
                    const double* sini, const double* cosi, const double* scot);

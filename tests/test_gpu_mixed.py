@@ -42,7 +42,9 @@ def one_step_l1(cfg, prims, warm=3):
 
 
 @pytest.mark.parametrize("make", [lambda: cases.ot3d(32), lambda: cases.kh2d(64), lambda: cases.blast3d(16, bc=2),
-                                  lambda: cases.golden_case("briowushock_x")])
+                                  lambda: cases.golden_case("briowushock_x"),
+                                  lambda: cases.spherical((16, 12, 8), mag=True, xi1s=0.2),
+                                  lambda: cases.golden_case("sedov_default")])
 def test_mixed_one_step_error(make):
     cfg, prims = make()
     l1 = one_step_l1(cfg, prims)
@@ -82,7 +84,7 @@ def l1_rel(a, b):
 # away by t=0.5 on Orszag-Tang.  The bounds below are that sensitivity with a
 # margin; the per-step bound of 1e-6 is test_mixed_one_step_error.
 @pytest.mark.parametrize("name,tol", [("briowushock_x", 2e-3), ("sodshock_x", 2e-3), ("briowushock_y", 2e-3),
-                                      ("orszagtang_xy", 2e-2)])
+                                      ("orszagtang_xy", 2e-2), ("sedov_default", 2e-3)])
 def test_mixed_whole_run_against_fp64(name, tol):
     cfg, prims = cases.golden_case(name)
     a = run_to_end(cfg, prims, 0)
