@@ -39,6 +39,10 @@ class HmnParams(ctypes.Structure):
                 ("nspc", _I)]
 
 
+class HmnMetric(ctypes.Structure):
+    _fields_ = [(k, _DP) for k in ("detg1", "idetg1", "sx1", "sini", "cosi", "scot", "sinc", "sisin")]
+
+
 class HmnError(RuntimeError):
     def __init__(self, code, where="", cell=None):
         self.code = code
@@ -84,7 +88,7 @@ def lib():
         L.hmn_checkpoint_begin.argtypes = [_P, _DP, _DPP, _DP, _DP, _DP]
         L.hmn_upload_scalars.argtypes = [_P, _DP]
         L.hmn_set_dirichlet.argtypes = [_P, _I, _I, _DP]
-        L.hmn_set_metric.argtypes = [_P, _I] + [_DP] * 6
+        L.hmn_set_metric.argtypes = [_P, _I, ctypes.POINTER(HmnMetric)]
         L.hmn_download_scalars.argtypes = [_P, _DP]
         L.hmn_checkpoint_wait.argtypes = [_P]
         L.hmn_stream.argtypes = [_P]
@@ -169,10 +173,16 @@ class Context:
 
     def set_metric(self, grid):
         """Spherical metric factors (metric.f90:102-151) from the grid's
-        ``detg``/``idetg``/``sx`` (r) and ``sini``/``cosi``/``scot`` (theta)."""
-        arrs = [np.ascontiguousarray(grid[a][k], dtype=np.float64)
-                for a, k in ((0, "detg"), (0, "idetg"), (0, "sx"), (1, "sini"), (1, "cosi"), (1, "scot"))]
-        self._check(lib().hmn_set_metric(self.h, 2, *[_dp(v) for v in arrs]), "hmn_set_metric")
+        ``detg``/``idetg``/``sx`` (r) and ``sini``/``cosi``/``scot``/``sinc``/
+        ``sisin`` (theta)."""
+        m = HmnMetric()
+        self._metric_arrays = []
+        for field, a, k in (("detg1", 0, "detg"), ("idetg1", 0, "idetg"), ("sx1", 0, "sx"), ("sini", 1, "sini"),
+                            ("cosi", 1, "cosi"), ("scot", 1, "scot"), ("sinc", 1, "sinc"), ("sisin", 1, "sisin")):
+            v = np.ascontiguousarray(grid[a][k], dtype=np.float64)
+            self._metric_arrays.append(v)
+            setattr(m, field, _dp(v))
+        self._check(lib().hmn_set_metric(self.h, 2, ctypes.byref(m)), "hmn_set_metric")
 
     def close(self):
         if getattr(self, "h", None):

@@ -260,10 +260,16 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
         raise ValueError("passive scalars on spherical grids are not on this path")
     grav = int(cfg.get("gravswitch", 0))
     if crdnt == 2 and grav:
-        raise ValueError("self-gravity on spherical grids is not on this path")
+        # setup_grv_hyperbolic (gravity_hyperbolic.f90:336-405) has spherical
+        # coefficients for (r, theta) with one phi cell and for 3-D grids; the
+        # outer radius takes the Robin condition (gbtype 1) here
+        if grav != 3 or not (solve[0] and solve[1]):
+            raise ValueError("spherical self-gravity needs gravswitch 3 on an (r, theta) or 3-D grid")
+        if int(cfg.get("gbtype", 0)) != 1:
+            raise ValueError("spherical self-gravity takes the Robin outer boundary (gbtype=1) on this path")
     if grav not in (0, 3):
         raise ValueError("only gravswitch 0 (off) or 3 (hyperbolic) is on this path")
-    if grav == 3 and dim != 3:
+    if grav == 3 and dim != 3 and crdnt == 0:
         raise ValueError("the Cartesian hyperbolic gravity solver needs a 3-D grid")
     extent = [(float(cfg["xi1s"]), float(cfg["xi1e"])), (float(cfg["xi2s"]), float(cfg["xi2e"])),
               (float(cfg["xi3s"]), float(cfg["xi3e"]))]

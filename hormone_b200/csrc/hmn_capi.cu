@@ -53,7 +53,11 @@ struct hmn_ctx {
   double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
   double* dir[3][2];         // Dirichlet ghost values per face (device)
   double* spcorg;            // passive scalars times density at RK stage 1
-  double* xi1_h;             // host copy of the r faces xi1(is-2..ie+2) for the metric
+  double* xi1_h;             // host copies of the grid arrays the metric set-up needs
+  double* axis_h;            // x, dx, dxi, idx of the three axes, (n+4) each
+  double* hgc;               // spherical Laplacian coefficients: 8 planes
+  double* gin;               // potential beyond r = xi1s after the last boundary pass (n1*n2)
+  double xi1s;
   // hmn_run's device loop as a CUDA graph of kRunGraphSteps steps, valid for
   // the primitive-buffer parity and phidamp factor it was captured with
   cudaGraphExec_t run_exec;
@@ -260,7 +264,7 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
       return HMN_EBADCFG;
     }
   }
-  if (par->gravswitch == 3 && ctx->dim != 3) {
+  if (par->gravswitch == 3 && ctx->dim < 2) {  // 3-D Cartesian, or spherical (r, theta) / 3-D (hmn_set_metric)
     delete ctx;
     return HMN_EBADCFG;
   }
@@ -312,12 +316,23 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     off += (size_t)kA * L;
   }
   ctx->xi1_h = (double*)malloc((size_t)(ctx->n[0] + 4) * sizeof(double));
-  if (!ctx->xi1_h) {
+  ctx->axis_h = (double*)malloc((size_t)4 * (ctx->n[0] + ctx->n[1] + ctx->n[2] + 12) * sizeof(double));
+  if (!ctx->xi1_h || !ctx->axis_h) {
+    free(ctx->xi1_h);
+    free(ctx->axis_h);
     cudaStreamDestroy(ctx->st);
     delete ctx;
     return HMN_ENOMEM;
   }
   memcpy(ctx->xi1_h, grid->xi[0], (size_t)(ctx->n[0] + 4) * sizeof(double));
+  {
+    double* h = ctx->axis_h;
+    for (int a = 0; a < 3; a++) {
+      const size_t L = (size_t)ctx->n[a] + 4;
+      const double* src[4] = {grid->x[a], grid->dx[a], grid->dxi[a], grid->idx[a]};
+      for (int q = 0; q < 4; q++, h += L) memcpy(h, src[q], L * sizeof(double));
+    }
+  }
   size_t bytes = ctx->plane * sizeof(double);
   int nplanes = 9;  // every RK buffer can also hold the 9 primitive planes
   e = cudaMalloc((void**)&ctx->geo, geo_len * sizeof(double));
@@ -439,7 +454,10 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   if (ctx->run_exec) cudaGraphExecDestroy(ctx->run_exec);
   cudaFree(ctx->geo);
   cudaFree(ctx->sphbuf);
+  cudaFree(ctx->hgc);
+  cudaFree(ctx->gin);
   free(ctx->xi1_h);
+  free(ctx->axis_h);
   cudaFree(ctx->prim_out);
   cudaFree(ctx->sc);
   if (ctx->sc_h) cudaFreeHost(ctx->sc_h);
@@ -456,11 +474,66 @@ static void drop_run_graph(hmn_ctx* ctx) {
   ctx->run_exec = nullptr;
 }
 
+// host copy of axis a's array q (0 x, 1 dx, 2 dxi, 3 idx), offset +2
+static const double* host_axis(const hmn_ctx* ctx, int a, int q) {
+  const double* h = ctx->axis_h;
+  for (int b = 0; b < a; b++) h += (size_t)4 * (ctx->n[b] + 4);
+  return h + (size_t)q * (ctx->n[a] + 4) + 2;
+}
+
+// setup_grv_hyperbolic (gravity_hyperbolic.f90:336-405) on a spherical grid:
+// lap_coeff(0..3) and the normalisation lap_coeff(-1) at coefficient index
+// (i,j,k) >= -1, in the reference's operation order (the axisymmetric form
+// for one phi cell, the 3-D form otherwise; Robin outer radius, gbtype 1)
+static void sph_lap_coeffs(const hmn_ctx* ctx, const double* sinc, const double* sini, int i, int j, int k,
+                           double c[5]) {
+  const double *x1 = host_axis(ctx, 0, 0), *dx1 = host_axis(ctx, 0, 1), *dxi1 = host_axis(ctx, 0, 2);
+  const double *dx2 = host_axis(ctx, 1, 1), *dxi2 = host_axis(ctx, 1, 2);
+  const double *dx3 = host_axis(ctx, 2, 1), *dxi3 = host_axis(ctx, 2, 2), *idx3 = host_axis(ctx, 2, 3);
+  const double* xi1 = ctx->xi1_h + 2;
+  const int gie = ctx->n[0] - 1, gje = ctx->n[1] - 1;
+  const double a = xi1[i], b = xi1[i - 1];
+  if (ctx->n[2] == 1) {  // :336-363
+    c[0] = -((a * a / dx1[i + 1] + b * b / dx1[i]) * sinc[j] * dxi2[j] +
+             (sini[j] / dx2[j + 1] + sini[j - 1] / dx2[j]) * dxi1[i]);
+    c[1] = a * a * sinc[j] * dxi2[j] / dx1[i + 1];
+    c[2] = sini[j] * dxi1[i] / dx2[j + 1];
+    c[3] = 0.0;
+    if (i == 0 && ctx->xi1s > 0.0) c[0] = c[0] + b * b * sinc[j] * dxi2[j] / dx1[i];
+    if (i == gie) {
+      c[0] = c[0] + c[1] * x1[i] / x1[i + 1];
+      c[1] = 0.0;
+    }
+    if (j == gje) {
+      c[0] = c[0] + c[2];
+      c[2] = 0.0;
+    }
+    c[4] = x1[i] * x1[i] * sinc[j] * dxi1[i] * dxi2[j];
+  } else {  // :367-400
+    c[0] = -((a * a / dx1[i + 1] + b * b / dx1[i]) * sinc[j] * dxi2[j] * dxi3[k] +
+             (sini[j] / dx2[j + 1] + sini[j - 1] / dx2[j]) * dxi1[i] * dxi3[k] +
+             (idx3[k] + idx3[k + 1]) * dxi1[i] * dxi2[j]);
+    c[1] = a * a * sinc[j] * dxi2[j] * dxi3[k] / dx1[i + 1];
+    c[2] = sini[j] * dxi1[i] * dxi3[k] / dx2[j + 1];
+    c[3] = dxi1[i] * dxi2[j] / dx3[k + 1];
+    if (j == gje) {
+      c[0] = c[0] + c[2];
+      c[2] = 0.0;
+    }
+    if (i == 0 && ctx->xi1s > 0.0) c[0] = c[0] + b * b * sinc[j] * dxi2[j] * dxi3[k] / dx1[i];
+    if (i == gie) {
+      c[0] = c[0] + c[1] * x1[i] / x1[i + 1];
+      c[1] = 0.0;
+    }
+    c[4] = x1[i] * x1[i] * sinc[j] * dxi1[i] * dxi2[j] * dxi3[k];
+  }
+}
+
 // metric.f90:102-151 for spherical polar coordinates: the caller's 1-D
 // factors plus the radial and polar products the kernels form the 2-D and
-// 3-D factors from (same single IEEE operations as the reference).
-extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, const double* idetg1, const double* sx1,
-                              const double* sini, const double* cosi, const double* scot) {
+// 3-D factors from (same single IEEE operations as the reference); with
+// self-gravity the Laplacian coefficient planes and the spherical dtg_unit.
+extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
   if (!ctx) return HMN_EINVAL;
   drop_run_graph(ctx);
   if (crdnt == 0) {
@@ -468,18 +541,21 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, cons
     return HMN_OK;
   }
   if (crdnt != 2) return HMN_EBADCFG;
-  if (!detg1 || !idetg1 || !sx1 || !sini || !cosi || !scot) return HMN_EINVAL;
-  // single grids without gravity or passive scalars (either precision); r solved
-  if (ctx->par.gravswitch != 0 || ctx->par.nspc != 0 || !ctx->solve[0]) return HMN_EBADCFG;
+  if (!mt || !mt->detg1 || !mt->idetg1 || !mt->sx1 || !mt->sini || !mt->cosi || !mt->scot) return HMN_EINVAL;
+  // single grids without passive scalars (either precision); r solved; self-gravity
+  // on (r, theta) grids with one phi cell or on 3-D grids
+  if (ctx->par.nspc != 0 || !ctx->solve[0]) return HMN_EBADCFG;
+  const bool grav = ctx->par.gravswitch == 3;
+  if (grav && (!ctx->solve[1] || !mt->sinc || !mt->sisin)) return HMN_EBADCFG;
   const int L1 = ctx->n[0] + 4, L2 = ctx->n[1] + 4;
-  std::vector<double> h((size_t)6 * L1 + (size_t)4 * L2, 0.0);
+  std::vector<double> h((size_t)6 * L1 + (size_t)5 * L2, 0.0);
   double *g1 = h.data(), *ig1 = g1 + L1, *s1 = ig1 + L1, *vr = s1 + L1, *hr2 = vr + L1, *ar2 = hr2 + L1;
-  double *si = ar2 + L1, *ra2 = si + L2, *cd = ra2 + L2, *sc = cd + L2;
+  double *si = ar2 + L1, *ra2 = si + L2, *cd = ra2 + L2, *sc = cd + L2, *ss = sc + L2;
   const double* xi = ctx->xi1_h;
   for (int s = 0; s < L1; s++) {
-    g1[s] = detg1[s];
-    ig1[s] = idetg1[s];
-    s1[s] = sx1[s];
+    g1[s] = mt->detg1[s];
+    ig1[s] = mt->idetg1[s];
+    s1[s] = mt->sx1[s];
     hr2[s] = 0.5 * (xi[s] * xi[s]);
     if (s > 0) {
       vr[s] = (xi[s] * xi[s] * xi[s] - xi[s - 1] * xi[s - 1] * xi[s - 1]) / 3.0;
@@ -487,11 +563,12 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, cons
     }
   }
   for (int s = 0; s < L2; s++) {
-    si[s] = sini[s];
-    sc[s] = scot[s];
+    si[s] = mt->sini[s];
+    sc[s] = mt->scot[s];
+    ss[s] = mt->sisin ? mt->sisin[s] : 0.0;
     if (s > 0) {
-      ra2[s] = 1.0 / (-cosi[s] + cosi[s - 1]);
-      cd[s] = cosi[s - 1] - cosi[s];
+      ra2[s] = 1.0 / (-mt->cosi[s] + mt->cosi[s - 1]);
+      cd[s] = mt->cosi[s - 1] - mt->cosi[s];
     }
   }
   if (!ctx->sphbuf) CK(cudaMalloc((void**)&ctx->sphbuf, h.size() * sizeof(double)), "cudaMalloc");
@@ -509,9 +586,57 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, cons
   M.ra2 = M.sini + L2;
   M.cd = M.sini + 2 * L2;
   M.scot = M.sini + 3 * L2;
+  M.sisin = M.sini + 4 * L2;
   M.fac_j = ctx->n[1] == 1 ? 2.0 : 1.0;
   M.fac_k = ctx->n[2] == 1 ? 4.0 : 1.0;
   M.on = 1;
+  ctx->xi1s = xi[1];  // xi1(is-1)
+  if (grav) {
+    // the Laplacian's 8 planes per cell: c0, the -x/+x/-y/+y/-z/+z weights, the normalisation
+    const int n0 = ctx->n[0], n1 = ctx->n[1], n2 = ctx->n[2];
+    const size_t P = ctx->plane;
+    std::vector<double> lc((size_t)8 * P);
+    const double *sinc = mt->sinc + 2, *sini = mt->sini + 2;
+    for (int k = 0; k < n2; k++)
+      for (int j = 0; j < n1; j++)
+        for (int i = 0; i < n0; i++) {
+          const size_t c = (size_t)i + (size_t)n0 * ((size_t)j + (size_t)n1 * k);
+          double cc[5], cx[5], cy[5], cz[5];
+          sph_lap_coeffs(ctx, sinc, sini, i, j, k, cc);
+          sph_lap_coeffs(ctx, sinc, sini, i - 1, j, k, cx);
+          sph_lap_coeffs(ctx, sinc, sini, i, j - 1, k, cy);
+          sph_lap_coeffs(ctx, sinc, sini, i, j, k - 1, cz);
+          const double v[8] = {cc[0], cx[1], cc[1], cy[2], cc[2], cz[3], cc[3], cc[4]};
+          for (int q = 0; q < 8; q++) lc[(size_t)q * P + c] = v[q];
+        }
+    if (!ctx->hgc) CK(cudaMalloc((void**)&ctx->hgc, lc.size() * sizeof(double)), "cudaMalloc");
+    if (!ctx->gin) CK(cudaMalloc((void**)&ctx->gin, (size_t)n1 * n2 * sizeof(double)), "cudaMalloc");
+    CK(cudaMemcpyAsync(ctx->hgc, lc.data(), lc.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st),
+       "metric");
+    CK(cudaMemsetAsync(ctx->gin, 0, (size_t)n1 * n2 * sizeof(double), ctx->st), "metric");
+    // tools.f90:160-183 with dtgrav_cell on the spherical dvol and face areas (metric.f90:117-130)
+    const double *dxi2 = host_axis(ctx, 1, 2), *dxi3 = host_axis(ctx, 2, 2);
+    const double off0 = 1.0, off1 = 1.0, off2 = ctx->solve[2] ? 1.0 : 0.0;
+    const double fj = M.fac_j, fk = M.fac_k;
+    double m = INFINITY;
+    for (int k = 0; k < n2; k++)
+      for (int j = 0; j < n1; j++)
+        for (int i = 0; i < n0; i++) {
+          const double a = xi[i + 2], bb = xi[i + 1];
+          const double cdj = mt->cosi[j + 1] - mt->cosi[j + 2];
+          const double dvol = (a * a * a - bb * bb * bb) / 3.0 * cdj * dxi3[k] * fj * fk;
+          const double sa1 = 0.5 * (bb * bb) * cdj * dxi3[k] * fj * fk + 0.5 * (a * a) * cdj * dxi3[k] * fj * fk;
+          const double sa2 = 0.5 * mt->sini[j + 1] * (a * a - bb * bb) * dxi3[k] * fk +
+                             0.5 * mt->sini[j + 2] * (a * a - bb * bb) * dxi3[k] * fk;
+          const double sa3 = 0.5 * (a * a - bb * bb) * dxi2[j] * fj + 0.5 * (a * a - bb * bb) * dxi2[j] * fj;
+          const double v = dvol / (1.0 * (off0 * sa1 + off1 * sa2 + off2 * sa3));
+          m = v < m ? v : m;
+        }
+    ctx->dtg_unit = m;
+    CK(cudaMemcpyAsync(&ctx->sc->dtg_unit, &ctx->dtg_unit, sizeof(double), cudaMemcpyHostToDevice, ctx->st),
+       "metric");
+    CK(cudaStreamSynchronize(ctx->st), "metric");
+  }
   return HMN_OK;
 }
 
@@ -780,12 +905,25 @@ extern "C" int hmn_phidamp(hmn_ctx* ctx) {
   return HMN_OK;
 }
 
+// hg_boundary_conditions on a spherical grid: of the ghost images only the
+// one beyond r = xi1s enters the Laplacian with a non-zero weight, and it
+// keeps the value of this pass through the next call's sub-cycles
+// (gravity_hyperbolic.f90:186-190); the stage kernels form the others.
+static int sph_gravity_boundary(hmn_ctx* ctx) {
+  if (!ctx->G.sph.on || !ctx->gin) return HMN_OK;
+  CK(cudaMemcpy2DAsync(ctx->gin, sizeof(double), ctx->gphi[ctx->gcur], (size_t)ctx->n[0] * sizeof(double),
+                       sizeof(double), (size_t)ctx->n[1] * ctx->n[2], cudaMemcpyDeviceToDevice, ctx->st),
+     "gravity boundary");
+  return HMN_OK;
+}
+
 extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
   if (!ctx) return HMN_EINVAL;
   if (ctx->par.gravswitch != 3) return HMN_OK;
+  if (!ctx->G.sph.on && ctx->dim != 3) return HMN_EBADCFG;  // the Cartesian solver is 3-D
   if (tn == 0) {  // grav_init_other: only the boundary images, which the kernels form on the fly
     ctx->grvtime = time;
-    return HMN_OK;
+    return sph_gravity_boundary(ctx);
   }
   // cgrav and dtgrav of the last hmn_timestep
   int rc = fetch_scalars(ctx);
@@ -820,14 +958,19 @@ extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
       a.stage1 = g == 1;
       a.last = g == ctx->par.grktype;
       a.sc = ctx->sc;
-      CK(launch_hg_stage(ctx->G, a, blocks_for(ctx), ctx->st), "hg stage");
+      a.lc = ctx->hgc;
+      a.gin = ctx->gin;
+      if (ctx->G.sph.on)
+        CK(launch_hg_stage_sph(ctx->G, a, ctx->st), "hg stage");
+      else
+        CK(launch_hg_stage(ctx->G, a, blocks_for(ctx), ctx->st), "hg stage");
       ctx->launches += 1;
       ctx->gcur = 1 - ctx->gcur;
     }
     ctx->grvtime = ctx->grvtime + dtgrav;
     ctx->cgrav_old = cgrav;
   }
-  return HMN_OK;
+  return sph_gravity_boundary(ctx);
 }
 
 extern "C" int hmn_set_gravity_clock(hmn_ctx* ctx, double grvtime, double cgrav_old) {

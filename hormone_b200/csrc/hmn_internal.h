@@ -51,6 +51,7 @@ struct SphGeo {
   const double* ra2;     // 1 / (cos(theta)(j-1) - cos(theta)(j)): theta factor of idetg2
   const double* cd;      // cos(theta)(j-1) - cos(theta)(j): theta factor of dvol, sa1
   const double* scot;    // (sin(j) - sin(j-1)) / (cos(j-1) - cos(j))
+  const double* sisin;   // (xi2(j) - xi2(j-1)) / (cos(j-1) - cos(j)): phi factor of the gravity source
 };
 
 struct GridDev {
@@ -126,6 +127,11 @@ struct HGArgs {
   double damp;             // applied to psi after the last stage
   int stage1, last;
   DevScalars* sc;
+  // spherical grids: the 8 coefficient planes of the Laplacian (c0, then the
+  // -x, +x, -y, +y, -z, +z neighbours' weights, then the normalisation) and
+  // the potential beyond r = xi1s as the last boundary pass left it
+  const double* lc;
+  const double* gin;
 };
 
 // One simulation of a batch, resident in device memory.  Every field the
@@ -173,6 +179,7 @@ cudaError_t launch_prim_from_u(const double* U, double* P, size_t plane, bool ma
 cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double gm1, double* out, double* p_out,
                             int nblocks, cudaStream_t st);
 cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cudaStream_t st);
+cudaError_t launch_hg_stage_sph(const GridDev& G, const HGArgs& A, cudaStream_t st);
 cudaError_t launch_advance(DevScalars* sc, cudaStream_t st);
 // batched launchers over a work list of (sim, tile) items; tile_kind selects
 // the compile-time tile (see batch_tile_kind), grid = persistent CTAs

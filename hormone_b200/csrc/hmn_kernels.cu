@@ -304,43 +304,50 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
   const size_t c = cidx(G, i, j, k);
   const size_t pl = A.plane;
   constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
-  if (A.gphi != nullptr) {
-    const double d = A.pin[c];
-    const double v[3] = {A.pin[PV * pl + c], A.pin[(PV + 1) * pl + c], A.pin[(PV + 2) * pl + c]};
+  if constexpr (SPH) {
+    // geometric sources and, with self-gravity, the force of the potential
+    // with the spherical ghost images (source.f90:113-150), all in FP64
     double frc[3];
-    const int ijk[3] = {i, j, k};
+    if (A.gphi != nullptr) gravity_force<true>(G, A.gphi, c, i, j, k, A.pin[c], frc);
+    sph_sources<MAG>(G, A, c, i, j, acc, A.gphi != nullptr ? frc : nullptr);
+  } else {
+    if (A.gphi != nullptr) {
+      const double d = A.pin[c];
+      const double v[3] = {A.pin[PV * pl + c], A.pin[(PV + 1) * pl + c], A.pin[(PV + 2) * pl + c]};
+      double frc[3];
+      const int ijk[3] = {i, j, k};
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const AxisGeo& g = G.g[a];
-      const int s = ijk[a];
-      // neighbours of the potential with the ghost images of the boundary
-      // (periodic copy, or the Robin image phi ~ 1/r)
-      double ph[3];
+      for (int a = 0; a < 3; a++) {
+        const AxisGeo& g = G.g[a];
+        const int s = ijk[a];
+        // neighbours of the potential with the ghost images of the boundary
+        // (periodic copy, or the Robin image phi ~ 1/r)
+        double ph[3];
 #pragma unroll
-      for (int o = -1; o <= 1; o++) {
-        int nb[3] = {i, j, k};
-        nb[a] = s + o;
-        if (nb[a] >= 0 && nb[a] < G.n[a]) {
-          ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
-        } else if (G.bc[a][0][0] == 0) {
-          nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
-          ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
-        } else {
-          const double xe = G.g[0].x[i + 2], ye = G.g[1].x[j + 2], ze = G.g[2].x[k + 2];
-          const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
-          const double re = sqrt(xe * xe + ye * ye + ze * ze), rg = sqrt(xg * xg + yg * yg + zg * zg);
-          ph[o + 1] = A.gphi[c] * re / rg;
+        for (int o = -1; o <= 1; o++) {
+          int nb[3] = {i, j, k};
+          nb[a] = s + o;
+          if (nb[a] >= 0 && nb[a] < G.n[a]) {
+            ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+          } else if (G.bc[a][0][0] == 0) {
+            nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
+            ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+          } else {
+            const double xe = G.g[0].x[i + 2], ye = G.g[1].x[j + 2], ze = G.g[2].x[k + 2];
+            const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
+            const double re = sqrt(xe * xe + ye * ye + ze * ze), rg = sqrt(xg * xg + yg * yg + zg * zg);
+            ph[o + 1] = A.gphi[c] * re / rg;
+          }
         }
+        const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
+        frc[a] = -((dxm * ip * ph[2] - dxp * im * ph[0]) / (dxm + dxp) + (dxp - dxm) * im * ip * ph[1]) * d;
       }
-      const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
-      frc[a] = -((dxm * ip * ph[2] - dxp * im * ph[0]) / (dxm + dxp) + (dxp - dxm) * im * ip * ph[1]) * d;
+      acc[1] = acc[1] + frc[0];
+      acc[2] = acc[2] + frc[1];
+      acc[3] = acc[3] + frc[2];
+      acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
     }
-    acc[1] = acc[1] + frc[0];
-    acc[2] = acc[2] + frc[1];
-    acc[3] = acc[3] + frc[2];
-    acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
   }
-  if constexpr (SPH) sph_sources<MAG>(G, A, c, i, j, acc);
   const double dtf = A.fact * A.sc->dt;
   double un[9];
 #pragma unroll
@@ -1101,6 +1108,57 @@ cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cuda
   const int bx = G.n[0] < 128 ? ((G.n[0] + 31) / 32) * 32 : 128;
   const dim3 grid((G.n[0] + bx - 1) / bx, G.n[1], G.n[2]);
   hg_stage_kernel<<<grid, bx, 0, st>>>(G, A);
+  return cudaGetLastError();
+}
+
+// The same RK sub-stage on a spherical grid (get_lapphi_hgsrc,
+// gravity_hyperbolic.f90:243-270): the coefficients of setup_grv_hyperbolic
+// come precomputed per cell (A.lc); the neighbour beyond r = xi1s is the
+// value the last boundary pass copied there (A.gin), the other neighbours
+// beyond a non-periodic face carry zero weight, and phi is periodic.
+__global__ void __launch_bounds__(128) hg_stage_sph_kernel(const GridDev G, const HGArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= G.n[0]) return;
+  const int n0 = G.n[0], n1 = G.n[1], n2 = G.n[2];
+  const size_t c = cidx(G, i, j, k), pl = A.plane;
+  const double* ph = A.phi_in;
+  const double* L = A.lc;
+  double lap = L[c] * ph[c];
+  lap = lap + L[pl + c] * (i > 0 ? ph[c - 1] : A.gin[j + (size_t)n1 * k]);
+  lap = lap + L[2 * pl + c] * (i + 1 < n0 ? ph[c + 1] : ph[c]);
+  if (n1 > 1) {
+    lap = lap + L[3 * pl + c] * (j > 0 ? ph[cidx(G, i, j - 1, k)] : ph[c]);
+    lap = lap + L[4 * pl + c] * (j + 1 < n1 ? ph[cidx(G, i, j + 1, k)] : ph[c]);
+  }
+  if (n2 > 1) {
+    lap = lap + L[5 * pl + c] * ph[cidx(G, i, j, k > 0 ? k - 1 : n2 - 1)];
+    lap = lap + L[6 * pl + c] * ph[cidx(G, i, j, k + 1 < n2 ? k + 1 : 0)];
+  }
+  const double lapphi = lap / L[7 * pl + c];
+  const double hgsrc = A.fourpiG * A.dens[c];
+  double o1, o2;
+  const double phi0 = ph[c], psi0 = A.psi_in[c];
+  if (A.stage1) {
+    o1 = phi0;
+    o2 = psi0;
+    A.org_phi[c] = o1;
+    A.org_psi[c] = o2;
+  } else {
+    o1 = A.org_phi[c];
+    o2 = A.org_psi[c];
+  }
+  const double pn = A.faco * o1 + A.facn * phi0 + A.fdc * psi0;
+  double sn = A.faco * o2 + A.facn * psi0 + A.fdc * (lapphi - hgsrc);
+  if (A.last) sn = sn * A.damp;
+  A.phi_out[c] = pn;
+  A.psi_out[c] = sn;
+}
+
+cudaError_t launch_hg_stage_sph(const GridDev& G, const HGArgs& A, cudaStream_t st) {
+  const int bx = G.n[0] < 128 ? ((G.n[0] + 31) / 32) * 32 : 128;
+  const dim3 grid((G.n[0] + bx - 1) / bx, G.n[1], G.n[2]);
+  hg_stage_sph_kernel<<<grid, bx, 0, st>>>(G, A);
   return cudaGetLastError();
 }
 

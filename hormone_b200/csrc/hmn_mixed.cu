@@ -273,41 +273,48 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
   const size_t c = cidx(G, i, j, k);
   const size_t pl = A.plane;
   constexpr int nv = MAG ? (GLM ? 9 : 8) : 5;
-  if (A.gphi != nullptr) {
-    // gravity source in FP64 (source.f90:70-85 with get_fieldforce :177-228)
-    const double d = A.pin[c];
-    const double v[3] = {A.pin[PV * pl + c], A.pin[(PV + 1) * pl + c], A.pin[(PV + 2) * pl + c]};
+  if constexpr (SPH) {
+    // geometric sources and, with self-gravity, the force of the potential
+    // with the spherical ghost images (source.f90:113-150), all in FP64
     double frc[3];
-    const int ijk[3] = {i, j, k};
+    if (A.gphi != nullptr) gravity_force<true>(G, A.gphi, c, i, j, k, A.pin[c], frc);
+    sph_sources<MAG>(G, A, c, i, j, acc, A.gphi != nullptr ? frc : nullptr);
+  } else {
+    if (A.gphi != nullptr) {
+      // gravity source in FP64 (source.f90:70-85 with get_fieldforce :177-228)
+      const double d = A.pin[c];
+      const double v[3] = {A.pin[PV * pl + c], A.pin[(PV + 1) * pl + c], A.pin[(PV + 2) * pl + c]};
+      double frc[3];
+      const int ijk[3] = {i, j, k};
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const AxisGeo& g = G.g[a];
-      const int s = ijk[a];
-      double ph[3];
+      for (int a = 0; a < 3; a++) {
+        const AxisGeo& g = G.g[a];
+        const int s = ijk[a];
+        double ph[3];
 #pragma unroll
-      for (int o = -1; o <= 1; o++) {
-        int nb[3] = {i, j, k};
-        nb[a] = s + o;
-        if (nb[a] >= 0 && nb[a] < G.n[a]) {
-          ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
-        } else if (G.bc[a][0][0] == 0) {
-          nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
-          ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
-        } else {
-          const double xe = G.g[0].x[i + 2], ye = G.g[1].x[j + 2], ze = G.g[2].x[k + 2];
-          const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
-          ph[o + 1] = A.gphi[c] * sqrt(xe * xe + ye * ye + ze * ze) / sqrt(xg * xg + yg * yg + zg * zg);
+        for (int o = -1; o <= 1; o++) {
+          int nb[3] = {i, j, k};
+          nb[a] = s + o;
+          if (nb[a] >= 0 && nb[a] < G.n[a]) {
+            ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+          } else if (G.bc[a][0][0] == 0) {
+            nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
+            ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+          } else {
+            const double xe = G.g[0].x[i + 2], ye = G.g[1].x[j + 2], ze = G.g[2].x[k + 2];
+            const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
+            ph[o + 1] = A.gphi[c] * sqrt(xe * xe + ye * ye + ze * ze) / sqrt(xg * xg + yg * yg + zg * zg);
+          }
         }
+        const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
+        frc[a] = -((dxm * ip * ph[2] - dxp * im * ph[0]) / (dxm + dxp) + (dxp - dxm) * im * ip * ph[1]) * d;
       }
-      const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
-      frc[a] = -((dxm * ip * ph[2] - dxp * im * ph[0]) / (dxm + dxp) + (dxp - dxm) * im * ip * ph[1]) * d;
+      acc[1] = acc[1] + frc[0];
+      acc[2] = acc[2] + frc[1];
+      acc[3] = acc[3] + frc[2];
+      acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
     }
-    acc[1] = acc[1] + frc[0];
-    acc[2] = acc[2] + frc[1];
-    acc[3] = acc[3] + frc[2];
-    acc[4] = acc[4] + (frc[0] * v[0] + frc[1] * v[1] + frc[2] * v[2]);
   }
-  if constexpr (SPH) sph_sources<MAG>(G, A, c, i, j, acc);  // geometric sources in FP64
   const double dtf = A.fact * A.sc->dt;
   double un[9];
 #pragma unroll

@@ -489,12 +489,56 @@ __device__ __forceinline__ void sph_div_weights(const GridDev& G, int i, int j, 
   }
 }
 
+// The gravitational potential at the neighbour o = -1 / +1 of cell c =
+// (i,j,k) along axis a, with the ghost images the boundary pass of the
+// hyperbolic solver forms: a periodic copy; on spherical grids copies at the
+// inner radius and the poles and phi ~ 1/r beyond the outer radius
+// (gravity_hyperbolic.f90:186-207, gbtype 1); on Cartesian grids the Robin
+// image phi ~ 1/r about the origin.
+template <bool SPH>
+__device__ __forceinline__ double gphi_at(const GridDev& G, const double* gphi, size_t c, int i, int j, int k,
+                                          int a, int o) {
+  int nb[3] = {i, j, k};
+  nb[a] += o;
+  if (nb[a] >= 0 && nb[a] < G.n[a]) return gphi[cidx(G, nb[0], nb[1], nb[2])];
+  if (G.bc[a][0][0] == 0) {
+    nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
+    return gphi[cidx(G, nb[0], nb[1], nb[2])];
+  }
+  if constexpr (SPH) {
+    if (a == 0 && o > 0) return gphi[c] * G.g[0].x[i + 2] / G.g[0].x[i + 3];
+    return gphi[c];
+  }
+  const double xe = G.g[0].x[i + 2], ye = G.g[1].x[j + 2], ze = G.g[2].x[k + 2];
+  const double xg = G.g[0].x[nb[0] + 2], yg = G.g[1].x[nb[1] + 2], zg = G.g[2].x[nb[2] + 2];
+  const double re = sqrt(xe * xe + ye * ye + ze * ze), rg = sqrt(xg * xg + yg * yg + zg * zg);
+  return gphi[c] * re / rg;
+}
+
+// -d(phi)/dx_a * rho of cell c along each axis (get_fieldforce,
+// source.f90:177-228: centred differences on the non-uniform centres)
+template <bool SPH>
+__device__ __forceinline__ void gravity_force(const GridDev& G, const double* gphi, size_t c, int i, int j, int k,
+                                              double d, double frc[3]) {
+  const int ijk[3] = {i, j, k};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const AxisGeo& g = G.g[a];
+    const int s = ijk[a];
+    const double pm = gphi_at<SPH>(G, gphi, c, i, j, k, a, -1), p0 = gphi[c];
+    const double pp = gphi_at<SPH>(G, gphi, c, i, j, k, a, 1);
+    const double dxm = g.dx[s + 2], dxp = g.dx[s + 3], im = g.idx[s + 2], ip = g.idx[s + 3];
+    frc[a] = -((dxm * ip * pp - dxp * im * pm) / (dxm + dxp) + (dxp - dxm) * im * ip * p0) * d;
+  }
+}
+
 // Spherical geometric source terms (source.f90:113-143) of cell c, from the
 // stage's input primitives with ptot = p + B^2/2 as `pressure` forms it
-// (eos.f90:758-768), added to the flux divergence in acc[].
+// (eos.f90:758-768), plus the gravity terms of :145-150 when grv is given,
+// added to the flux divergence in acc[].
 template <bool MAG>
 __device__ __forceinline__ void sph_sources(const GridDev& G, const StageArgs& A, size_t c, int i, int j,
-                                            double acc[9]) {
+                                            double acc[9], const double* grv) {
   const SphGeo& M = G.sph;
   const size_t pl = A.plane;
   const double d = A.pin[c];
@@ -517,6 +561,13 @@ __device__ __forceinline__ void sph_sources(const GridDev& G, const StageArgs& A
     r3 = r3 + (b1 * b3 + b2 * b3 * sc) * s1;
     acc[6] = acc[6] + (b2 * v1 - b1 * v2) * s1;
     acc[7] = acc[7] + ((v2 * b3 - b2 * v3) * sc - (b1 * v3 - b3 * v1)) * s1;
+  }
+  if (grv != nullptr) {
+    const double ss = M.sisin[j + 2];
+    r1 = r1 + grv[0];
+    r2 = r2 + grv[1] * s1;
+    r3 = r3 + grv[2] * s1 * ss;
+    acc[4] = acc[4] + (grv[0] * v1 + grv[1] * v2 * s1 + grv[2] * v3 * s1 * ss);
   }
   acc[1] = acc[1] + r1;
   acc[2] = acc[2] + r2;

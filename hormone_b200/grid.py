@@ -134,10 +134,11 @@ def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
     theta cell or eq_sym), uniform, with volumetric centres; phi over
     [-pi, pi], uniform (one cell stands for a quarter turn).  Extra keys:
     axis 0 ``detg`` (xi1**2), ``idetg`` and ``sx`` (over is-1..ie+1);
-    axis 1 ``sini``/``cosi`` (is-2..ie+2) and ``scot`` (js-1..je+1)."""
+    axis 1 ``sini``/``cosi``/``sinc`` (js-2..je+2), ``scot`` and ``sisin``
+    (js-1..je+1).  With self-gravity the two outer radial ghosts continue
+    the last cell ratio (:331-343)."""
     n1, n2, n3 = (int(v) for v in cfg["n"])
-    if int(cfg.get("gravswitch", 0)) != 0:
-        raise ValueError("self-gravity on spherical grids is not on this path")
+    grav = int(cfg.get("gravswitch", 0)) != 0
     if 1 < n3 < 4:
         raise ValueError(f"Error from ke {n3}: a spherical grid needs one or at least four phi cells")
     if int(cfg.get("jmesh", 0)) != 0 or int(cfg.get("kmesh", 0)) != 0:
@@ -151,7 +152,7 @@ def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
     else:
         raise ValueError(f"imesh={imesh}: only uniform (0) and geometrical-series (1) meshes are on this path")
     r = axis_from_widths(widths, lo)
-    x, xi, dx, idx = (r[k].tolist() for k in ("x", "xi", "dx", "idx"))
+    x, xi, dx, idx, dxi, idxi = (r[k].tolist() for k in ("x", "xi", "dx", "idx", "dxi", "idxi"))
     for s in range(1, n1 + 4):  # Fortran is-1 .. ie+2 (:323-329)
         a, b = xi[s], xi[s - 1]
         x[s] = 0.75 * (a + b) * (a * a + b * b) / (a * a + a * b + b * b)
@@ -159,7 +160,20 @@ def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
             x[1] = -x[2]
         dx[s] = x[s] - x[s - 1]
         idx[s] = 1.0 / dx[s]
-    r.update(x=np.array(x), dx=np.array(dx), idx=np.array(idx))
+    if grav:  # :331-343, the potential's grid being the hydro grid (gie = ie)
+        for s in (n1 + 2, n1 + 3):
+            dxi[s] = dxi[s - 1] * dxi[n1 + 1] / dxi[n1]
+            idxi[s] = 1.0 / dxi[s]
+            xi[s] = xi[s - 1] + dxi[s]
+            a, b = xi[s], xi[s - 1]
+            x[s] = 0.75 * (a + b) * (a * a + b * b) / (a * a + a * b + b * b)
+            dx[s] = x[s] - x[s - 1]
+            idx[s] = 1.0 / dx[s]
+        dx[0] = dxi[0]
+        idx = [1.0 / v for v in dx]
+        idxi = [1.0 / v for v in dxi]
+    r.update(x=np.array(x), xi=np.array(xi), dx=np.array(dx), idx=np.array(idx), dxi=np.array(dxi),
+             idxi=np.array(idxi))
 
     pi = math.pi  # acos(-1d0)
     xi2e = pi * 0.5 if (n2 == 1 or bool(cfg.get("eq_sym", False))) else pi
@@ -167,6 +181,7 @@ def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
     x, xi, dx, idx = (th[k].tolist() for k in ("x", "xi", "dx", "idx"))
     sc = [quad_sin_cos(v) for v in xi]
     si, ci = [v[0] for v in sc], [v[1] for v in sc]
+    sinc = [quad_sin_cos(v)[0] for v in x]  # arithmetic centres, before the volumetric ones
     for s in range(1, n2 + 4):  # js-1 .. je+2 (:385-392)
         x[s] = (xi[s - 1] * ci[s - 1] - xi[s] * ci[s] + si[s] - si[s - 1]) / (ci[s - 1] - ci[s])
         if s == 2:
@@ -186,11 +201,14 @@ def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
         detg[s] = a * a
         idetg[s] = 3.0 / (dxi[s] * (a * a + a * b + b * b))
         sx[s] = 1.5 * (a + b) / (a * a + a * b + b * b)
-    scot = [0.0] * (n2 + 4)
+    scot, sisin = [0.0] * (n2 + 4), [0.0] * (n2 + 4)
+    xi2 = th["xi"].tolist()
     for s in range(1, n2 + 3):
         scot[s] = (si[s] - si[s - 1]) / (ci[s - 1] - ci[s])
+        sisin[s] = (xi2[s] - xi2[s - 1]) / (ci[s - 1] - ci[s])
     r.update(detg=np.array(detg), idetg=np.array(idetg), sx=np.array(sx))
-    th.update(sini=np.array(si), cosi=np.array(ci), scot=np.array(scot))
+    th.update(sini=np.array(si), cosi=np.array(ci), scot=np.array(scot), sinc=np.array(sinc),
+              sisin=np.array(sisin))
     return [r, th, ph]
 
 

@@ -200,6 +200,24 @@ def polytrope_n1(cfg, grid, rho_floor: float = 1e-6):
     return out, phi
 
 
+def polytrope_n1_spherical(cfg, grid, rho_floor: float = 1e-6):
+    """The n=1 polytrope of ``polytrope_n1`` on a spherical polar grid
+    centred on it: the same profiles of the radius x1 of each cell.
+    Returns (prims, grvphi)."""
+    out = _blank(cfg)
+    K = 2.0 / PI
+    GM = 4.0 / PI
+    r = np.broadcast_to(centres(grid, 0)[None, None, :], out["d"].shape)
+    inside = r < 1.0
+    pr = np.where(inside & (r > 0.0), PI * r, 1.0)
+    poly = np.where(inside, np.where(r > 0.0, np.sin(pr) / pr, 1.0), 0.0)
+    out["d"][:] = np.maximum(poly, rho_floor)
+    out["p"][:] = K * poly * poly + rho_floor * GM / np.maximum(r, 1.0)
+    rs = np.where(r > 0.0, r, 1.0)
+    phi = np.ascontiguousarray(np.where(inside, -GM * (1.0 + poly), -GM / rs))
+    return out, phi
+
+
 def sedov(cfg, grid, energy: float = 1.0, radius: float = 0.05, rho0: float = 1.0, p0: float = 1e-5):
     """Cartesian Sedov-type blast: ``energy`` spread evenly over the cells
     whose centres lie within ``radius`` of the box centre."""

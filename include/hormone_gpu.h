@@ -71,15 +71,30 @@ typedef struct {
 int hmn_create(const hmn_grid* grid, const hmn_params* params, hmn_ctx** out);
 
 /* metric (src/main/metric.f90:102-151) for spherical polar coordinates
- * (crdnt 2: axes 1-3 are r, theta, phi, built as gridset.f90:294-423).
- * detg1, idetg1, sx1 cover is-2..ie+2 and sini, cosi, scot js-2..je+2, as
- * module `grid` holds them after `metric`; the kernels form idetg2, idetg3,
- * dvol and sa1..3 from them in the reference's operation order.  crdnt 0
- * (Cartesian, the default) takes no arrays.  Spherical grids run as single
- * grids (either precision) with r solved and without gravity or passive
- * scalars (HMN_EBADCFG otherwise).  Call before the first step. */
-int hmn_set_metric(hmn_ctx* ctx, int crdnt, const double* detg1, const double* idetg1, const double* sx1,
-                   const double* sini, const double* cosi, const double* scot);
+ * (crdnt 2: axes 1-3 are r, theta, phi, built as gridset.f90:294-423): the
+ * 1-D factors module `grid` holds after `metric`, each from index is-2
+ * (r) or js-2 (theta) to ie+2 / je+2.  sinc (sin of the arithmetic theta
+ * centres) and sisin are read only with self-gravity (gravswitch 3). */
+typedef struct {
+  const double* detg1;   /* xi1**2 */
+  const double* idetg1;
+  const double* sx1;
+  const double* sini;    /* sin and cos of the theta faces */
+  const double* cosi;
+  const double* scot;
+  const double* sinc;
+  const double* sisin;
+} hmn_metric;
+
+/* Sets the coordinate system; crdnt 0 (Cartesian, the default) takes no
+ * arrays.  The kernels form idetg2, idetg3, dvol and sa1..3 from the 1-D
+ * factors in the reference's operation order, and with gravswitch 3 the
+ * spherical Laplacian coefficients of setup_grv_hyperbolic
+ * (gravity_hyperbolic.f90:336-405; (r, theta) with one phi cell, or 3-D;
+ * Robin outer radius, gbtype 1).  Spherical grids run as single grids in
+ * either precision with r solved and without passive scalars (HMN_EBADCFG
+ * otherwise).  Call before the first step. */
+int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* m);
 
 /* Device copy of the state after initialcondition/conserve/pressure
  * (hormone.f90:94-100).  u: conserved array (ufnmax planes); prim: d, v1,

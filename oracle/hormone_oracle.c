@@ -89,6 +89,8 @@ typedef struct {
   int crdnt;
   double *detg1, *idetg1, *sx1;   /* r faces / cells */
   double *sini, *cosi, *scot;     /* theta faces / cells */
+  double *sinc, *sisin;           /* sin of the arithmetic theta centres; dtheta/(cos-cos) */
+  double xi1s;                    /* inner radius (the inner-boundary term of the gravity coefficients) */
   double fac_j, fac_k;
   /* scalars */
   double dt, ch, time, t_out, t_end, dt_out, cfmax;
@@ -151,6 +153,7 @@ Oracle *hmo_create(int nx, int ny, int nz, int mag_on, int limiter, int rktype, 
   o->lapphi = zalloc(N); o->hgsrc = zalloc(N); o->gsrc = zalloc(N);
   o->detg1 = zalloc((size_t)nx + 4); o->idetg1 = zalloc((size_t)nx + 4); o->sx1 = zalloc((size_t)nx + 4);
   o->sini = zalloc((size_t)ny + 4); o->cosi = zalloc((size_t)ny + 4); o->scot = zalloc((size_t)ny + 4);
+  o->sinc = zalloc((size_t)ny + 4); o->sisin = zalloc((size_t)ny + 4);
   o->fac_j = 1.0; o->fac_k = 1.0;
   return o;
 }
@@ -170,6 +173,7 @@ void hmo_destroy(Oracle *o) {
   free(o->grvphi); free(o->grvpsi); free(o->gorg1); free(o->gorg2); free(o->lapphi); free(o->hgsrc); free(o->gsrc);
   for (int a = 0; a < 3; a++) { free(o->dir[a][0]); free(o->dir[a][1]); }
   free(o->detg1); free(o->idetg1); free(o->sx1); free(o->sini); free(o->cosi); free(o->scot);
+  free(o->sinc); free(o->sisin);
   for (int n = 0; n < o->spn; n++) {
     free(o->spc[n]); free(o->spcorg[n]);
     for (int a = 0; a < 3; a++) { free(o->dspc[a][n]); free(o->spcflx[a][n]); }
@@ -225,7 +229,7 @@ void hmo_set_gravity(Oracle *o, int gravswitch, double HGfac, double hgcfl, doub
    arrays are reset to dxi and the two ghost layers are re-accumulated
    (gridset.f90:71-81). */
 /* gridset.f90:46-81 from the cell widths dxi(is-2:ie+2) of any Cartesian mesh */
-void hmo_make_axis(Oracle *o, int a, double xis, const double *widths) {
+static void make_axis(Oracle *o, int a, double xis, const double *widths, int cart_grav) {
   int n = o->n[a];
   double *x = o->x[a], *xi = o->xi[a], *dx = o->dx[a], *dxi = o->dxi[a], *idx = o->idx[a], *idxi = o->idxi[a];
 #define G2(arr, i) arr[(i) + 2]
@@ -243,7 +247,7 @@ void hmo_make_axis(Oracle *o, int a, double xis, const double *widths) {
     G2(x, i) = G2(x, i - 1) + G2(dx, i);
     G2(xi, i) = G2(xi, i - 1) + G2(dxi, i);
   }
-  if (o->gravswitch != 0) {
+  if (cart_grav) {
     for (int i = -2; i <= n + 1; i++) {
       G2(dx, i) = G2(dxi, i);
       G2(idx, i) = 1.0 / G2(dx, i);
@@ -259,6 +263,10 @@ void hmo_make_axis(Oracle *o, int a, double xis, const double *widths) {
     }
   }
 #undef G2
+}
+
+void hmo_make_axis(Oracle *o, int a, double xis, const double *widths) {
+  make_axis(o, a, xis, widths, o->gravswitch != 0);
 }
 
 /* cell widths dxi(is-2:ie+2) of a geometrical-series mesh (imesh=1):
@@ -308,7 +316,8 @@ static double qcos(double x) { return (double)cosq((__float128)x); }
    metric.f90:102-151. */
 int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1min, int eq_sym) {
   const int n1 = o->n[0], n2 = o->n[1], n3 = o->n[2];
-  if (o->gravswitch != 0 || (n3 > 1 && n3 < 4)) return HMO_EBADCFG;
+  if (n3 > 1 && n3 < 4) return HMO_EBADCFG;
+  o->xi1s = xi1s;
   const double pi = acos(-1.0);
   double *w = zalloc((size_t)(n1 > n2 ? (n1 > n3 ? n1 : n3) : (n2 > n3 ? n2 : n3)) + 4);
   /* r */
@@ -318,9 +327,10 @@ int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1
   } else {
     for (int i = 0; i < n1 + 4; i++) w[i] = (xi1e - xi1s) / (double)n1;
   }
-  hmo_make_axis(o, 0, xi1s, w);
+  make_axis(o, 0, xi1s, w, 0);
   {
     double *x = o->x[0] + 2, *xi = o->xi[0] + 2, *dx = o->dx[0] + 2, *idx = o->idx[0] + 2;
+    double *dxi = o->dxi[0] + 2, *idxi = o->idxi[0] + 2;
     for (int i = -1; i <= n1 + 1; i++) { /* :323-329 */
       x[i] = 0.75 * (xi[i] + xi[i - 1]) * (xi[i] * xi[i] + xi[i - 1] * xi[i - 1]) /
              (xi[i] * xi[i] + xi[i] * xi[i - 1] + xi[i - 1] * xi[i - 1]);
@@ -328,16 +338,29 @@ int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1
       dx[i] = x[i] - x[i - 1];
       idx[i] = 1.0 / dx[i];
     }
+    if (o->gravswitch != 0) { /* :331-343 with the potential's grid equal to the hydro grid (gie = ie) */
+      for (int i = n1; i <= n1 + 1; i++) {
+        dxi[i] = dxi[i - 1] * dxi[n1 - 1] / dxi[n1 - 2];
+        idxi[i] = 1.0 / dxi[i];
+        xi[i] = xi[i - 1] + dxi[i];
+        x[i] = 0.75 * (xi[i] + xi[i - 1]) * (xi[i] * xi[i] + xi[i - 1] * xi[i - 1]) /
+               (xi[i] * xi[i] + xi[i] * xi[i - 1] + xi[i - 1] * xi[i - 1]);
+        dx[i] = x[i] - x[i - 1];
+        idx[i] = 1.0 / dx[i];
+      }
+      dx[-2] = dxi[-2];
+      for (int i = -2; i <= n1 + 1; i++) { idx[i] = 1.0 / dx[i]; idxi[i] = 1.0 / dxi[i]; }
+    }
   }
   /* theta */
   double xi2e = (n2 == 1 || eq_sym) ? pi * 0.5 : pi;
   int jetmp = n2 == 1 ? 1 : n2;
   for (int j = 0; j < n2 + 4; j++) w[j] = xi2e / (double)jetmp;
-  hmo_make_axis(o, 1, 0.0, w);
+  make_axis(o, 1, 0.0, w, 0);
   {
     double *x = o->x[1] + 2, *xi = o->xi[1] + 2, *dx = o->dx[1] + 2, *idx = o->idx[1] + 2;
-    double *si = o->sini + 2, *ci = o->cosi + 2;
-    for (int j = -2; j <= n2 + 1; j++) { si[j] = qsin(xi[j]); ci[j] = qcos(xi[j]); }
+    double *si = o->sini + 2, *ci = o->cosi + 2, *sc = o->sinc + 2;
+    for (int j = -2; j <= n2 + 1; j++) { si[j] = qsin(xi[j]); ci[j] = qcos(xi[j]); sc[j] = qsin(x[j]); }
     for (int j = -1; j <= n2 + 1; j++) { /* :385-392 */
       x[j] = (xi[j - 1] * ci[j - 1] - xi[j] * ci[j] + si[j] - si[j - 1]) / (ci[j - 1] - ci[j]);
       if (j == 0) x[j - 1] = -x[j];
@@ -348,7 +371,7 @@ int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1
   /* phi */
   int ketmp = n3 == 1 ? 4 : n3;
   for (int k = 0; k < n3 + 4; k++) w[k] = (pi - -pi) / (double)ketmp;
-  hmo_make_axis(o, 2, -pi, w);
+  make_axis(o, 2, -pi, w, 0);
   free(w);
   /* metric.f90:102-151 */
   {
@@ -360,8 +383,12 @@ int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1
       s1[i] = 1.5 * (xi[i] + xi[i - 1]) / (xi[i] * xi[i] + xi[i] * xi[i - 1] + xi[i - 1] * xi[i - 1]);
     }
     const double *si = o->sini + 2, *ci = o->cosi + 2;
-    double *sc = o->scot + 2;
-    for (int j = -1; j <= n2; j++) sc[j] = (si[j] - si[j - 1]) / (ci[j - 1] - ci[j]);
+    const double *xi2 = o->xi[1] + 2;
+    double *sc = o->scot + 2, *ss = o->sisin + 2;
+    for (int j = -1; j <= n2; j++) {
+      sc[j] = (si[j] - si[j - 1]) / (ci[j - 1] - ci[j]);
+      ss[j] = (xi2[j] - xi2[j - 1]) / (ci[j - 1] - ci[j]);
+    }
   }
   o->fac_k = n3 == 1 ? 4.0 : 1.0;
   o->fac_j = n2 == 1 ? 2.0 : 1.0;
@@ -370,10 +397,10 @@ int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1
 }
 
 /* metric arrays of a spherical grid: 0 detg1, 1 idetg1, 2 sx1 (n0+4 each),
-   3 sini, 4 cosi, 5 scot (n1+4 each) */
+   3 sini, 4 cosi, 5 scot, 6 sinc, 7 sisin (n1+4 each) */
 int hmo_get_metric(Oracle *o, int which, double *out) {
-  const double *src[6] = {o->detg1, o->idetg1, o->sx1, o->sini, o->cosi, o->scot};
-  if (which < 0 || which > 5) return -1;
+  const double *src[8] = {o->detg1, o->idetg1, o->sx1, o->sini, o->cosi, o->scot, o->sinc, o->sisin};
+  if (which < 0 || which > 7) return -1;
   size_t L = (size_t)o->n[which < 3 ? 0 : 1] + 4;
   memcpy(out, src[which], L * sizeof(double));
   return 0;
@@ -920,6 +947,13 @@ static void source(Oracle *o) {
             o->src[IMG2][c] = (b2 * v1 - b1 * v2) * s1;
             o->src[IMG3][c] = ((v2 * b3 - b2 * v3) * sc - (b1 * v3 - b3 * v1)) * s1;
           }
+          if (grav) { /* source.f90:145-150 */
+            const double g1 = o->grv[0][c], g2 = o->grv[1][c], g3 = o->grv[2][c], si = o->sisin[j + 2];
+            o->src[IMO1][c] = o->src[IMO1][c] + g1;
+            o->src[IMO2][c] = o->src[IMO2][c] + g2 * s1;
+            o->src[IMO3][c] = o->src[IMO3][c] + g3 * s1 * si;
+            o->src[IENE][c] = g1 * v1 + g2 * v2 * s1 + g3 * v3 * s1 * si;
+          }
           continue;
         }
         if (grav) {
@@ -1160,6 +1194,43 @@ static void lap_coeffs(const Oracle *o, int i, int j, int k, double c[7], double
   *cnorm = dxi1[i] * dxi2[j] * dxi3[k];
 }
 
+/* lap_coeff(0..3) and the normalisation lap_coeff(-1) at coefficient index
+   (i,j,k), i, j, k >= -1, of a spherical grid (setup_grv_hyperbolic,
+   gravity_hyperbolic.f90:336-400): the axisymmetric (r, theta) form for one
+   phi cell, the 3-D form otherwise; the Robin condition at the outer radius
+   (gbtype 1), Neumann at the last theta face, and the inner-radius term when
+   the grid does not reach r = 0. */
+static void lap_coeffs_sph(const Oracle *o, int i, int j, int k, double c[5]) {
+  const double *x1 = o->x[0] + 2, *xi1 = o->xi[0] + 2, *dx1 = o->dx[0] + 2, *dxi1 = o->dxi[0] + 2;
+  const double *dx2 = o->dx[1] + 2, *dxi2 = o->dxi[1] + 2;
+  const double *dx3 = o->dx[2] + 2, *dxi3 = o->dxi[2] + 2, *idx3 = o->idx[2] + 2;
+  const double *sinc = o->sinc + 2, *sini = o->sini + 2;
+  const int gie = o->n[0] - 1, gje = o->n[1] - 1;
+  const double a = xi1[i], b = xi1[i - 1];
+  if (o->n[2] == 1) { /* :336-363 */
+    c[0] = -((a * a / dx1[i + 1] + b * b / dx1[i]) * sinc[j] * dxi2[j] +
+             (sini[j] / dx2[j + 1] + sini[j - 1] / dx2[j]) * dxi1[i]);
+    c[1] = a * a * sinc[j] * dxi2[j] / dx1[i + 1];
+    c[2] = sini[j] * dxi1[i] / dx2[j + 1];
+    c[3] = 0.0;
+    if (i == 0 && o->xi1s > 0.0) c[0] = c[0] + b * b * sinc[j] * dxi2[j] / dx1[i];
+    if (i == gie) { c[0] = c[0] + c[1] * x1[i] / x1[i + 1]; c[1] = 0.0; }
+    if (j == gje) { c[0] = c[0] + c[2]; c[2] = 0.0; }
+    c[4] = x1[i] * x1[i] * sinc[j] * dxi1[i] * dxi2[j];
+  } else { /* :367-400 */
+    c[0] = -((a * a / dx1[i + 1] + b * b / dx1[i]) * sinc[j] * dxi2[j] * dxi3[k] +
+             (sini[j] / dx2[j + 1] + sini[j - 1] / dx2[j]) * dxi1[i] * dxi3[k] +
+             (idx3[k] + idx3[k + 1]) * dxi1[i] * dxi2[j]);
+    c[1] = a * a * sinc[j] * dxi2[j] * dxi3[k] / dx1[i + 1];
+    c[2] = sini[j] * dxi1[i] * dxi3[k] / dx2[j + 1];
+    c[3] = dxi1[i] * dxi2[j] / dx3[k + 1];
+    if (j == gje) { c[0] = c[0] + c[2]; c[2] = 0.0; }
+    if (i == 0 && o->xi1s > 0.0) c[0] = c[0] + b * b * sinc[j] * dxi2[j] * dxi3[k] / dx1[i];
+    if (i == gie) { c[0] = c[0] + c[1] * x1[i] / x1[i + 1]; c[1] = 0.0; }
+    c[4] = x1[i] * x1[i] * sinc[j] * dxi1[i] * dxi2[j] * dxi3[k];
+  }
+}
+
 static inline int wrap(int s, int n, int per) {
   if (!per) return s;
   if (s < 0) return s + n;
@@ -1173,6 +1244,33 @@ static void get_lapphi_hgsrc(Oracle *o) {
   double fourpiG = 4.0 * M_PI * o->G;
   int px = o->bc[0][0][0] == 0, py = o->bc[1][0][0] == 0, pz = o->bc[2][0][0] == 0;
   const double *ph = o->grvphi;
+  if (o->crdnt == 2) { /* :243-270 with the spherical coefficients; ghosts as hg_boundary_conditions left them */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          double c[5], cxm[5], cym[5], czm[5];
+          lap_coeffs_sph(o, i, j, k, c);
+          lap_coeffs_sph(o, i - 1, j, k, cxm);
+          size_t cc = IX(o, i, j, k);
+          double lap = c[0] * ph[cc];
+          lap = lap + cxm[1] * ph[IX(o, i - 1, j, k)];
+          lap = lap + c[1] * ph[IX(o, i + 1, j, k)];
+          if (ny > 1) {
+            lap_coeffs_sph(o, i, j - 1, k, cym);
+            lap = lap + cym[2] * ph[IX(o, i, j - 1, k)];
+            lap = lap + c[2] * ph[IX(o, i, j + 1, k)];
+          }
+          if (nz > 1) {
+            lap_coeffs_sph(o, i, j, k - 1, czm);
+            lap = lap + czm[3] * ph[IX(o, i, j, wrap(k - 1, nz, pz))];
+            lap = lap + c[3] * ph[IX(o, i, j, wrap(k + 1, nz, pz))];
+          }
+          o->lapphi[cc] = lap / c[4];
+          o->hgsrc[cc] = fourpiG * o->gsrc[cc];
+        }
+    return;
+  }
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < ny; j++)
@@ -1196,6 +1294,28 @@ static void get_lapphi_hgsrc(Oracle *o) {
    phi_g = phi_edge * r_edge / r_g of gravity_hyperbolic.f90:190, applied on
    every non-periodic face; periodic faces copy the opposite edge. */
 static void hg_boundary_conditions(Oracle *o) {
+  if (o->crdnt == 2) { /* gravity_hyperbolic.f90:186-216, gbtype 1 */
+    const int nx = o->n[0], ny = o->n[1], nz = o->n[2];
+    const double *x1 = o->x[0] + 2;
+    double *ph = o->grvphi;
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++) {
+        ph[IX(o, -1, j, k)] = ph[IX(o, 0, j, k)];
+        ph[IX(o, nx, j, k)] = ph[IX(o, nx - 1, j, k)] * x1[nx - 1] / x1[nx];
+      }
+    for (int k = 0; k < nz; k++)
+      for (int i = -1; i <= nx; i++) {
+        ph[IX(o, i, -1, k)] = ph[IX(o, i, 0, k)];
+        ph[IX(o, i, ny, k)] = ph[IX(o, i, ny - 1, k)];
+      }
+    if (nz > 1)
+      for (int j = -1; j <= ny; j++)
+        for (int i = -1; i <= nx; i++) {
+          ph[IX(o, i, j, -1)] = ph[IX(o, i, j, nz - 1)];
+          ph[IX(o, i, j, nz)] = ph[IX(o, i, j, 0)];
+        }
+    return;
+  }
   for (int a = 0; a < 3; a++) {
     int n = o->n[a];
     int per = o->bc[a][0][0] == 0;
@@ -1277,6 +1397,15 @@ void hmo_gravity_setup(Oracle *o, double cgrav_old) {
         double s1 = dxi2[j] * dxi3[k] + dxi2[j] * dxi3[k];
         double s2 = dxi1[i] * dxi3[k] + dxi1[i] * dxi3[k];
         double s3 = dxi1[i] * dxi2[j] + dxi1[i] * dxi2[j];
+        if (o->crdnt == 2) { /* dtgrav_cell with metric.f90:117-130 */
+          const double *xi = o->xi[0] + 2, *si = o->sini + 2, *ci = o->cosi + 2;
+          const double fj = o->fac_j, fk = o->fac_k, a = xi[i], b = xi[i - 1];
+          dvol = (a * a * a - b * b * b) / 3.0 * (ci[j - 1] - ci[j]) * dxi3[k] * fj * fk;
+          s1 = 0.5 * (b * b) * (ci[j - 1] - ci[j]) * dxi3[k] * fj * fk +
+               0.5 * (a * a) * (ci[j - 1] - ci[j]) * dxi3[k] * fj * fk;
+          s2 = 0.5 * si[j - 1] * (a * a - b * b) * dxi3[k] * fk + 0.5 * si[j] * (a * a - b * b) * dxi3[k] * fk;
+          s3 = 0.5 * (a * a - b * b) * dxi2[j] * fj + 0.5 * (a * a - b * b) * dxi2[j] * fj;
+        }
         double v = dvol / (1.0 * (off[0] * s1 + off[1] * s2 + off[2] * s3));
         m = fmin2(m, v);
       }

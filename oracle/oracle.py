@@ -152,9 +152,9 @@ class Oracle:
 
     def metric(self) -> dict:
         """Spherical metric factors: detg1, idetg1, sx1 (n0+4) and sini,
-        cosi, scot (n1+4)."""
+        cosi, scot, sinc, sisin (n1+4)."""
         out = {}
-        for w, name in enumerate(("detg1", "idetg1", "sx1", "sini", "cosi", "scot")):
+        for w, name in enumerate(("detg1", "idetg1", "sx1", "sini", "cosi", "scot", "sinc", "sisin")):
             a = np.zeros(self.cfg["n"][0 if w < 3 else 1] + 4)
             lib().hmo_get_metric(self.h, w, _dp(a))
             out[name] = a

@@ -122,3 +122,14 @@ def spherical(n=(24, 16, 1), mag=True, seed=5, xi1s=0.0, imesh=0, limiter="modif
         prims["b2"][:] = -0.2 * np.sin(th) + 0.02 * rng.uniform(-1.0, 1.0, shape)
         prims["b3"][:] = 0.02 * np.sin(th) * rng.uniform(-1.0, 1.0, shape)
     return cfg, prims
+
+
+def polytrope_spherical(n=(24, 12, 8), xi1s=0.0, xi1e=2.0, imesh=0):
+    """The n=1 polytrope on a spherical polar grid with hyperbolic
+    self-gravity (Robin outer boundary, gbtype=1)."""
+    ov = dict(ie=n[0], je=n[1], ke=n[2], crdnt=2, mag_on=False, gamma=2.0, gravswitch=3, gbtype=1, G=1.0,
+              courant=0.9, xi1s=xi1s, xi1e=xi1e, imesh=imesh, x1min=0.02, t_end=1.0, dt_out=1.0,
+              bc1is=1, bc1iv=1, bc1os=2, bc1ov=2)
+    cfg = config.resolve("polytrope_sph", overrides=ov)
+    prims, phi = ic.polytrope_n1_spherical(cfg, G.make_grid(cfg))
+    return cfg, prims, phi

@@ -103,9 +103,11 @@ def test_geometric_mesh_matches_the_oracle_restatement():
     assert abs(grid[0]["xi"][-3] - 1.0) < 1e-9  # the last face lands on xi1e
 
 
-@pytest.mark.parametrize("n,imesh,xi1s", [((500, 1, 1), 0, 0.0), ((24, 16, 1), 0, 0.0), ((16, 12, 8), 0, 0.0),
-                                          ((20, 1, 8), 1, 0.1), ((10, 5, 4), 0, 0.2)])
-def test_spherical_grid_matches_the_oracle_restatement(n, imesh, xi1s):
+@pytest.mark.parametrize("n,imesh,xi1s,grav", [((500, 1, 1), 0, 0.0, 0), ((24, 16, 1), 0, 0.0, 0),
+                                               ((16, 12, 8), 0, 0.0, 0), ((20, 1, 8), 1, 0.1, 0),
+                                               ((10, 5, 4), 0, 0.2, 0), ((20, 16, 1), 1, 0.1, 3),
+                                               ((16, 8, 8), 0, 0.2, 3)])
+def test_spherical_grid_matches_the_oracle_restatement(n, imesh, xi1s, grav):
     """crdnt=2 (gridset.f90:294-423, metric.f90:102-151): the host's axes,
     volumetric centres, quad-precision sin/cos and metric factors equal the
     oracle's C restatement (which uses libquadmath) bit for bit."""
@@ -115,7 +117,7 @@ def test_spherical_grid_matches_the_oracle_restatement(n, imesh, xi1s):
     from oracle.oracle import Oracle
 
     cfg = config.resolve("spherical", overrides=dict(ie=n[0], je=n[1], ke=n[2], crdnt=2, xi1s=xi1s, xi1e=1.0,
-                                                      imesh=imesh, x1min=0.03))
+                                                      imesh=imesh, x1min=0.03, gravswitch=grav, gbtype=1))
     assert cfg["bc"][1].tolist() == ([[1, 1], [1, 1]] if n[1] > 1 else [[3, 3], [3, 3]])
     grid = G.make_grid(cfg)
     o = Oracle(cfg)
@@ -125,7 +127,8 @@ def test_spherical_grid_matches_the_oracle_restatement(n, imesh, xi1s):
             assert np.array_equal(ax[k], grid[a][k]), (a, k)
     m = o.metric()
     for name, a, key in (("detg1", 0, "detg"), ("idetg1", 0, "idetg"), ("sx1", 0, "sx"),
-                         ("sini", 1, "sini"), ("cosi", 1, "cosi"), ("scot", 1, "scot")):
+                         ("sini", 1, "sini"), ("cosi", 1, "cosi"), ("scot", 1, "scot"),
+                         ("sinc", 1, "sinc"), ("sisin", 1, "sisin")):
         assert np.array_equal(m[name], grid[a][key]), name
     dv = G.spherical_dvol(grid, cfg["n"])
     full = 4.0 / 3.0 * np.pi * (1.0 - xi1s ** 3)

@@ -207,3 +207,15 @@ def test_spherical_coordinates(make):
     (timestep.f90:175-178 with metric.f90:117-130), bitwise vs the oracle."""
     cfg, prims = make()
     run_pair(cfg, prims, 12)
+
+
+@pytest.mark.parametrize("n,xi1s", [((24, 12, 8), 0.0), ((20, 16, 1), 0.1), ((16, 8, 8), 0.2)],
+                         ids=["3d-from-origin", "r-theta-shell", "3d-shell"])
+def test_spherical_self_gravity(n, xi1s):
+    """Hyperbolic self-gravity on spherical grids: the Laplacian of
+    setup_grv_hyperbolic (axisymmetric and 3-D, Robin outer radius, the
+    inner-radius term of a shell and its ghost held through the
+    sub-cycles), the spherical gravity source terms and dtg_unit, bitwise
+    against the oracle with the potential compared at the end."""
+    cfg, prims, phi = cases.polytrope_spherical(n, xi1s=xi1s)
+    run_pair(cfg, prims, 8, grvphi=phi)
