@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope", "briowu", "sedov"], default="ot3d",
+    ap.add_argument("--workload", choices=["ot3d", "kh-batch", "serve", "polytrope", "polytrope-sph", "briowu", "sedov"], default="ot3d",
                     help="ot3d: the headline (3-D Orszag-Tang 256^3); kh-batch: 512 uneven 2-D KH boxes batched vs "
                          "one at a time; serve: a Poisson request stream through the continuous-batching server; "
                          "polytrope: 192^3 self-gravitating polytrope with hyperbolic gravity")
@@ -619,6 +619,91 @@ def run_polytrope(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def poly_sph_config(n, xi1s=0.1):
+    from hormone_b200 import config
+
+    ov = dict(ie=n[0], je=n[1], ke=n[2], crdnt=2, mag_on=False, gamma=2.0, gravswitch=3, gbtype=1, G=1.0,
+              courant=0.9, xi1s=xi1s, xi1e=2.0, t_end=1e30, dt_out=1e30, bc1is=1, bc1iv=1, bc1os=2, bc1ov=2)
+    return config.resolve("polytrope_sph", overrides=ov)
+
+
+def run_polytrope_sph(args, rank, world, local_rank):
+    """The n=1 polytrope on a 3-D spherical polar grid (r in [0.1, 2], full
+    theta and phi; 160 x 80 x 160 cells) with hyperbolic self-gravity, FP64:
+    zone-updates/s over the timed steps (CFL + gravity sub-cycles + 3 fused
+    stages), mass drift, and the L1 error against the oracle on a 48 x 24 x 32
+    grid of the same set-up over 40 steps."""
+    import numpy as np
+    import torch
+
+    from hormone_b200 import grid as G, ic
+    from hormone_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    n = (160, 80, 160)
+    cfg = poly_sph_config(n)
+    grid = G.make_grid(cfg)
+    prims, phi = ic.polytrope_n1_spherical(cfg, grid)
+    dv = G.spherical_dvol(grid, cfg["n"])
+    sim = Simulation(cfg, prims, grvphi=phi)
+    stream = torch.cuda.ExternalStream(sim.ctx.stream_ptr())
+    mass0 = float(np.sum(sim.state()["u"][0] * dv))
+    sim.run(max_steps=args.warmup)
+    torch.cuda.synchronize()
+    sim.ctx.sync()
+    steps = args.steps * 20
+    l0 = sim.ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        sim.run(max_steps=steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = sim.ctx.launches() - l0
+    mass1 = float(np.sum(sim.state()["u"][0] * dv))
+    t_sim = sim.time
+    sim.close()
+    cells = n[0] * n[1] * n[2]
+    l1 = cpu = None
+    if not args.no_cpu:
+        from oracle.oracle import Oracle
+
+        m = (48, 24, 32)
+        c2 = poly_sph_config(m)
+        p2, f2 = ic.polytrope_n1_spherical(c2, G.make_grid(c2))
+        o = Oracle(c2)
+        o.set_prims(p2)
+        o.set_gravity_state(f2, None, 0.0)
+        o.start()
+        s2 = Simulation(c2, p2, grvphi=f2)
+        k = 40
+        t0 = time.perf_counter()
+        for _ in range(k):
+            o.step()
+        el = time.perf_counter() - t0
+        s2.run(max_steps=k)
+        a, b = s2.state()["u"], o.u()
+        s2.close()
+        l1 = {name: float(np.sum(np.abs(a[q] - b[q])) / max(np.sum(np.abs(b[q])), 1e-300))
+              for q, name in enumerate(("rho", "m1", "m2", "m3", "E"))}
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": m[0] * m[1] * m[2] * k / el, "unit": METRIC, "cores": cores, "kind": "port",
+               "sample": f"{m[0]}x{m[1]}x{m[2]} grid of the same set-up, {k} steps ({el:.1f} s) of the CPU "
+                         "restatement, OpenMP"}
+    line = {"metric": METRIC, "value": cells * steps / (ms * 1e-3), "unit": METRIC, "n_gpus": 1, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"polytrope-n1-spherical-hyperbolic-gravity-{n[0]}x{n[1]}x{n[2]}",
+                       "crdnt": 2, "r": [0.1, 2.0], "G": 1.0, "K": 2 / math.pi, "gamma": 2.0,
+                       "HGfac": cfg["HGfac"], "hgcfl": cfg["hgcfl"], "gbtype": 1,
+                       "l2": "inputs larger than L2 (5 x 8 B x 2.05 M cells per RK buffer, 8 coefficient planes)"},
+            "polytrope": {"t": t_sim, "mass_drift": (mass1 - mass0) / mass0, "l1_vs_oracle_48x24x32_40_steps": l1},
+            "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_briowu(args, rank=0, world=1, local_rank=0):
     """The Brio-Wu shock tube of the benchmark list (1024 cells on [0,1],
     gamma=2, Bx=0.75, minmod, CFL 0.4, to t=0.1): time to solution of the
@@ -804,6 +889,8 @@ def main():
             run_kh_batch(args, rank, world, local_rank)
         elif args.workload == "serve":
             run_serve(args, rank, world, local_rank)
+        elif args.workload == "polytrope-sph":
+            run_polytrope_sph(args, rank, world, local_rank)
         elif args.workload == "polytrope":
             run_polytrope(args, rank, world, local_rank)
         elif args.workload == "briowu":
