@@ -81,7 +81,7 @@ class Batch:
         (pool memory or slots exhausted)."""
         L = capi.lib()
         if int(cfg.get("crdnt", 0)) != 0:
-            raise ValueError("batches hold Cartesian grids; a spherical grid runs as its own Simulation")
+            raise ValueError("batches hold Cartesian grids; a curvilinear grid runs as its own Simulation")
         grid = grid if grid is not None else gridmod.make_grid(cfg)
         if prims is None:
             prims = ic.make(cfg, grid)

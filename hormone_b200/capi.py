@@ -168,21 +168,23 @@ class Context:
         if rc != 0:
             raise HmnError(rc, "hmn_create")
         self.h = h
-        if int(cfg.get("crdnt", 0)) == 2:
-            self.set_metric(grid)
+        if int(cfg.get("crdnt", 0)) in (1, 2):
+            self.set_metric(grid, int(cfg["crdnt"]))
 
-    def set_metric(self, grid):
-        """Spherical metric factors (metric.f90:102-151) from the grid's
-        ``detg``/``idetg``/``sx`` (r) and ``sini``/``cosi``/``scot``/``sinc``/
-        ``sisin`` (theta)."""
+    def set_metric(self, grid, crdnt: int = 2):
+        """Curvilinear metric factors (metric.f90:53-151) from the grid's
+        ``detg``/``idetg``/``sx`` (r) and, spherical, ``sini``/``cosi``/
+        ``scot``/``sinc``/``sisin`` (theta)."""
         m = HmnMetric()
         self._metric_arrays = []
         for field, a, k in (("detg1", 0, "detg"), ("idetg1", 0, "idetg"), ("sx1", 0, "sx"), ("sini", 1, "sini"),
                             ("cosi", 1, "cosi"), ("scot", 1, "scot"), ("sinc", 1, "sinc"), ("sisin", 1, "sisin")):
+            if k not in grid[a]:  # the theta factors of a cylindrical grid
+                continue
             v = np.ascontiguousarray(grid[a][k], dtype=np.float64)
             self._metric_arrays.append(v)
             setattr(m, field, _dp(v))
-        self._check(lib().hmn_set_metric(self.h, 2, ctypes.byref(m)), "hmn_set_metric")
+        self._check(lib().hmn_set_metric(self.h, crdnt, ctypes.byref(m)), "hmn_set_metric")
 
     def close(self):
         if getattr(self, "h", None):

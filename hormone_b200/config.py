@@ -204,8 +204,11 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     if dim == 0:
         raise ValueError("Error from gridset: no direction to solve")
     crdnt = int(cfg.get("crdnt", 0))
-    if crdnt not in (0, 2):
-        raise ValueError("Cartesian (crdnt=0) and spherical (crdnt=2) coordinates are on this path")
+    if crdnt not in (0, 1, 2):
+        raise ValueError("Cartesian (0), cylindrical (1) and spherical (2) coordinates are on this path")
+    if crdnt == 1 and n[1] != 1:
+        raise ValueError("cylindrical grids with a solved phi axis are not on this path (gridset reads an unset "
+                         "width for their phi ghosts); use one phi cell (axisymmetric R-z)")
     if int(cfg.get("eostype", 0)) != 0:
         raise ValueError("only the ideal-gas EOS (eostype=0) is on this path")
     mag_on = bool(cfg["mag_on"])
@@ -221,6 +224,8 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
             x, y = bc[a, 0, sv], bc[a, 1, sv]
             if x * y == 0 and x + y != 0:
                 raise ValueError(f"boundary condition axis {a + 1}: both sides must be periodic")
+    if crdnt == 1:  # periodic phi (checksetup.f90:110-111)
+        bc[1] = 0
     if crdnt == 2:  # polar boundaries (checksetup.f90:112-115, :134-137)
         bc[1] = 1
         bc[2] = 0
@@ -256,9 +261,11 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     nspc = int(cfg.get("spn", 0)) if comp == 2 else 0
     if nspc < 0 or nspc > 4:
         raise ValueError("at most 4 passive scalars are on this path")
-    if crdnt == 2 and nspc:
-        raise ValueError("passive scalars on spherical grids are not on this path")
+    if crdnt and nspc:
+        raise ValueError("passive scalars on curvilinear grids are not on this path")
     grav = int(cfg.get("gravswitch", 0))
+    if crdnt == 1 and grav:
+        raise ValueError("self-gravity on cylindrical grids is not on this path")
     if crdnt == 2 and grav:
         # setup_grv_hyperbolic (gravity_hyperbolic.f90:336-405) has spherical
         # coefficients for (r, theta) with one phi cell and for 3-D grids; the
@@ -277,6 +284,8 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
         half = n[1] == 1 or bool(cfg.get("eq_sym", False))
         extent[1] = (0.0, math.pi * 0.5 if half else math.pi)
         extent[2] = (-math.pi, math.pi)
+    if crdnt == 1:  # a quarter turn of phi for one phi cell (gridset.f90:209-231)
+        extent[1] = (extent[1][0], extent[1][0] + 2.0 * math.pi / 4.0)
     cfg.update(
         n=n, solve=solve, dim=dim, mag_on=mag_on, glm=glm, nvar=nvar, bc=bc, crdnt=crdnt,
         extent=extent,

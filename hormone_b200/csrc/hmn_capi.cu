@@ -529,6 +529,42 @@ static void sph_lap_coeffs(const hmn_ctx* ctx, const double* sinc, const double*
   }
 }
 
+// metric.f90:53-100 for cylindrical coordinates with one phi cell (the
+// axisymmetric R-z form; a solved phi axis is refused because gridset
+// reads an unset width dxi2(js-2) for its ghost centres); no gravity or
+// passive scalars
+static int set_cylindrical(hmn_ctx* ctx, const hmn_metric* mt) {
+  if (!mt || !mt->detg1 || !mt->idetg1 || !mt->sx1) return HMN_EINVAL;
+  if (ctx->n[1] != 1 || ctx->par.gravswitch != 0 || ctx->par.nspc != 0 || !ctx->solve[0]) return HMN_EBADCFG;
+  const int L1 = ctx->n[0] + 4;
+  std::vector<double> h((size_t)6 * L1, 0.0);
+  double *g1 = h.data(), *ig1 = g1 + L1, *s1 = ig1 + L1, *ar2 = s1 + 3 * L1;
+  const double* xi = ctx->xi1_h;
+  for (int s = 0; s < L1; s++) {
+    g1[s] = mt->detg1[s];
+    ig1[s] = mt->idetg1[s];
+    s1[s] = mt->sx1[s];
+    if (s > 0) ar2[s] = xi[s] * xi[s] - xi[s - 1] * xi[s - 1];
+  }
+  cudaFree(ctx->sphbuf);  // sized for this coordinate system
+  ctx->sphbuf = nullptr;
+  CK(cudaMalloc((void**)&ctx->sphbuf, h.size() * sizeof(double)), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->sphbuf, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st), "metric");
+  CK(cudaStreamSynchronize(ctx->st), "metric");
+  SphGeo M{};
+  const double* b = ctx->sphbuf;
+  M.detg1 = b;
+  M.idetg1 = b + L1;
+  M.sx1 = b + 2 * L1;
+  M.ar2 = b + 5 * L1;
+  M.fac_j = 4.0;
+  M.fac_k = 1.0;
+  M.crd = 1;
+  M.on = 1;
+  ctx->G.sph = M;
+  return HMN_OK;
+}
+
 // metric.f90:102-151 for spherical polar coordinates: the caller's 1-D
 // factors plus the radial and polar products the kernels form the 2-D and
 // 3-D factors from (same single IEEE operations as the reference); with
@@ -540,6 +576,7 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
     ctx->G.sph = SphGeo{};
     return HMN_OK;
   }
+  if (crdnt == 1) return set_cylindrical(ctx, mt);
   if (crdnt != 2) return HMN_EBADCFG;
   if (!mt || !mt->detg1 || !mt->idetg1 || !mt->sx1 || !mt->sini || !mt->cosi || !mt->scot) return HMN_EINVAL;
   // single grids without passive scalars (either precision); r solved; self-gravity
@@ -571,7 +608,9 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
       cd[s] = mt->cosi[s - 1] - mt->cosi[s];
     }
   }
-  if (!ctx->sphbuf) CK(cudaMalloc((void**)&ctx->sphbuf, h.size() * sizeof(double)), "cudaMalloc");
+  cudaFree(ctx->sphbuf);  // sized for this coordinate system
+  ctx->sphbuf = nullptr;
+  CK(cudaMalloc((void**)&ctx->sphbuf, h.size() * sizeof(double)), "cudaMalloc");
   CK(cudaMemcpyAsync(ctx->sphbuf, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st), "metric");
   CK(cudaStreamSynchronize(ctx->st), "metric");
   SphGeo& M = ctx->G.sph;
@@ -589,6 +628,7 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
   M.sisin = M.sini + 4 * L2;
   M.fac_j = ctx->n[1] == 1 ? 2.0 : 1.0;
   M.fac_k = ctx->n[2] == 1 ? 4.0 : 1.0;
+  M.crd = 2;
   M.on = 1;
   ctx->xi1s = xi[1];  // xi1(is-1)
   if (grav) {

@@ -33,17 +33,20 @@ struct AxisGeo {
 };
 constexpr int kGeoArrays = 15;
 
-// Spherical polar coordinates (r, theta, phi as axes 1-3): the 1-D factors
-// of the metric (metric.f90:102-151), each at offset +2 like the axis
-// arrays.  The 2-D and 3-D factors of the reference (idetg2, idetg3, dvol,
-// sa1..3) are formed from them per cell in the reference's operation order.
-// on = 0 for Cartesian grids.
+// Curvilinear coordinates: spherical polar (crd 2; r, theta, phi as axes
+// 1-3) or cylindrical with one phi cell (crd 1; R, phi, z).  The 1-D
+// factors of the metric (metric.f90:53-151), each at offset +2 like the
+// axis arrays.  The 2-D and 3-D factors of the reference (idetg2, idetg3,
+// dvol, sa1..3) are formed from them per cell in the reference's operation
+// order.  on = 0 for Cartesian grids; the theta arrays are unset for crd 1.
 struct SphGeo {
   int on;
-  double fac_j, fac_k;   // 2 for a single theta cell, 4 for a single phi cell, else 1
-  const double* detg1;   // xi1(i)^2: weight of the r flux through the high face of cell i
-  const double* idetg1;  // 3 / (dxi1 (xi1(i)^2 + xi1(i) xi1(i-1) + xi1(i-1)^2))
-  const double* sx1;     // 1.5 (xi1(i) + xi1(i-1)) / (same sum of squares)
+  int crd;
+  double fac_j, fac_k;   // spherical: 2 for a single theta cell, 4 for a single phi cell, else 1;
+                         // cylindrical: fac_j = 4 (dvol, sa1, sa3 of the single phi cell)
+  const double* detg1;   // weight of the r flux through the high face of cell i: xi1^2 (xi1 cylindrical)
+  const double* idetg1;  // 3 / (dxi1 (xi1(i)^2 + xi1(i) xi1(i-1) + xi1(i-1)^2)) (2 / (xi1(i)^2 - xi1(i-1)^2))
+  const double* sx1;     // 1.5 (xi1(i) + xi1(i-1)) / (same sum of squares) (2 / (xi1(i) + xi1(i-1)))
   const double* vr;      // (xi1(i)^3 - xi1(i-1)^3) / 3: radial factor of dvol
   const double* hr2;     // 0.5 xi1(i)^2: radial factor of sa1
   const double* ar2;     // xi1(i)^2 - xi1(i-1)^2: radial factor of sa2, sa3

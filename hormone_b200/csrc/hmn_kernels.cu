@@ -483,7 +483,14 @@ __device__ __forceinline__ bool cfl_cell(const GridDev& G, const double* P, size
     cf3 = cs + fabs(v3);
   }
   const double dxi1 = G.g[0].dxi[i + 2], dxi2 = G.g[1].dxi[j + 2], dxi3 = G.g[2].dxi[k + 2];
-  if (G.sph.on) {  // metric.f90:117-130
+  if (G.sph.on && G.sph.crd == 1) {  // metric.f90:80-96, one phi cell: dvol, sa1, sa3 times four
+    const SphGeo& M = G.sph;
+    const double ar = M.ar2[i + 2], f4 = M.fac_j;
+    const double dvol = 0.5 * ar * dxi2 * dxi3 * f4;
+    const double sa1m = M.detg1[i + 1] * dxi2 * dxi3 * f4, sa1p = M.detg1[i + 2] * dxi2 * dxi3 * f4;
+    const double sa2 = dxi1 * dxi3, sa3 = 0.5 * ar * dxi2 * f4;
+    dti = dvol / (cf1 * off0 * (sa1m + sa1p) + cf2 * off1 * (sa2 + sa2) + cf3 * off2 * (sa3 + sa3));
+  } else if (G.sph.on) {  // metric.f90:117-130
     const SphGeo& M = G.sph;
     const double cd = M.cd[j + 2], fj = M.fac_j, fk = M.fac_k, ar = M.ar2[i + 2];
     const double dvol = M.vr[i + 2] * cd * dxi3 * fj * fk;

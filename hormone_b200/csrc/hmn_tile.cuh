@@ -482,8 +482,9 @@ __device__ __forceinline__ void sph_div_weights(const GridDev& G, int i, int j, 
     cw = M.ra2[j + 2] * M.sx1[i + 2];
     fm = M.sini[j + 1];
     fp = M.sini[j + 2];
-  } else {  // idetg3 = idetg2 * dxi2 * idxi3 / fac_k
-    cw = M.ra2[j + 2] * M.sx1[i + 2] * G.g[1].dxi[j + 2] * G.g[2].idxi[k + 2] / M.fac_k;
+  } else {  // idetg3 = idetg2 * dxi2 * idxi3 / fac_k (spherical), idxi3 (cylindrical)
+    cw = M.crd == 1 ? G.g[2].idxi[k + 2]
+                    : M.ra2[j + 2] * M.sx1[i + 2] * G.g[1].dxi[j + 2] * G.g[2].idxi[k + 2] / M.fac_k;
     fm = 1.0;
     fp = 1.0;
   }
@@ -550,6 +551,19 @@ __device__ __forceinline__ void sph_sources(const GridDev& G, const StageArgs& A
     b2 = A.pin[(PB + 1) * pl + c];
     b3 = A.pin[(PB + 2) * pl + c];
     pt = pt + 0.5 * (b1 * b1 + b2 * b2 + b3 * b3);
+  }
+  if (M.crd == 1) {  // cylindrical (source.f90:88-111; phi unsolved, no gravity)
+    const double s1 = M.sx1[i + 2];
+    double r1 = (d * v2 * v2 + pt) * s1;
+    double r2 = -(d * v1 * v2 * s1);
+    if (MAG) {
+      r1 = r1 - b2 * b2 * s1;
+      r2 = r2 + b1 * b2 * s1;
+      acc[6] = acc[6] + (b1 * v3 - b3 * v1) * s1;
+    }
+    acc[1] = acc[1] + r1;
+    acc[2] = acc[2] + r2;
+    return;
   }
   const double s1 = M.sx1[i + 2], sc = M.scot[j + 2];
   double r1 = (d * (v2 * v2 + v3 * v3) + 2.0 * pt) * s1;

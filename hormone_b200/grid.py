@@ -212,11 +212,56 @@ def spherical_grid(cfg) -> List[Dict[str, np.ndarray]]:
     return [r, th, ph]
 
 
+def cylindrical_grid(cfg) -> List[Dict[str, np.ndarray]]:
+    """Cylindrical axes (crdnt=1: R, phi, z) with one phi cell, as
+    gridset.f90:145-292 builds them without gravity: R uniform or a
+    geometrical series with the volumetric centres
+    sqrt((xi1(i-1)^2 + xi1(i)^2)/2) (the ghost below the first face
+    mirrored), a quarter turn of phi, z uniform or a geometrical series; and
+    the metric factors of metric.f90:53-100 on axis 0: ``detg`` (xi1),
+    ``idetg`` (2/(xi1(i)^2-xi1(i-1)^2)) and ``sx`` (2/(xi1(i)+xi1(i-1)))."""
+    n1, n2, n3 = (int(v) for v in cfg["n"])
+    if n2 != 1:
+        raise ValueError("cylindrical grids take one phi cell on this path")
+    out = []
+    for a, (mesh_key, min_key) in ((0, MESH_KEYS[0]), (2, MESH_KEYS[2])):
+        n, (lo, hi) = cfg["n"][a], cfg["extent"][a]
+        mesh = int(cfg.get(mesh_key, 0)) if n > 1 else 0
+        if mesh == 0:
+            widths = [(hi - lo) / float(n)] * (n + 4)
+        elif mesh == 1:
+            widths = geometric_widths(n, lo, hi, float(cfg[min_key]))
+        else:
+            raise ValueError(f"{mesh_key}={mesh}: only uniform (0) and geometrical-series (1) meshes are on this path")
+        out.append(axis_from_widths(widths, lo))
+    r, z = out
+    x, xi, dx, idx = (r[k].tolist() for k in ("x", "xi", "dx", "idx"))
+    for s in range(1, n1 + 4):  # Fortran is-1 .. ie+2 (:187-193)
+        x[s] = math.sqrt((xi[s - 1] * xi[s - 1] + xi[s] * xi[s]) * 5e-1)
+        if s == 1:
+            x[s] = -x[s]
+        dx[s] = x[s] - x[s - 1]
+        idx[s] = 1.0 / dx[s]
+    detg, idetg, sx = [0.0] * (n1 + 4), [0.0] * (n1 + 4), [0.0] * (n1 + 4)
+    for s in range(1, n1 + 3):
+        a, b = xi[s], xi[s - 1]
+        detg[s] = a
+        idetg[s] = 2.0 / (a * a - b * b)
+        sx[s] = 2.0 / (a + b)
+    r.update(x=np.array(x), dx=np.array(dx), idx=np.array(idx), detg=np.array(detg), idetg=np.array(idetg),
+             sx=np.array(sx))
+    ph = axis_from_widths([2.0 * math.pi / 4.0] * (n2 + 4), float(cfg["extent"][1][0]))
+    return [r, ph, z]
+
+
 def make_grid(cfg) -> List[Dict[str, np.ndarray]]:
     """The three axes of gridset.f90: uniform (mesh 0) or geometrical series
-    (mesh 1, first cell x?min wide); spherical polar with crdnt=2."""
+    (mesh 1, first cell x?min wide); cylindrical with crdnt=1, spherical
+    polar with crdnt=2."""
     if int(cfg.get("crdnt", 0)) == 2:
         return spherical_grid(cfg)
+    if int(cfg.get("crdnt", 0)) == 1:
+        return cylindrical_grid(cfg)
     grav = int(cfg.get("gravswitch", 0)) != 0
     out = []
     for a in range(3):

@@ -87,7 +87,9 @@ typedef struct {
 } hmn_metric;
 
 /* Sets the coordinate system; crdnt 0 (Cartesian, the default) takes no
- * arrays.  The kernels form idetg2, idetg3, dvol and sa1..3 from the 1-D
+ * arrays, crdnt 1 (cylindrical R, phi, z; metric.f90:53-100) only detg1,
+ * idetg1 and sx1, and needs one phi cell (gridset.f90:209-231 reads an
+ * unset width for the ghosts of a solved phi axis) and no gravity.  The kernels form idetg2, idetg3, dvol and sa1..3 from the 1-D
  * factors in the reference's operation order, and with gravswitch 3 the
  * spherical Laplacian coefficients of setup_grv_hyperbolic
  * (gravity_hyperbolic.f90:336-405; (r, theta) with one phi cell, or 3-D;

@@ -16,15 +16,18 @@
  * src/main/tests.f90:46-292.
  *
  *   grid            src/main/gridset.f90:40-80 (uniform Cartesian),
- *                   :294-423 (spherical polar r, theta, phi)
- *   metric          src/main/metric.f90:26-51 (Cartesian), :102-151 (spherical)
+ *                   :294-423 (spherical polar r, theta, phi), :145-292
+ *                   (cylindrical R, phi, z without a solved phi)
+ *   metric          src/main/metric.f90:26-51 (Cartesian), :53-100
+ *                   (cylindrical), :102-151 (spherical)
  *   limiters        src/main/fluxlimiter.f90:94-129
  *   slopes          src/main/interpolation.f90:49-484
  *   face fluxes     src/main/numflux.f90:46-563
  *   HLLD + GLM      src/main/hlldflux.f90:19-179
  *   EOS (ideal)     src/main/eos.f90:195-274,351-365,742-866
- *   source          src/main/source.f90:14-85,177-228; spherical geometric
- *                   terms :113-143, pinned by tests/sedov_default[_flat].bin
+ *   source          src/main/source.f90:14-85,177-228; cylindrical geometric
+ *                   terms :88-111; spherical :113-150, pinned by
+ *                   tests/sedov_default[_flat].bin
  *   RK + primitive  src/main/rungekutta.f90:16-232
  *   boundaries      src/main/boundarycondition.f90:14-1442 (codes 0-3; 4/5
  *                   linear extrapolation as :302-327,419-468; 9 Dirichlet
@@ -393,6 +396,62 @@ int hmo_make_spherical(Oracle *o, int imesh, double xi1s, double xi1e, double x1
   o->fac_k = n3 == 1 ? 4.0 : 1.0;
   o->fac_j = n2 == 1 ? 2.0 : 1.0;
   o->crdnt = 2;
+  return HMO_OK;
+}
+
+/* Cylindrical grid (crdnt=1) without gravity and with phi unsolved (one
+   phi cell): R from xi1s (uniform, or a geometrical series) with the
+   volumetric centres sqrt((xi1(i-1)^2 + xi1(i)^2)/2), a quarter turn of
+   phi, z from xi3s to xi3e (uniform or geometrical series); then the metric
+   of metric.f90:53-100 (gridset.f90:145-292).  A solved phi axis is
+   refused: gridset reads an unset width dxi2(js-2) for its ghost centres. */
+int hmo_make_cylindrical(Oracle *o, int imesh, double xi1s, double xi1e, double x1min, int kmesh, double xi3s,
+                         double xi3e, double x3min) {
+  const int n1 = o->n[0], n2 = o->n[1], n3 = o->n[2];
+  if (o->gravswitch != 0 || n2 != 1) return HMO_EBADCFG;
+  const double pi = acos(-1.0);
+  int nmax = n1 > n3 ? n1 : n3;
+  double *w = zalloc((size_t)nmax + 4);
+  if (imesh == 1) {
+    int rc = geometric_widths(n1, xi1s, xi1e, x1min, w);
+    if (rc) { free(w); return rc; }
+  } else {
+    for (int i = 0; i < n1 + 4; i++) w[i] = (xi1e - xi1s) / (double)n1;
+  }
+  make_axis(o, 0, xi1s, w, 0);
+  {
+    double *x = o->x[0] + 2, *xi = o->xi[0] + 2, *dx = o->dx[0] + 2, *idx = o->idx[0] + 2;
+    for (int i = -1; i <= n1 + 1; i++) { /* :187-193 */
+      x[i] = sqrt((xi[i - 1] * xi[i - 1] + xi[i] * xi[i]) * 5e-1);
+      if (i == -1) x[i] = -x[i];
+      dx[i] = x[i] - x[i - 1];
+      idx[i] = 1.0 / dx[i];
+    }
+  }
+  /* phi: four cells of the full turn stand for one (:209-231) */
+  for (int j = 0; j < n2 + 4; j++) w[j] = 2.0 * pi / 4.0;
+  make_axis(o, 1, 0.0, w, 0);
+  /* z */
+  if (kmesh == 1 && n3 > 1) {
+    int rc = geometric_widths(n3, xi3s, xi3e, x3min, w);
+    if (rc) { free(w); return rc; }
+  } else {
+    for (int k = 0; k < n3 + 4; k++) w[k] = (xi3e - xi3s) / (double)n3;
+  }
+  make_axis(o, 2, xi3s, w, 0);
+  free(w);
+  { /* metric.f90:53-100 */
+    const double *xi = o->xi[0] + 2;
+    double *g1 = o->detg1 + 2, *ig1 = o->idetg1 + 2, *s1 = o->sx1 + 2;
+    for (int i = -1; i <= n1; i++) {
+      g1[i] = xi[i];
+      ig1[i] = 2.0 / (xi[i] * xi[i] - xi[i - 1] * xi[i - 1]);
+      s1[i] = 2.0 / (xi[i] + xi[i - 1]);
+    }
+  }
+  o->fac_j = 4.0; /* dvol, sa1, sa3 of one phi cell times four (:92-96) */
+  o->fac_k = 1.0;
+  o->crdnt = 1;
   return HMO_OK;
 }
 
@@ -932,6 +991,20 @@ static void source(Oracle *o) {
       for (int i = 0; i < nx; i++) {
         size_t c = IX(o, i, j, k);
         for (int q = 0; q < 9; q++) o->src[q][c] = 0.0;
+        if (o->crdnt == 1) {
+          /* cylindrical geometric terms (source.f90:88-111) */
+          const double d = o->d[c], v1 = o->v[0][c], v2 = o->v[1][c], v3 = o->v[2][c], pt = o->ptot[c];
+          const double s1 = o->sx1[i + 2];
+          o->src[IMO1][c] = (d * v2 * v2 + pt) * s1;
+          o->src[IMO2][c] = -(d * v1 * v2 * s1);
+          if (o->mag_on) {
+            const double b1 = o->b[0][c], b2 = o->b[1][c], b3 = o->b[2][c];
+            o->src[IMO1][c] = o->src[IMO1][c] - b2 * b2 * s1;
+            o->src[IMO2][c] = o->src[IMO2][c] + b1 * b2 * s1;
+            o->src[IMG2][c] = (b1 * v3 - b3 * v1) * s1;
+          }
+          continue;
+        }
         if (o->crdnt == 2) {
           /* spherical geometric terms (source.f90:113-143; no gravity here) */
           const double d = o->d[c], v1 = o->v[0][c], v2 = o->v[1][c], v3 = o->v[2][c], pt = o->ptot[c];
@@ -1016,6 +1089,17 @@ static void rungekutta(Oracle *o) {
         for (int i = 0; i < nx; i++) {
           size_t c = IX(o, i, j, k);
           if (o->rungen == 1) UO[c] = U[c];
+          if (o->crdnt == 1) {
+            /* idetg1 (detg1 = xi1) along R; idetg2 = idxi2/x1 (never used: phi is unsolved); idetg3 = idxi3 */
+            const double *g1 = o->detg1 + 2;
+            double id2 = 1.0 / o->x[0][i + 2] * idxi2[j];
+            U[c] = faco * UO[c] + facn * U[c] +
+                   fact * dt *
+                       (o->idetg1[i + 2] * (g1[i - 1] * F1[IX(o, i - 1, j, k)] - g1[i] * F1[c]) +
+                        id2 * (1.0 * F2[IX(o, i, j - 1, k)] - 1.0 * F2[c]) +
+                        idxi3[k] * (F3[IX(o, i, j, k - 1)] - F3[c]) + S[c]);
+            continue;
+          }
           if (o->crdnt == 2) {
             /* idetg1, idetg2 = sx1/(cos(theta_-)-cos(theta_+)), idetg3 (metric.f90:105-130) */
             const double *g1 = o->detg1 + 2, *si = o->sini + 2, *ci = o->cosi + 2, *s1 = o->sx1 + 2;
@@ -1105,6 +1189,17 @@ int hmo_timestep(Oracle *o) {
         double sa1m = dxi2[j] * dxi3[k], sa1p = dxi2[j] * dxi3[k];
         double sa2m = dxi1[i] * dxi3[k], sa2p = dxi1[i] * dxi3[k];
         double sa3m = dxi1[i] * dxi2[j], sa3p = dxi1[i] * dxi2[j];
+        if (o->crdnt == 1) { /* metric.f90:80-96, one phi cell: dvol, sa1, sa3 times four */
+          const double *xi = o->xi[0] + 2;
+          const double a = xi[i], b = xi[i - 1], f4 = o->fac_j;
+          dvol = 0.5 * (a * a - b * b) * dxi2[j] * dxi3[k] * f4;
+          sa1m = b * dxi2[j] * dxi3[k] * f4;
+          sa1p = a * dxi2[j] * dxi3[k] * f4;
+          sa2m = dxi1[i] * dxi3[k];
+          sa2p = sa2m;
+          sa3p = 0.5 * (a * a - b * b) * dxi2[j] * f4;
+          sa3m = sa3p;
+        }
         if (o->crdnt == 2) { /* metric.f90:117-130 */
           const double *xi = o->xi[0] + 2, *si = o->sini + 2, *ci = o->cosi + 2;
           const double fj = o->fac_j, fk = o->fac_k;

@@ -54,6 +54,8 @@ def lib():
         L.hmo_make_geometric_axis.restype = _I
         L.hmo_make_spherical.argtypes = [_P, _I, _D, _D, _D, _I]
         L.hmo_make_spherical.restype = _I
+        L.hmo_make_cylindrical.argtypes = [_P, _I, _D, _D, _D, _I, _D, _D, _D]
+        L.hmo_make_cylindrical.restype = _I
         L.hmo_get_metric.argtypes = [_P, _I, _DP]
         L.hmo_get_metric.restype = _I
         L.hmo_get_axis.argtypes = [_P, _I] + [_DP] * 6
@@ -120,8 +122,14 @@ class Oracle:
             if L.hmo_make_spherical(self.h, imesh, float(lo), float(hi), float(cfg.get("x1min", 0.0)),
                                     int(bool(cfg.get("eq_sym", False)))) != 0:
                 raise ValueError("spherical grid: bad settings")
+        if int(cfg.get("crdnt", 0)) == 1:
+            (r0, r1), (z0, z1) = cfg["extent"][0], cfg["extent"][2]
+            if L.hmo_make_cylindrical(self.h, int(cfg.get("imesh", 0)) if n[0] > 1 else 0, float(r0), float(r1),
+                                      float(cfg.get("x1min", 0.0)), int(cfg.get("kmesh", 0)) if n[2] > 1 else 0,
+                                      float(z0), float(z1), float(cfg.get("x3min", 0.0))) != 0:
+                raise ValueError("cylindrical grid: bad settings")
         for a, (lo, hi) in enumerate(cfg["extent"]):
-            if int(cfg.get("crdnt", 0)) == 2:
+            if int(cfg.get("crdnt", 0)) in (1, 2):
                 break
             if cfg["n"][a] > 1 and int(cfg.get(mesh_keys[a], 0)) == 1:
                 xmin = float(cfg[("x1min", "x2min", "x3min")[a]])

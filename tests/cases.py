@@ -133,3 +133,30 @@ def polytrope_spherical(n=(24, 12, 8), xi1s=0.0, xi1e=2.0, imesh=0):
     cfg = config.resolve("polytrope_sph", overrides=ov)
     prims, phi = ic.polytrope_n1_spherical(cfg, G.make_grid(cfg))
     return cfg, prims, phi
+
+
+def cylindrical(n=(32, 1, 24), mag=True, seed=9, xi1s=0.0, imesh=0, kmesh=0, limiter="modified_mc"):
+    """An axisymmetric cylindrical grid (crdnt=1: R, z with one phi cell)
+    holding a seeded over-pressured core with small random velocities and a
+    field along z plus a small toroidal part vanishing on the axis."""
+    rng = np.random.default_rng(seed)
+    ov = dict(ie=n[0], je=1, ke=n[2], crdnt=1, mag_on=mag, gamma=1.6666666666666667, xi1s=xi1s, xi1e=1.0,
+              xi3s=-0.5, xi3e=0.5, imesh=imesh, x1min=0.03, kmesh=kmesh, x3min=0.04, flux_limiter=limiter,
+              t_end=1.0, dt_out=1.0, courant=0.8, bc1is=1, bc1iv=1, bc1os=2, bc1ov=2,
+              bc3is=0, bc3iv=0, bc3os=0, bc3ov=0)
+    cfg = config.resolve("cylindrical", overrides=ov)
+    grid = G.make_grid(cfg)
+    r = G.centres(grid, 0)[None, None, :]
+    z = G.centres(grid, 2)[:, None, None]
+    shape = (n[2], 1, n[0])
+    prims = {k: np.zeros(shape) for k in ("d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi")}
+    prims["d"][:] = 1.0 + 0.2 * rng.random(shape)
+    prims["p"][:] = np.where(r * r + z * z < 0.09, 2.0, 0.5) * (1.0 + 0.1 * rng.random(shape))
+    prims["v1"][:] = 0.1 * rng.uniform(-1.0, 1.0, shape)
+    prims["v2"][:] = 0.1 * r * rng.uniform(-1.0, 1.0, shape)
+    prims["v3"][:] = 0.1 * rng.uniform(-1.0, 1.0, shape)
+    if mag:
+        prims["b1"][:] = 0.02 * rng.uniform(-1.0, 1.0, shape)
+        prims["b2"][:] = 0.05 * r * rng.uniform(-1.0, 1.0, shape)
+        prims["b3"][:] = 0.2 + 0.02 * rng.uniform(-1.0, 1.0, shape)
+    return cfg, prims

@@ -133,3 +133,29 @@ def test_spherical_grid_matches_the_oracle_restatement(n, imesh, xi1s, grav):
     dv = G.spherical_dvol(grid, cfg["n"])
     full = 4.0 / 3.0 * np.pi * (1.0 - xi1s ** 3)
     assert abs(dv.sum() / full - 1.0) < 1e-12  # the cells tile the spherical shell
+
+
+@pytest.mark.parametrize("n,imesh,kmesh,xi1s", [((40, 1, 32), 0, 0, 0.0), ((30, 1, 1), 1, 0, 0.0),
+                                               ((24, 1, 20), 1, 1, 0.1)])
+def test_cylindrical_grid_matches_the_oracle_restatement(n, imesh, kmesh, xi1s):
+    """crdnt=1 (gridset.f90:145-292, metric.f90:53-100): the host's axes,
+    volumetric R centres and metric factors equal the oracle's bit for bit;
+    a solved phi axis is refused."""
+    import numpy as np
+
+    from hormone_b200 import config, grid as G
+    from oracle.oracle import Oracle
+
+    cfg = config.resolve("cyl", overrides=dict(ie=n[0], je=n[1], ke=n[2], crdnt=1, xi1s=xi1s, xi1e=1.0, xi3s=-0.5,
+                                                xi3e=0.5, imesh=imesh, x1min=0.03, kmesh=kmesh, x3min=0.04))
+    grid = G.make_grid(cfg)
+    o = Oracle(cfg)
+    for a in range(3):
+        ax = o.axis(a)
+        for k in G.AXIS_KEYS:
+            assert np.array_equal(ax[k], grid[a][k]), (a, k)
+    m = o.metric()
+    for name, key in (("detg1", "detg"), ("idetg1", "idetg"), ("sx1", "sx")):
+        assert np.array_equal(m[name], grid[0][key]), name
+    with pytest.raises(ValueError):
+        config.resolve("cyl", overrides=dict(ie=8, je=8, ke=8, crdnt=1))

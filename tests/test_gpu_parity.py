@@ -219,3 +219,16 @@ def test_spherical_self_gravity(n, xi1s):
     against the oracle with the potential compared at the end."""
     cfg, prims, phi = cases.polytrope_spherical(n, xi1s=xi1s)
     run_pair(cfg, prims, 8, grvphi=phi)
+
+
+@pytest.mark.parametrize("make", [lambda: cases.cylindrical((32, 1, 24), mag=True),
+                                  lambda: cases.cylindrical((40, 1, 1), mag=True),
+                                  lambda: cases.cylindrical((24, 1, 20), mag=False, xi1s=0.1, imesh=1, kmesh=1),
+                                  lambda: cases.cylindrical((30, 1, 16), mag=True, xi1s=0.2, limiter="minmod")],
+                         ids=["r-z-mhd", "radial-mhd", "r-z-stretched-shell", "r-z-minmod"])
+def test_cylindrical_coordinates(make):
+    """crdnt=1 with one phi cell: the xi1-weighted radial divergence
+    (rungekutta.f90:42-53 with metric.f90:53-100), the cylindrical source
+    terms (source.f90:88-111) and CFL, bitwise vs the oracle."""
+    cfg, prims = make()
+    run_pair(cfg, prims, 12)
