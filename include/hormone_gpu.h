@@ -286,7 +286,9 @@ int hmn_batch_destroy(hmn_batch* b);
  * `stream` (a cudaStream_t, NULL for the default stream); nothing is
  * synchronised.  The scratch is a static device array of 114,784 bytes
  * per GPU that loads the library: at most 4096 cells per axis (larger
- * grids return HMN_EINVAL), gravswitch must be 0.  The first call on a
+ * grids return HMN_EINVAL), gravswitch must be 0, and the grid is taken
+ * as Cartesian (a curvilinear grid's timestep goes through hmn_timestep,
+ * which has its metric).  The first call on a
  * device looks up the array's device address; make it before any stream
  * capture.  Calls that overlap on the GPU share the array and race: the
  * caller must order them. */

@@ -40,3 +40,34 @@ def test_bad_configuration_is_rejected():
     with pytest.raises(capi.HmnError) as ei:
         capi.Context(bad, G.make_grid(cfg))
     assert ei.value.code == capi.HMN_EBADCFG
+
+
+def test_curvilinear_metric_outside_the_path_is_rejected():
+    """hmn_set_metric returns HMN_EBADCFG for a cylindrical grid with a
+    solved phi axis, for passive scalars on a spherical grid and for an
+    unknown coordinate system; the host-side configuration refuses the
+    same set-ups before any device call."""
+    from hormone_b200 import config
+
+    cfg, prims = cases.spherical((12, 8, 4), mag=False, xi1s=0.2)
+    grid = G.make_grid(cfg)
+    ctx = capi.Context(cfg, grid)  # spherical: accepted
+    m = capi.HmnMetric()
+    for code in (3, -1):
+        assert capi.lib().hmn_set_metric(ctx.h, code, capi.ctypes.byref(m)) == capi.HMN_EBADCFG
+    ctx.close()
+    # a 3-D Cartesian context asked to become cylindrical (phi solved)
+    cfg3, _ = cases.ot3d(8)
+    ctx3 = capi.Context(cfg3, G.make_grid(cfg3))
+    keep = [np.ones(12) for _ in range(3)]
+    m.detg1, m.idetg1, m.sx1 = (capi._dp(a) for a in keep)
+    assert capi.lib().hmn_set_metric(ctx3.h, 1, capi.ctypes.byref(m)) == capi.HMN_EBADCFG
+    ctx3.close()
+    with pytest.raises(ValueError):
+        config.resolve("cyl", overrides=dict(ie=8, je=8, ke=8, crdnt=1))
+    with pytest.raises(ValueError):
+        config.resolve("sph", overrides=dict(ie=8, je=8, ke=8, crdnt=2, compswitch=2, spn=2))
+    with pytest.raises(ValueError):
+        config.resolve("sph", overrides=dict(ie=8, je=8, ke=8, crdnt=2, gravswitch=3, gbtype=0))
+    with pytest.raises(ValueError):
+        config.resolve("sph", overrides=dict(ie=8, je=1, ke=1, crdnt=2, gravswitch=3, gbtype=1))
