@@ -89,6 +89,7 @@ def lib():
         L.hmn_upload_scalars.argtypes = [_P, _DP]
         L.hmn_set_dirichlet.argtypes = [_P, _I, _I, _DP]
         L.hmn_set_metric.argtypes = [_P, _I, ctypes.POINTER(HmnMetric)]
+        L.hmn_set_flux_boundary.argtypes = [_P, _I, _I, _DP]
         L.hmn_download_scalars.argtypes = [_P, _DP]
         L.hmn_checkpoint_wait.argtypes = [_P]
         L.hmn_stream.argtypes = [_P]
@@ -98,7 +99,8 @@ def lib():
         for name in ("hmn_create", "hmn_upload", "hmn_timestep", "hmn_gravity_step", "hmn_hydro_step", "hmn_phidamp",
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
                      "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait",
-                     "hmn_upload_scalars", "hmn_download_scalars", "hmn_set_dirichlet", "hmn_set_metric"):
+                     "hmn_upload_scalars", "hmn_download_scalars", "hmn_set_dirichlet", "hmn_set_metric",
+                     "hmn_set_flux_boundary"):
             getattr(L, name).restype = _I
         _lib = L
     return _lib
@@ -274,6 +276,13 @@ class Context:
         if out is not None and spc is not None:
             out["spc"] = np.ascontiguousarray(np.moveaxis(spc, -1, 0))
         return out
+
+    def set_flux_boundary(self, flux):
+        """Boundary code 10 at the inner x3 face: its flux, 9 conserved slots
+        then the scalars (fluxboundary.f90:42-87)."""
+        a = np.ascontiguousarray(flux, dtype=np.float64)
+        self._flux_boundary = a
+        self._check(lib().hmn_set_flux_boundary(self.h, 2, 0, _dp(a)), "hmn_set_flux_boundary")
 
     def set_dirichlet(self, axis: int, side: int, vals: np.ndarray):
         """Ghost values of a code-9 face: (8 + nspc, 2, n_slow, n_fast) for the

@@ -237,9 +237,12 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
         bc[2] = 3
     for a in range(3):
         if solve[a]:
-            for code in bc[a].reshape(-1):
-                if code not in (0, 1, 2, 3, 4, 5, 9):
-                    raise ValueError(f"boundary code {code} on axis {a + 1} is not supported on this path")
+            for io in range(2):
+                for code in bc[a, io]:
+                    if code == 10 and a == 2 and io == 0 and bc[2, 0, 0] == bc[2, 0, 1] == 10:
+                        continue  # the flux boundary exists at the inner x3 face only (fluxboundary.f90:22-28)
+                    if code not in (0, 1, 2, 3, 4, 5, 9):
+                        raise ValueError(f"boundary code {code} on axis {a + 1} is not supported on this path")
     if float(cfg["courant"]) > 1.0:
         raise ValueError("courant number should be <= 1.0")
     unit = _UNITS[str(cfg["dt_unit"])]

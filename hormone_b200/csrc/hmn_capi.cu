@@ -52,6 +52,7 @@ struct hmn_ctx {
   int tma_ok;
   double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
   double* dir[3][2];         // Dirichlet ghost values per face (device)
+  double* fb;                // boundary code 10: the inner x3 face's flux (device, 9 + nspc)
   double* spcorg;            // passive scalars times density at RK stage 1
   double* xi1_h;             // host copies of the grid arrays the metric set-up needs
   double* axis_h;            // x, dx, dxi, idx of the three axes, (n+4) each
@@ -254,11 +255,15 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   for (int a = 0; a < 3; a++) {
     if (!ctx->solve[a]) continue;
     for (int io = 0; io < 2; io++)
-      for (int sv = 0; sv < 2; sv++)
-        if (!((ctx->bc[a][io][sv] >= 0 && ctx->bc[a][io][sv] <= 5) || ctx->bc[a][io][sv] == 9)) {
+      for (int sv = 0; sv < 2; sv++) {
+        const int code = ctx->bc[a][io][sv];
+        // code 10 exists only at the inner x3 face, for scalars and vectors alike (fluxboundary.f90:22-28)
+        const bool flux10 = code == 10 && a == 2 && io == 0 && ctx->bc[2][0][0] == 10 && ctx->bc[2][0][1] == 10;
+        if (!((code >= 0 && code <= 5) || code == 9 || flux10)) {
           delete ctx;
           return HMN_EBADCFG;
         }
+      }
     if (ctx->n[a] < 2) {
       delete ctx;
       return HMN_EBADCFG;
@@ -446,6 +451,7 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   cudaFree(ctx->spcorg);
   for (int a = 0; a < 3; a++)
     for (int io = 0; io < 2; io++) cudaFree(ctx->dir[a][io]);
+  cudaFree(ctx->fb);
   for (int b = 0; b < 2; b++) {
     cudaFree(ctx->gphi[b]);
     cudaFree(ctx->gpsi[b]);
@@ -783,8 +789,9 @@ static int enqueue_stage(hmn_ctx* ctx, int s) {
   const int rk = ctx->par.rktype;
   for (int a = 0; a < 3; a++)
     for (int io = 0; io < 2; io++)
-      if (ctx->solve[a] && (ctx->bc[a][io][0] == 9 || ctx->bc[a][io][1] == 9) && !ctx->G.dir[a][io])
-        return HMN_EBADCFG;  // code 9 needs hmn_set_dirichlet first
+      if (ctx->solve[a] && (ctx->bc[a][io][0] >= 9 || ctx->bc[a][io][1] >= 9) && !ctx->G.dir[a][io])
+        return HMN_EBADCFG;  // codes 9 and 10 need hmn_set_dirichlet first
+  if (ctx->solve[2] && ctx->bc[2][0][0] == 10 && !ctx->fb) return HMN_EBADCFG;  // and hmn_set_flux_boundary
   double* A = ctx->buf[0];
   double* B = ctx->buf[1];
   double* C = ctx->buf[2];
@@ -872,6 +879,21 @@ extern "C" int hmn_set_dirichlet(hmn_ctx* ctx, int axis, int side, const double*
   return HMN_OK;
 }
 
+// boundary code 10 (fluxboundary.f90:42-87): the flux through the inner x3
+// face, 9 conserved slots and then the scalars; the reference sets it for
+// the wind-tunnel inflow
+extern "C" int hmn_set_flux_boundary(hmn_ctx* ctx, int axis, int side, const double* flux) {
+  if (!ctx || !flux) return HMN_EINVAL;
+  if (axis != 2 || side != 0 || ctx->bc[2][0][0] != 10) return HMN_EBADCFG;
+  const size_t m = (size_t)(9 + ctx->par.nspc);
+  if (!ctx->fb) CK(cudaMalloc((void**)&ctx->fb, (9 + 4) * sizeof(double)), "flux boundary");
+  CK(cudaMemcpyAsync(ctx->fb, flux, m * sizeof(double), cudaMemcpyHostToDevice, ctx->st), "flux boundary");
+  CK(cudaStreamSynchronize(ctx->st), "sync");
+  drop_run_graph(ctx);
+  ctx->G.fb = ctx->G.zhalo[0] ? nullptr : ctx->fb;  // a slab above the first has no such face
+  return HMN_OK;
+}
+
 // ---------------------------------------------------------------------------
 // slab decomposition along z (mpi_domain.F90's role for this path)
 
@@ -890,6 +912,7 @@ extern "C" int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, cons
   drop_run_graph(ctx);
   ctx->G.zhalo[0] = recv_lo;
   ctx->G.zhalo[1] = recv_hi;
+  ctx->G.fb = recv_lo ? nullptr : ctx->fb;  // code 10 lives on the grid's inner z face only
   ctx->G.zwrap[0] = recv_lo && wrap_lo ? 1 : 0;
   ctx->G.zwrap[1] = recv_hi && wrap_hi ? 1 : 0;
   return HMN_OK;

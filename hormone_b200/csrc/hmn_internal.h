@@ -75,6 +75,9 @@ struct GridDev {
   // (layer l at coordinate -2+l inner, n+l outer; the other two axes in
   // increasing order, the lower one fastest)
   const double* dir[3][2];
+  // boundary code 10 at the inner z face: the flux through that face
+  // (9 conserved slots, then the scalars), or nullptr
+  const double* fb;
   SphGeo sph;
 };
 

@@ -207,6 +207,15 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
       sm.F[IMG1 + c2][w] = fl[7];
       if (GLM) sm.F[I9WV][w] = fl[8];
     }
+    // boundary code 10: the inner z face carries the host's flux
+    // (numflux.f90:566 -> fluxboundary.f90:42-87)
+    if (AX == 2 && G.fb != nullptr && t0[2] + f == 0) {
+#pragma unroll
+      for (int q = 0; q < 9; q++) sm.F[q][w] = G.fb[q];
+      if constexpr (TL::SP > 0)
+        for (int n = 0; n < A.nspc; n++) sm.F[9 + n][w] = G.fb[9 + n];
+      continue;
+    }
     // passive scalars: face fractions upwinded by the mass flux and
     // renormalised to sum 1 (numflux.f90:200-212)
     if constexpr (TL::SP > 0) {

@@ -204,6 +204,11 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
       hlld<float>(fl, cfl, cfr, (float)v1l, (float)v1r, (float)v2l, (float)v2r, (float)v3l, (float)v3r, dlf, drf,
                   (float)el, (float)er, ptl, ptr, b1lf, b1rf, b2lf, b2rf, b3lf, b3rf, (float)phil, (float)phir, ch);
     }
+    if (AX == 2 && G.fb != nullptr && t0[2] + f == 0) {  // boundary code 10 (fluxboundary.f90:42-87)
+#pragma unroll
+      for (int q = 0; q < 9; q++) sm.F[q][w] = (float)G.fb[q];
+      continue;
+    }
     sm.F[ICNT][w] = fl[0];
     sm.F[IMO1 + cn][w] = fl[1];
     sm.F[IMO1 + c1][w] = fl[2];

@@ -182,7 +182,8 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
       g1 = g0 - (f0 - g0) * dxa[-1] / dxa[0];
     }
   };
-  // Dirichlet values of this ghost (code 9): 8 + nspc planes x 2 layers x face cells
+  // Dirichlet values of this ghost (code 9; code 10 keeps the host's ghosts the
+  // same way): 8 + nspc planes x 2 layers x face cells
   const double* D = G.dir[ax][io];
   const int oa0 = ax == 0 ? 1 : 0, oa1 = ax == 2 ? 1 : 2;
   const size_t area = (size_t)G.n[oa0] * G.n[oa1];
@@ -197,7 +198,7 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
     if (g1 <= 0.0) g0 = g1 = A.gm1 * P[PEINT * pl + cs];
     pg = far ? g1 : g0;
     phig = GLM ? P[PPHI * pl + cs] * A.phifac : 0.0;
-  } else if (bs == 9) {
+  } else if (bs == 9 || bs == 10) {
     dg = D[hd];
     pg = D[2 * area + hd];
     phig = 0.0;
@@ -222,7 +223,7 @@ __device__ __forceinline__ void stage_cell(const GridDev& G, const StageArgs& A,
       const double vedge = P[(PV + ax) * pl + cv];
       v[ax] = v[ax] * (io == 1 ? 0.5 + fsign(0.5, vedge) : 0.5 - fsign(0.5, vedge));
     }
-  } else if (bv == 9) {
+  } else if (bv == 9 || bv == 10) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       v[c] = D[(size_t)(2 + c) * 2 * area + hd];
@@ -283,7 +284,7 @@ __device__ __forceinline__ size_t scalar_image(const GridDev& G, int i, int j, i
   return cidx(G, c3[0], c3[1], c3[2]);
 }
 
-// The Dirichlet values of a ghost cell's face (scalar code 9), or nullptr;
+// The Dirichlet values of a ghost cell's face (scalar code 9 or 10), or nullptr;
 // with the cell's index in that face's 2 x n1 x n2 layout and the face area.
 __device__ __forceinline__ int out_axis(const GridDev& G, int i, int j, int k) {
   return (i < 0 || i >= G.n[0]) ? 0 : ((j < 0 || j >= G.n[1]) ? 1 : ((k < 0 || k >= G.n[2]) ? 2 : -1));
@@ -293,7 +294,7 @@ __device__ __forceinline__ const double* dirichlet_face(const GridDev& G, int i,
   if (ax < 0) return nullptr;
   const int c3[3] = {i, j, k};
   const int io = c3[ax] < 0 ? 0 : 1;
-  return G.bc[ax][io][0] == 9 ? G.dir[ax][io] : nullptr;
+  return G.bc[ax][io][0] >= 9 ? G.dir[ax][io] : nullptr;
 }
 __device__ __forceinline__ size_t dirichlet_area(const GridDev& G, int i, int j, int k) {
   const int ax = out_axis(G, i, j, k);

@@ -43,7 +43,8 @@ typedef struct {
   int n[3];           /* ie-is+1, je-js+1, ke-ks+1 */
   int ghost;          /* ghost layers of the caller's 3-D arrays (0 or 2) */
   int bc[3][2][2];    /* boundary codes [axis][inner,outer][scalar,vector], after checksetup.f90:109-128:
-                       0 periodic, 1 reflective, 2 outgoing, 3 free, 4/5 linear, 9 Dirichlet */
+                       0 periodic, 1 reflective, 2 outgoing, 3 free, 4/5 linear, 9 Dirichlet,
+                       10 flux (inner x3 face only) */
   const double* x[3];
   const double* xi[3];
   const double* dx[3];
@@ -140,6 +141,15 @@ int hmn_download(hmn_ctx* ctx, double* u, double* const prim[9], double* grvphi,
  * outflow-only normal velocity) need no data; code 10 (the wind-tunnel flux
  * boundary, fluxboundary.f90) is not on this path. */
 int hmn_set_dirichlet(hmn_ctx* ctx, int axis, int side, const double* vals);
+
+/* Boundary code 10 (src/main/fluxboundary.f90:42-87, the wind-tunnel
+ * inflow): the flux through the inner x3 face, replacing the Riemann flux
+ * there after numflux (numflux.f90:566).  flux holds the 9 conserved slots
+ * (d, m1, m2, m3, E, B1, B2, B3, phi) and then nspc scalar fluxes.  Only
+ * axis 2, side 0, with bc3is = bc3iv = 10; the ghost layers beyond that
+ * face, which the reference never rewrites, are set with hmn_set_dirichlet
+ * as for code 9.  Both are needed before the first step. */
+int hmn_set_flux_boundary(hmn_ctx* ctx, int axis, int side, const double* flux);
 
 /* Passive scalars (compswitch 2: module physval's spc(1:spn,i,j,k), species
  * fastest, then i, j, k with the grid's ghost layers): upload the mass

@@ -31,7 +31,9 @@
  *   RK + primitive  src/main/rungekutta.f90:16-232
  *   boundaries      src/main/boundarycondition.f90:14-1442 (codes 0-3; 4/5
  *                   linear extrapolation as :302-327,419-468; 9 Dirichlet
- *                   as :104-115,196-212 from per-face ghost values)
+ *                   as :104-115,196-212 from per-face ghost values; 10 at
+ *                   the inner x3 face: ghosts never rewritten, the face
+ *                   flux from fluxboundary.f90:42-87)
  *   timestep        src/main/timestep.f90:15-183
  *   phidamp         src/main/source.f90:239-260
  *   hyperbolic grav src/main/gravity_hyperbolic.f90:19-125,230-280 with a
@@ -87,6 +89,9 @@ typedef struct {
   /* Dirichlet ghost values per face: 8 + spn planes (d, p, v1..3, b1..3,
      spc) x 2 layers x face cells, layer l at coordinate -2+l (inner) or n+l */
   double *dir[3][2];
+  /* boundary code 10 at the inner x3 face: the flux through that face,
+     9 + spn values in conserved order (fluxboundary.f90:42-87) */
+  double *fbflux;
   /* coordinate system: 0 Cartesian, 2 spherical polar (r, theta, phi) with
      the metric factors of metric.f90:102-151 (offset +2 like the axes) */
   int crdnt;
@@ -175,6 +180,7 @@ void hmo_destroy(Oracle *o) {
   }
   free(o->grvphi); free(o->grvpsi); free(o->gorg1); free(o->gorg2); free(o->lapphi); free(o->hgsrc); free(o->gsrc);
   for (int a = 0; a < 3; a++) { free(o->dir[a][0]); free(o->dir[a][1]); }
+  free(o->fbflux);
   free(o->detg1); free(o->idetg1); free(o->sx1); free(o->sini); free(o->cosi); free(o->scot);
   free(o->sinc); free(o->sisin);
   for (int n = 0; n < o->spn; n++) {
@@ -202,6 +208,13 @@ int hmo_set_dirichlet(Oracle *o, int a, int io, const double *vals) {
   size_t m = (size_t)(8 + o->spn) * 2 * o->n[oa[0]] * o->n[oa[1]];
   if (!o->dir[a][io]) o->dir[a][io] = zalloc(m);
   memcpy(o->dir[a][io], vals, m * sizeof(double));
+  return HMO_OK;
+}
+
+/* boundary code 10 (fluxboundary3i): the face flux of the inner x3 face */
+int hmo_set_flux_boundary(Oracle *o, const double *flux) {
+  if (!o->fbflux) o->fbflux = zalloc(9 + MAXSPC);
+  memcpy(o->fbflux, flux, (size_t)(9 + o->spn) * sizeof(double));
   return HMO_OK;
 }
 
@@ -631,6 +644,8 @@ static void bc_axis(Oracle *o, int a) {
             case 2: case 3: ss = edge; break;
             case 4: case 5: break;
             case 9:
+            case 10: /* code 10 never writes its ghosts (boundarycondition.f90:999,1139): they keep the
+                        values the host set, given here as for code 9 */
               if (!D) { set_err(o, HMO_EBADCFG, a, io, 0); return; }
               o->d[cg] = D[0 * 2 * area + h]; o->p[cg] = D[1 * 2 * area + h];
               if (o->mag_on) o->phi[cg] = 0.0;
@@ -651,6 +666,7 @@ static void bc_axis(Oracle *o, int a) {
             case 2: case 3: sv = edge; break;
             case 4: case 5: break;
             case 9:
+            case 10:
               if (!D) { set_err(o, HMO_EBADCFG, a, io, 1); return; }
               for (int c = 0; c < 3; c++) {
                 o->v[c][cg] = D[(size_t)(2 + c) * 2 * area + h];
@@ -846,6 +862,19 @@ static void hlldflux(double f[9], double cfl, double cfr, double v1l, double v1r
 }
 
 /* numflux.f90:46-563 */
+/* fluxboundary3i (fluxboundary.f90:42-87, called at numflux.f90:566): the
+   flux through the inner x3 face replaced by the host-given wind flux */
+static void fluxboundary(Oracle *o) {
+  if (o->bc[2][0][0] != 10 || !o->solve[2]) return;
+  if (!o->fbflux) { set_err(o, HMO_EBADCFG, 2, 0, 10); return; }
+  for (int j = 0; j < o->n[1]; j++)
+    for (int i = 0; i < o->n[0]; i++) {
+      size_t f = IX(o, i, j, -1);
+      for (int q = 0; q < 9; q++) o->flux[2][q][f] = o->fbflux[q];
+      for (int ns = 0; ns < o->spn; ns++) o->spcflx[2][ns][f] = o->fbflux[9 + ns];
+    }
+}
+
 static void numflux(Oracle *o) {
   interpolation(o);
   double gam = o->gamma, gm1 = o->gamma - 1.0;
@@ -954,6 +983,7 @@ static void numflux(Oracle *o) {
         }
     if (bad) set_err(o, HMO_ENEG_EINT, bi, bj, bk);
   }
+  fluxboundary(o);
 }
 
 /* ------------------------------------------------------------------------ */

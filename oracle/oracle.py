@@ -66,6 +66,8 @@ def lib():
         L.hmo_set_spc.argtypes = [_P, _I, _DP]
         L.hmo_set_dirichlet.argtypes = [_P, _I, _I, _DP]
         L.hmo_set_dirichlet.restype = _I
+        L.hmo_set_flux_boundary.argtypes = [_P, _DP]
+        L.hmo_set_flux_boundary.restype = _I
         L.hmo_gravity_setup.argtypes = [_P, _D]
         L.hmo_start.argtypes = [_P]
         L.hmo_start.restype = _I
@@ -185,6 +187,12 @@ class Oracle:
         self._keep_dir = getattr(self, "_keep_dir", {})
         self._keep_dir[(axis, side)] = a
         lib().hmo_set_dirichlet(self.h, int(axis), int(side), _dp(a.reshape(-1)))
+
+    def set_flux_boundary(self, flux):
+        """Boundary code 10: the inner x3 face's flux (9 + nspc values)."""
+        a = np.ascontiguousarray(flux, dtype=np.float64)
+        self._keep_fb = a
+        lib().hmo_set_flux_boundary(self.h, _dp(a))
 
     def set_gravity_state(self, grvphi, grvpsi=None, cgrav_old=0.0):
         a = np.ascontiguousarray(grvphi, dtype=np.float64).reshape(-1)

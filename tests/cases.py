@@ -160,3 +160,52 @@ def cylindrical(n=(32, 1, 24), mag=True, seed=9, xi1s=0.0, imesh=0, kmesh=0, lim
         prims["b2"][:] = 0.05 * r * rng.uniform(-1.0, 1.0, shape)
         prims["b3"][:] = 0.2 + 0.02 * rng.uniform(-1.0, 1.0, shape)
     return cfg, prims
+
+
+def wind_tunnel(n=(16, 12, 20), mag=False, nspc=0, seed=13):
+    """A box fed through its inner x3 face by boundary code 10: a uniform
+    wind (d, p, v3) enters with the flux of fluxboundary.f90:42-87, the
+    ghosts below that face hold the wind state, the other faces are
+    outgoing; a dense seeded clump sits in the flow.  Returns (cfg, prims,
+    flux vector, Dirichlet ghost planes of the inner x3 face)."""
+    rng = np.random.default_rng(seed)
+    ov = dict(ie=n[0], je=n[1], ke=n[2], mag_on=mag, gamma=1.6666666666666667, t_end=1.0, dt_out=1.0, courant=0.8,
+              xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5, xi3s=-0.5, xi3e=0.5)
+    for a in (1, 2, 3):
+        for tag in ("is", "os", "iv", "ov"):
+            ov[f"bc{a}{tag}"] = 2
+    ov.update(bc3is=10, bc3iv=10)
+    if nspc:
+        ov.update(compswitch=2, spn=nspc)
+    cfg = config.resolve("windtunnel", overrides=ov)
+    grid = G.make_grid(cfg)
+    x, y, z = (G.centres(grid, a) for a in range(3))
+    r2 = x[None, None, :] ** 2 + y[None, :, None] ** 2 + z[:, None, None] ** 2
+    shape = (n[2], n[1], n[0])
+    dw, pw, vw = 1.0, 0.6, 0.8
+    prims = {k: np.zeros(shape) for k in ("d", "p", "v1", "v2", "v3", "b1", "b2", "b3", "phi")}
+    prims["d"][:] = np.where(r2 < 0.04, 10.0, dw) * (1.0 + 0.05 * rng.random(shape))
+    prims["p"][:] = pw
+    prims["v3"][:] = np.where(r2 < 0.04, 0.0, vw)
+    if mag:
+        prims["b1"][:] = 0.1
+        prims["b3"][:] = 0.2
+    gm1 = cfg["gamma"] - 1.0
+    ew = pw / gm1 + 0.5 * dw * vw * vw
+    flux = np.zeros(9 + nspc)
+    flux[0] = dw * vw
+    flux[3] = dw * vw * vw + pw
+    flux[4] = (ew + pw) * vw
+    if mag:  # the field is carried in by the wind (B x v along z)
+        flux[4] = flux[4] + (0.1 * 0.1) * vw
+        flux[5] = -0.1 * vw
+    area = n[0] * n[1]
+    ghosts = np.zeros((8 + nspc, 2, area))
+    ghosts[0], ghosts[1], ghosts[4] = dw, pw, vw
+    if mag:
+        ghosts[5], ghosts[7] = 0.1, 0.2
+    if nspc:
+        prims = add_scalars(cfg, prims)
+        flux[9 + nspc - 1] = flux[0]  # the wind is the last species (fluxboundary.f90:80-81)
+        ghosts[8 + nspc - 1] = 1.0
+    return cfg, prims, flux, ghosts

@@ -33,10 +33,12 @@ def compare(o, s, where):
         assert np.array_equal(st["spc"][n], o.get(f"spc{n}")), f"{where}: scalar {n} differs"
 
 
-def run_pair(cfg, prims, nsteps, grvphi=None, cgrav_old=0.0, check_every=1, dirichlet=None):
+def run_pair(cfg, prims, nsteps, grvphi=None, cgrav_old=0.0, check_every=1, dirichlet=None, fluxbound=None):
     o = Oracle(cfg)
     for (axis, side), vals in (dirichlet or {}).items():
         o.set_dirichlet(axis, side, vals)
+    if fluxbound is not None:
+        o.set_flux_boundary(fluxbound)
     o.set_prims(prims)
     if grvphi is not None:
         o.set_gravity_state(grvphi, None, cgrav_old)
@@ -44,6 +46,8 @@ def run_pair(cfg, prims, nsteps, grvphi=None, cgrav_old=0.0, check_every=1, diri
     s = Simulation(cfg, prims, grvphi=grvphi, cgrav_old=cgrav_old)
     for (axis, side), vals in (dirichlet or {}).items():
         s.ctx.set_dirichlet(axis, side, vals)
+    if fluxbound is not None:
+        s.ctx.set_flux_boundary(fluxbound)
     compare(o, s, "initial state")
     assert s.dt == o.scalars()["dt"] and s.ch == o.scalars()["ch"]
     for n in range(nsteps):
@@ -232,3 +236,12 @@ def test_cylindrical_coordinates(make):
     terms (source.f90:88-111) and CFL, bitwise vs the oracle."""
     cfg, prims = make()
     run_pair(cfg, prims, 12)
+
+
+@pytest.mark.parametrize("mag,nspc", [(False, 0), (True, 0), (False, 2)], ids=["hydro", "mhd", "two-species"])
+def test_flux_boundary_code_10(mag, nspc):
+    """Boundary code 10 at the inner x3 face: the host's wind flux replaces
+    the Riemann flux there (numflux.f90:566, fluxboundary.f90:42-87) and the
+    ghosts keep the host's values, bitwise vs the oracle."""
+    cfg, prims, flux, ghosts = cases.wind_tunnel(mag=mag, nspc=nspc)
+    run_pair(cfg, prims, 12, dirichlet={(2, 0): ghosts.reshape(-1)}, fluxbound=flux)
