@@ -44,7 +44,8 @@ def one_step_l1(cfg, prims, warm=3):
 @pytest.mark.parametrize("make", [lambda: cases.ot3d(32), lambda: cases.kh2d(64), lambda: cases.blast3d(16, bc=2),
                                   lambda: cases.golden_case("briowushock_x"),
                                   lambda: cases.spherical((16, 12, 8), mag=True, xi1s=0.2),
-                                  lambda: cases.golden_case("sedov_default")])
+                                  lambda: cases.golden_case("sedov_default"),
+                                  lambda: cases.cylindrical((32, 1, 24), mag=True)])
 def test_mixed_one_step_error(make):
     cfg, prims = make()
     l1 = one_step_l1(cfg, prims)

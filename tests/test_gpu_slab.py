@@ -47,6 +47,13 @@ def test_spherical_phi_wedges():
     run_both(cfg, prims, 2, 5)
 
 
+def test_cylindrical_z_slabs():
+    """An axisymmetric cylindrical grid (R, z) split along z into three
+    slabs, with periodic z."""
+    cfg, prims = cases.cylindrical((24, 1, 18), mag=True)
+    run_both(cfg, prims, 3, 5)
+
+
 def test_riemann_with_scalars():
     cfg, prims = cases.riemann3d(n=(12, 10, 8), bc=(3, 1, 0), nspc=2)
     run_both(cfg, prims, 2, 5)
