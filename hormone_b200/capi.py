@@ -1,7 +1,8 @@
 """ctypes binding of libhormone_b200.so (the C ABI of include/hormone_gpu.h).
 
 This is the Python side of the same boundary a Fortran ISO_C_BINDING shim
-binds.  There is no CPU fallback: if the library or a
+binds (the shim keeps the reference's timestep, gravity, hydro_step and
+phidamp names around these entry points).  There is no CPU fallback: if the library or a
 CUDA device is missing, creating a context raises.
 """
 from __future__ import annotations

@@ -124,7 +124,7 @@ def orszagtang3d(cfg, grid, seed: int = 20261203, amp: float = 1e-3) -> Dict[str
 
 
 def kelvin_helmholtz(cfg, grid, rho_ratio: float, bx: float, width: float = 0.05, ptb: float = 0.01):
-    """Periodic tanh shear layer (BASELINE's KH boxes; the reference's own
+    """Periodic tanh shear layer (the batched Kelvin-Helmholtz benchmark boxes; the reference's own
     KHtests.f90 uses an exponential profile and passive scalars instead):
     vx = 0.5*tanh((|y|-0.25)/width), rho = 1 outside and ``rho_ratio`` inside
     the layer, p = 2.5, vy = ptb*sin(4 pi x), Bx = ``bx``."""

@@ -4,8 +4,8 @@ Every case starts both implementations from the same initial primitives and
 compares dt and the full conserved and primitive state after every step.
 The FP64 kernels keep the reference's operation order with no fused
 multiply-adds, so the expected difference is exactly zero (-0 and +0 compare
-equal); the tolerance the north-star target states (1e-12 relative per step)
-is therefore met with margin.
+equal); a stated per-step tolerance of 1e-12 relative is therefore met
+with margin.
 """
 import numpy as np
 import pytest
