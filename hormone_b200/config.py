@@ -262,8 +262,8 @@ def checksetup(raw: Dict[str, Any]) -> Dict[str, Any]:
     # passive scalars are carried with compswitch 2 (compswitch 1 only changes
     # the mean molecular weight, which the ideal-gas step does not use)
     nspc = int(cfg.get("spn", 0)) if comp == 2 else 0
-    if nspc < 0 or nspc > 4:
-        raise ValueError("at most 4 passive scalars are on this path")
+    if nspc < 0 or nspc > 8:
+        raise ValueError("at most 8 passive scalars are on this path")
     if crdnt and nspc:
         raise ValueError("passive scalars on curvilinear grids are not on this path")
     grav = int(cfg.get("gravswitch", 0))

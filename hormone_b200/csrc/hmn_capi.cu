@@ -238,8 +238,8 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
   if (par->rktype < 1 || par->rktype > 3 || par->limiter < 0 || par->limiter > 2) return HMN_EBADCFG;
   if (par->gravswitch != 0 && par->gravswitch != 3) return HMN_EBADCFG;
   if (par->precision != 0 && par->precision != 1) return HMN_EBADCFG;
-  // passive scalars: at most 4, FP64 form only
-  if (par->nspc < 0 || par->nspc > 4 || (par->nspc > 0 && par->precision != 0)) return HMN_EBADCFG;
+  // passive scalars: at most 8, FP64 form only
+  if (par->nspc < 0 || par->nspc > 8 || (par->nspc > 0 && par->precision != 0)) return HMN_EBADCFG;
   hmn_ctx* ctx = new (std::nothrow) hmn_ctx();
   if (!ctx) return HMN_ENOMEM;
   memset(ctx, 0, sizeof(*ctx));
@@ -886,7 +886,7 @@ extern "C" int hmn_set_flux_boundary(hmn_ctx* ctx, int axis, int side, const dou
   if (!ctx || !flux) return HMN_EINVAL;
   if (axis != 2 || side != 0 || ctx->bc[2][0][0] != 10) return HMN_EBADCFG;
   const size_t m = (size_t)(9 + ctx->par.nspc);
-  if (!ctx->fb) CK(cudaMalloc((void**)&ctx->fb, (9 + 4) * sizeof(double)), "flux boundary");
+  if (!ctx->fb) CK(cudaMalloc((void**)&ctx->fb, (9 + 8) * sizeof(double)), "flux boundary");
   CK(cudaMemcpyAsync(ctx->fb, flux, m * sizeof(double), cudaMemcpyHostToDevice, ctx->st), "flux boundary");
   CK(cudaStreamSynchronize(ctx->st), "sync");
   drop_run_graph(ctx);

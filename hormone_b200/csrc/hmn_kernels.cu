@@ -716,26 +716,32 @@ void stage_tile(const int solve[3], int precision, int nspc, int tile[3]) {
   }
 }
 
+// The stage tiles whose shared-memory layout has room for SP passive
+// scalars (8 x 8 x 4 in 3-D; with 8 scalars its 203 KB allow one CTA per SM)
+template <int SP, int MINB3>
+static cudaError_t launch_scalar_tiles(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  const int* t = A.tile;
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4)
+    return launch_stage_tl<Tile<8, 8, 4, 384, MINB3, SP>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1)
+    return launch_stage_tl<Tile<16, 16, 1, 288, MINB3, SP>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16)
+    return launch_stage_tl<Tile<16, 1, 16, 288, MINB3, SP>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16)
+    return launch_stage_tl<Tile<1, 16, 16, 288, MINB3, SP>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1, 288, 2, SP>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1, 288, 2, SP>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256, 288, 2, SP>>(G, A, mag, glm, nullptr, st);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st) {
   if (G.sph.on) return launch_stage_spherical(G, A, mag, glm, st);
   const int* t = A.tile;
-  if (A.nspc > 0) {  // tiles with room for up to 4 passive scalars
-    using S3 = Tile<8, 8, 4, 384, 2, 4>;
-    if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<S3>(G, A, mag, glm, nullptr, st);
-    if (t[0] == 16 && t[1] == 16 && t[2] == 1)
-      return launch_stage_tl<Tile<16, 16, 1, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
-    if (t[0] == 16 && t[1] == 1 && t[2] == 16)
-      return launch_stage_tl<Tile<16, 1, 16, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
-    if (t[0] == 1 && t[1] == 16 && t[2] == 16)
-      return launch_stage_tl<Tile<1, 16, 16, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
-    if (t[0] == 256 && t[1] == 1 && t[2] == 1)
-      return launch_stage_tl<Tile<256, 1, 1, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
-    if (t[0] == 1 && t[1] == 256 && t[2] == 1)
-      return launch_stage_tl<Tile<1, 256, 1, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
-    if (t[0] == 1 && t[1] == 1 && t[2] == 256)
-      return launch_stage_tl<Tile<1, 1, 256, 288, 2, 4>>(G, A, mag, glm, nullptr, st);
-    return cudaErrorInvalidValue;
+  if (A.nspc > 0) {  // tiles with room for up to 4, or up to 8, passive scalars
+    if (A.nspc <= 4) return launch_scalar_tiles<4, 2>(G, A, mag, glm, st);
+    return launch_scalar_tiles<8, 1>(G, A, mag, glm, st);
   }
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
   if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, tm, st);

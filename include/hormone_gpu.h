@@ -65,7 +65,7 @@ typedef struct {
   int maxtngrv;
   int outstyle, endstyle;
   int precision;   /* 0 FP64 (bit-compatible), 1 FP32 flux / FP64 accumulation */
-  int nspc;        /* passive scalars: spn with compswitch 2, else 0 (at most 4; FP64 single grids) */
+  int nspc;        /* passive scalars: spn with compswitch 2, else 0 (at most 8; FP64 single grids) */
 } hmn_params;
 
 /* allocations.f90 + metric.f90 for this grid: allocates device state. */

@@ -62,7 +62,7 @@
 
 enum { ICNT = 0, IMO1 = 1, IMO2 = 2, IMO3 = 3, IENE = 4, IMG1 = 5, IMG2 = 6, IMG3 = 7, I9WV = 8 };
 enum { S_D = 0, S_E, S_M1, S_M2, S_M3, S_B1, S_B2, S_B3, NSLOPE };
-#define MAXSPC 4
+#define MAXSPC 8
 
 typedef struct {
   int n[3];           /* interior cells per axis */

@@ -30,14 +30,20 @@ def kh2d(n=32, ratio=2.0, bx=0.05, bc_y=0, limiter="modified_mc"):
 
 
 def add_scalars(cfg, prims, seed=11):
-    """Two passive scalars that sum to one: a smooth seeded field and its
-    complement (what compswitch 2 carries)."""
+    """Passive scalars that sum to one (what compswitch 2 carries): for two,
+    a smooth seeded field and its complement; for more, seeded positive
+    weights normalised per cell."""
     rng = np.random.default_rng(seed)
     shape = prims["d"].shape
-    base = 0.5 + 0.4 * np.sin(np.arange(shape[2]) * 0.37)[None, None, :] * np.cos(np.arange(shape[1]) * 0.21)[None, :, None]
-    x = np.clip(base + 0.05 * rng.uniform(-1, 1, size=shape), 0.0, 1.0)
+    n = int(cfg.get("nspc", 2)) or 2
     prims = dict(prims)
-    prims["spc"] = np.stack([x, 1.0 - x])
+    if n == 2:
+        base = 0.5 + 0.4 * np.sin(np.arange(shape[2]) * 0.37)[None, None, :] * np.cos(np.arange(shape[1]) * 0.21)[None, :, None]
+        x = np.clip(base + 0.05 * rng.uniform(-1, 1, size=shape), 0.0, 1.0)
+        prims["spc"] = np.stack([x, 1.0 - x])
+        return prims
+    w = rng.uniform(0.1, 1.0, size=(n,) + shape)
+    prims["spc"] = w / w.sum(axis=0)
     return prims
 
 

@@ -139,11 +139,15 @@ def test_tma_staged_region_fp64(monkeypatch, make):
 @pytest.mark.parametrize("make", [lambda: cases.golden_case("KHinstability"),
                                   lambda: cases.golden_case("KHinstability_flat"),
                                   lambda: cases.blast3d(14, bc=1, nspc=2),
-                                  lambda: cases.riemann3d(nspc=2)])
+                                  lambda: cases.riemann3d(nspc=2),
+                                  lambda: cases.blast3d(14, bc=1, nspc=6),
+                                  lambda: cases.riemann3d(nspc=8),
+                                  lambda: cases.riemann3d(n=(20, 18, 1), bc=(3, 0, 3), nspc=5)])
 def test_passive_scalars(make):
-    """Two passive scalars advected with the mass flux (numflux.f90:200-212,
-    rungekutta.f90:61-86): 2-D KH (the reference's own test), and 3-D with
-    reflective, free and periodic boundaries, MHD and hydro."""
+    """Passive scalars advected with the mass flux (numflux.f90:200-212,
+    rungekutta.f90:61-86): 2-D KH with two (the reference's own test), and
+    3-D and 2-D grids with 2 to 8 (the 8-scalar tiles) under reflective,
+    free and periodic boundaries, MHD and hydro."""
     cfg, prims = make()
     run_pair(cfg, prims, 6)
 
