@@ -220,7 +220,7 @@ extern "C" int hmn_batch_add(hmn_batch* b, const hmn_grid* grid, const hmn_param
       if (grid->n[a] < 2) return HMN_EBADCFG;
       for (int io = 0; io < 2; io++)
         for (int sv = 0; sv < 2; sv++)
-          if (grid->bc[a][io][sv] < 0 || grid->bc[a][io][sv] > 3) return HMN_EBADCFG;
+          if (grid->bc[a][io][sv] < 0 || grid->bc[a][io][sv] > 5) return HMN_EBADCFG;  // codes 0-5
     }
   }
   const int kind = batch_tile_kind(solve);

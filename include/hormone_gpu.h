@@ -245,7 +245,7 @@ int hmn_destroy(hmn_ctx* ctx);
  * them, each on its own clock (its own CFL dt, t_end, ch), with one
  * persistent launch per phase; each simulation's result is bit-identical
  * to running it alone through hmn_create/hmn_run.  Supported grids: 3-D,
- * 2-D in the x-y plane and 1-D along x, boundary codes 0-3, no gravity,
+ * 2-D in the x-y plane and 1-D along x, boundary codes 0-5, no gravity,
  * one rktype per batch. */
 typedef struct hmn_batch hmn_batch;
 

@@ -32,6 +32,10 @@ def mix():
     c, p = cases.blast3d(10, bc=3, mag=False)
     c = dict(c); c["t_end"] = 0.01
     sims.append((c, p))
+    for code in (4, 5):  # linear extrapolation, and with outflow only, on every face
+        c, p = cases.blast3d(9, bc=code, mag=True)
+        c = dict(c); c["t_end"] = 0.01
+        sims.append((c, p))
     return sims
 
 
