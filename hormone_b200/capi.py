@@ -358,6 +358,8 @@ def _bind_slab(L):
     L.hmn_slab_halo_bytes.argtypes = [_P]
     L.hmn_slab_halo_bytes.restype = ctypes.c_size_t
     L.hmn_set_slab.argtypes = [_P, _P, _P, _P, _P, _I, _I]
+    L.hmn_set_slab_push.argtypes = [_P, _P * 2, _P * 2, _P * 2, _P * 2, _I, _I]
+    L.hmn_set_slab_push.restype = _I
     L.hmn_pack_halos.argtypes = [_P]
     L.hmn_hydro_stage.argtypes = [_P, _I]
     L.hmn_cfl_local.argtypes = [_P, _D, _D, _D]
@@ -382,6 +384,15 @@ class SlabContext(Context):
         L = _bind_slab(lib())
         self._check(L.hmn_set_slab(self.h, send_lo or None, send_hi or None, recv_lo or None, recv_hi or None,
                                    int(bool(wrap_lo)), int(bool(wrap_hi))), "hmn_set_slab")
+
+    def set_slab_push(self, recv_lo, recv_hi, push_lo, push_hi, wrap_lo=False, wrap_hi=False):
+        """The push exchange: pairs (parity 0, 1) of device addresses (0 on
+        a physical face) of this slab's halo buffers and of the neighbours'
+        buffers its stages store into."""
+        L = _bind_slab(lib())
+        arr = lambda pair: (_P * 2)(*[v or None for v in pair])  # noqa: E731
+        self._check(L.hmn_set_slab_push(self.h, arr(recv_lo), arr(recv_hi), arr(push_lo), arr(push_hi),
+                                        int(bool(wrap_lo)), int(bool(wrap_hi))), "hmn_set_slab_push")
 
     def pack_halos(self):
         self._check(_bind_slab(lib()).hmn_pack_halos(self.h), "hmn_pack_halos")

@@ -51,6 +51,12 @@ struct hmn_ctx {
   TmaMaps tmaps[2];          // tensor maps of pbuf[0], pbuf[1] for TMA staging of 3-D tiles
   int tma_ok;
   double* zsend[2];          // slab decomposition: caller's send buffers (low, high z face)
+  // push exchange: this slab's halo buffers [low, high][parity] and the
+  // neighbours' buffers its stages store into [low neighbour, high][parity];
+  // zpar is the parity holding the halos of the current state
+  const double* zrecv[2][2];
+  double* zpush[2][2];
+  int zpush_on, zpar;
   double* dir[3][2];         // Dirichlet ghost values per face (device)
   double* fb;                // boundary code 10: the inner x3 face's flux (device, 9 + nspc)
   double* spcorg;            // passive scalars times density at RK stage 1
@@ -827,6 +833,12 @@ static int enqueue_stage(hmn_ctx* ctx, int s) {
       a.tiles[d] = ctx->tiles[d];
     }
     a.stage = s;
+    if (ctx->zpush_on) {  // read the halos of this parity, store into the other
+      ctx->G.zhalo[0] = ctx->zrecv[0][ctx->zpar];
+      ctx->G.zhalo[1] = ctx->zrecv[1][ctx->zpar];
+      a.push[0] = ctx->zpush[0][ctx->zpar ^ 1];
+      a.push[1] = ctx->zpush[1][ctx->zpar ^ 1];
+    }
     a.nspc = ctx->par.nspc;
     a.spcorg = ctx->spcorg;
     const TmaMaps* tm = ctx->tma_ok ? &ctx->tmaps[ctx->pcur] : nullptr;
@@ -836,6 +848,7 @@ static int enqueue_stage(hmn_ctx* ctx, int s) {
       CK(launch_stage(ctx->G, a, ctx->mag, ctx->glm, tm, ctx->st), "stage");
     ctx->launches += 1;
     ctx->pcur = 1 - ctx->pcur;
+    if (ctx->zpush_on) ctx->zpar ^= 1;
   }
   if (s == rk) {
     if (rk == 1) {
@@ -918,8 +931,52 @@ extern "C" int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, cons
   return HMN_OK;
 }
 
+// Push exchange between z slabs: each stage's kernel stores its two bottom
+// and two top layers into the neighbours' halo buffers as it writes them
+// (on several GPUs the buffers are the neighbours' memory: the exchange
+// rides inside the stage).  Buffers alternate by stage parity, so a stage
+// never overwrites halos a neighbour may still be reading; between stages
+// every slab must have finished the previous one (the caller's barrier).
+extern "C" int hmn_set_slab_push(hmn_ctx* ctx, const double* const recv_lo[2], const double* const recv_hi[2],
+                                 double* const push_lo[2], double* const push_hi[2], int wrap_lo, int wrap_hi) {
+  if (!ctx || !recv_lo || !recv_hi || !push_lo || !push_hi) return HMN_EINVAL;
+  if (!ctx->solve[0] || !ctx->solve[1] || !ctx->solve[2] || ctx->n[2] < 2 || ctx->par.gravswitch != 0 ||
+      ctx->G.sph.on)
+    return HMN_EBADCFG;  // 3-D Cartesian grids
+  for (int q = 0; q < 2; q++)
+    if ((recv_lo[q] == nullptr) != (push_lo[q] == nullptr) || (recv_hi[q] == nullptr) != (push_hi[q] == nullptr))
+      return HMN_EINVAL;
+  for (int q = 0; q < 2; q++) {
+    ctx->zrecv[0][q] = recv_lo[q];
+    ctx->zrecv[1][q] = recv_hi[q];
+    ctx->zpush[0][q] = push_lo[q];
+    ctx->zpush[1][q] = push_hi[q];
+  }
+  ctx->zpush_on = 1;
+  ctx->zpar = 0;
+  ctx->zsend[0] = ctx->zsend[1] = nullptr;
+  drop_run_graph(ctx);
+  ctx->G.zhalo[0] = recv_lo[0];
+  ctx->G.zhalo[1] = recv_hi[0];
+  ctx->G.fb = recv_lo[0] ? nullptr : ctx->fb;
+  ctx->G.zwrap[0] = recv_lo[0] && wrap_lo ? 1 : 0;
+  ctx->G.zwrap[1] = recv_hi[0] && wrap_hi ? 1 : 0;
+  return HMN_OK;
+}
+
+// push mode: store the current state's boundary layers into the neighbours'
+// halo buffers of the current parity (after an upload, before the first stage)
+static int push_current_halos(hmn_ctx* ctx) {
+  CK(launch_pack_zhalos(ctx->pbuf[ctx->pcur], ctx->n, 10 + ctx->par.nspc, ctx->zpush[0][ctx->zpar],
+                        ctx->zpush[1][ctx->zpar], blocks_for(ctx), ctx->st),
+     "push halos");
+  ctx->launches += 1;
+  return HMN_OK;
+}
+
 extern "C" int hmn_pack_halos(hmn_ctx* ctx) {
   if (!ctx) return HMN_EINVAL;
+  if (ctx->zpush_on) return push_current_halos(ctx);
   if (!slab_exchanges(ctx)) return HMN_OK;  // a single slab has nothing to send
   CK(launch_pack_zhalos(ctx->pbuf[ctx->pcur], ctx->n, 10 + ctx->par.nspc, ctx->zsend[0], ctx->zsend[1],
                         blocks_for(ctx), ctx->st),

@@ -116,6 +116,9 @@ struct StageArgs {
   int nspc;             // passive scalars (primitive planes NP.. of pin/pout)
   int stage;            // RK stage, 1-based
   double* spcorg;       // spc * density at stage 1 (rungekutta.f90:67), nspc planes
+  // z slabs exchanging by push: the low ([0]) and high ([1]) neighbours'
+  // halo buffers this stage's output layers go to (nullptr: no neighbour)
+  double* push[2];
 };
 
 // Arguments of one hyperbolic-gravity RK stage (hmn_kernels.cu: hg_stage_kernel).

@@ -276,7 +276,7 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
 
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
 // (x fastest).  Shared by the single-grid and the batched kernels.
-template <bool MAG, bool GLM, class TL, bool SPH = false>
+template <bool MAG, bool GLM, class TL, bool SPH = false, bool PUSH = false>
 __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageArgs& A, SmemT<TL>& sm, int tile_id,
                                                  const TmaMaps* tm) {
   const int tid = threadIdx.x;
@@ -402,14 +402,15 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
       Po[(size_t)(NP + n) * pl + c] = (A.faco * xo + A.facn * x * A.pin[c] + dtf * accs[n]) / d;
     }
   }
+  if constexpr (PUSH) push_boundary_layers(G, A, Po, c, i, j, k);
 }
 
-template <bool MAG, bool GLM, class TL, bool SPH = false>
+template <bool MAG, bool GLM, class TL, bool SPH = false, bool PUSH = false>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel(const GridDev G, const StageArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
   if (A.sc->done) return;
-  stage_tile_exact<MAG, GLM, TL, SPH>(G, A, sm, blockIdx.x, nullptr);
+  stage_tile_exact<MAG, GLM, TL, SPH, PUSH>(G, A, sm, blockIdx.x, nullptr);
 }
 
 // the same stage with the stencil region staged by TMA (3-D tiles)
@@ -716,6 +717,40 @@ void stage_tile(const int solve[3], int precision, int nspc, int tile[3]) {
   }
 }
 
+// z slabs exchanging by push: the stage kernel also stores its two
+// boundary layers into the neighbours' halo buffers (3-D Cartesian tiles)
+template <bool MAG, bool GLM, class TL>
+static cudaError_t launch_stage_push_t(const GridDev& G, const StageArgs& A, cudaStream_t st) {
+  constexpr int smem = (int)sizeof(SmemT<TL>);
+  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<MAG, GLM, TL, false, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  stage_kernel<MAG, GLM, TL, false, true><<<blocks, TL::NT, smem, st>>>(G, A);
+  return cudaGetLastError();
+}
+
+template <class TL>
+static cudaError_t launch_stage_push_tl(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  if (mag && glm) return launch_stage_push_t<true, true, TL>(G, A, st);
+  if (mag) return launch_stage_push_t<true, false, TL>(G, A, st);
+  return launch_stage_push_t<false, false, TL>(G, A, st);
+}
+
+static cudaError_t launch_stage_push(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  const int* t = A.tile;
+  if (G.sph.on || t[2] == 1) return cudaErrorInvalidValue;
+  if (A.nspc > 4) return launch_stage_push_tl<Tile<8, 8, 4, 384, 1, 8>>(G, A, mag, glm, st);
+  if (A.nspc > 0) return launch_stage_push_tl<Tile<8, 8, 4, 384, 2, 4>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_push_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, st);
+  if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_push_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, st);
+  return cudaErrorInvalidValue;
+}
+
 // The stage tiles whose shared-memory layout has room for SP passive
 // scalars (8 x 8 x 4 in 3-D; with 8 scalars its 203 KB allow one CTA per SM)
 template <int SP, int MINB3>
@@ -737,6 +772,7 @@ static cudaError_t launch_scalar_tiles(const GridDev& G, const StageArgs& A, boo
 
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st) {
+  if (A.push[0] != nullptr || A.push[1] != nullptr) return launch_stage_push(G, A, mag, glm, st);
   if (G.sph.on) return launch_stage_spherical(G, A, mag, glm, st);
   const int* t = A.tile;
   if (A.nspc > 0) {  // tiles with room for up to 4, or up to 8, passive scalars

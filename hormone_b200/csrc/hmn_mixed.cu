@@ -251,7 +251,7 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
 
 // One tile of one RK stage; `tile_id` enumerates the tiles of the grid
 // (x fastest).  Shared by the single-grid and the batched kernels.
-template <bool MAG, bool GLM, class TL, bool SPH = false>
+template <bool MAG, bool GLM, class TL, bool SPH = false, bool PUSH = false>
 __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageArgs& A, SmemMixed<TL>& sm, int tile_id,
                                                  const TmaMaps* tm) {
   const int tid = threadIdx.x;
@@ -357,14 +357,15 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
     A.sc->err_j = j;
     A.sc->err_k = k;
   }
+  if constexpr (PUSH) push_boundary_layers(G, A, Po, c, i, j, k);
 }
 
-template <bool MAG, bool GLM, class TL, bool SPH = false>
+template <bool MAG, bool GLM, class TL, bool SPH = false, bool PUSH = false>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) stage_kernel_mixed(const GridDev G, const StageArgs A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
   if (A.sc->done) return;
-  stage_tile_mixed<MAG, GLM, TL, SPH>(G, A, sm, blockIdx.x, nullptr);
+  stage_tile_mixed<MAG, GLM, TL, SPH, PUSH>(G, A, sm, blockIdx.x, nullptr);
 }
 
 // the same stage with the stencil region staged by TMA (3-D tiles)
@@ -449,8 +450,37 @@ static cudaError_t launch_mixed_spherical(const GridDev& G, const StageArgs& A, 
   return cudaErrorInvalidValue;
 }
 
+// z slabs exchanging by push (see push_boundary_layers): 3-D Cartesian tiles
+template <bool MAG, bool GLM, class TL>
+static cudaError_t launch_mixed_push_t(const GridDev& G, const StageArgs& A, cudaStream_t st) {
+  constexpr int smem = (int)sizeof(SmemMixed<TL>);
+  const int blocks = A.tiles[0] * A.tiles[1] * A.tiles[2];
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel_mixed<MAG, GLM, TL, false, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  stage_kernel_mixed<MAG, GLM, TL, false, true><<<blocks, TL::NT, smem, st>>>(G, A);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_mixed_push(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st) {
+  const int* t = A.tile;
+  if (G.sph.on || t[2] == 1) return cudaErrorInvalidValue;
+  using T4 = Tile<8, 8, 4, 384, 2>;
+  using T8 = Tile<8, 8, 8, 640, 1>;
+  const bool t884 = t[0] == 8 && t[1] == 8 && t[2] == 4, t888 = t[0] == 8 && t[1] == 8 && t[2] == 8;
+  if (!t884 && !t888) return cudaErrorInvalidValue;
+  if (mag && glm) return t884 ? launch_mixed_push_t<true, true, T4>(G, A, st) : launch_mixed_push_t<true, true, T8>(G, A, st);
+  if (mag) return t884 ? launch_mixed_push_t<true, false, T4>(G, A, st) : launch_mixed_push_t<true, false, T8>(G, A, st);
+  return t884 ? launch_mixed_push_t<false, false, T4>(G, A, st) : launch_mixed_push_t<false, false, T8>(G, A, st);
+}
+
 cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                                cudaStream_t st) {
+  if (A.push[0] != nullptr || A.push[1] != nullptr) return launch_mixed_push(G, A, mag, glm, st);
   if (G.sph.on) return launch_mixed_spherical(G, A, mag, glm, st);
   const int* t = A.tile;
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_mixed_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);

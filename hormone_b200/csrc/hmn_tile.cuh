@@ -467,6 +467,25 @@ __device__ __forceinline__ StageArgs batch_stage_args(SimDesc& S, int stage, int
 // 2 = 1-D x 256
 constexpr int kBatchKinds = 3;
 
+// z slabs exchanging by push: a cell of the two bottom (top) layers also
+// stores the primitive planes it just wrote into the low (high) neighbour's
+// halo buffer, plane p layer l at (p * 2 + l) * nx * ny + i + nx * j, the
+// layout the neighbour's staging reads.  On several GPUs the buffer is the
+// neighbour's memory, so the exchange runs inside the stage, cell by cell.
+__device__ __forceinline__ void push_boundary_layers(const GridDev& G, const StageArgs& A, const double* Po,
+                                                     size_t c, int i, int j, int k) {
+  const size_t hp = (size_t)G.n[0] * G.n[1], hc = (size_t)i + (size_t)G.n[0] * j, pl = A.plane;
+  const int np = NP + A.nspc;
+#pragma unroll
+  for (int side = 0; side < 2; side++) {
+    double* D = A.push[side];
+    const int l = side == 0 ? k : k - (G.n[2] - 2);
+    if (D == nullptr || l < 0 || l > 1) continue;
+    const size_t o = (size_t)l * hp + hc;
+    for (int p = 0; p < np; p++) D[(size_t)p * 2 * hp + o] = Po[(size_t)p * pl + c];
+  }
+}
+
 // Spherical metric weights of the flux divergence of cell (i,j,k) along AX
 // (rungekutta.f90:42-53 with metric.f90:105-125): the cell adds
 // cw (fm F(low face) - fp F(high face)).  Along phi the reference has no face

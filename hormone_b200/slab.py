@@ -10,13 +10,19 @@ bit-identical to the same cells of the undecomposed run: every cell sees the
 same neighbours and the same operation order, and min/max reductions are
 exact.
 
-Two exchanges are provided:
+Two ways to move the halos:
 
-- ``TorchExchange``: one process per slab over ``torch.distributed``.  It
-  uses NCCL with CUDA tensors on GPUs and gloo with CPU tensors for the
-  host-side tests.
-- ``LocalExchange``: all slabs in one process, e.g. on one GPU, exchanging
-  by device copies.
+- copy: before every stage each slab packs its boundary layers
+  (``hmn_pack_halos``) and the exchange delivers them to the neighbours'
+  halo buffers.  ``TorchExchange`` does it with point-to-point messages over
+  ``torch.distributed`` (NCCL with CUDA tensors, gloo with CPU tensors for
+  the host-side tests); ``LocalExchange`` with device copies.
+- push (``hmn_set_slab_push``): each stage's kernel stores its boundary
+  layers straight into the neighbours' halo buffers as it writes them
+  (double-buffered by stage parity); between stages only a barrier runs.
+  ``LocalExchange(mode="push")`` runs it with all slabs in one process;
+  ``SymmetricHalos`` allocates the halo buffers in symmetric memory so that
+  one process per GPU can store into its neighbours' buffers.
 """
 from __future__ import annotations
 
@@ -50,6 +56,17 @@ def neighbours(rank: int, world: int, periodic: bool) -> Tuple[Optional[int], Op
     return lo, hi
 
 
+def push_links(world: int, periodic: bool) -> List[Dict[str, Optional[Tuple[int, str]]]]:
+    """For each rank of the push exchange: whose halo buffer its bottom
+    layers go to (the low neighbour's "hi" buffers) and its top layers
+    (the high neighbour's "lo" buffers); None on a physical face."""
+    out = []
+    for r in range(world):
+        lo, hi = neighbours(r, world, periodic)
+        out.append({"lo": None if lo is None else (lo, "hi"), "hi": None if hi is None else (hi, "lo")})
+    return out
+
+
 def slab_config(cfg: dict, k0: int, k1: int) -> dict:
     """The configuration of the slab [k0, k1): same settings, n[2] = k1 - k0."""
     c = dict(cfg)
@@ -80,9 +97,11 @@ class SlabSimulation:
     phases that the exchange interleaves."""
 
     def __init__(self, cfg: dict, prims_global: Dict[str, np.ndarray], k0: int, k1: int, precision: int = 0,
-                 halo_alloc=None, local: bool = False):
+                 halo_alloc=None, local: bool = False, mode: str = "copy"):
         """prims_global: the global primitives (sliced here), or with
-        local=True the slab's own primitives."""
+        local=True the slab's own primitives.  mode "copy" allocates send and
+        receive halo buffers, "push" two receive buffers per face (one per
+        stage parity)."""
         import torch
 
         self.cfg_global = cfg
@@ -100,8 +119,13 @@ class SlabSimulation:
         if self.nspc:
             self.ctx.upload_scalars(st["spc"])
         n = self.ctx.halo_bytes() // 8
+        self.halo_n = n
+        self.mode = mode
         alloc = halo_alloc or (lambda m: torch.zeros(m, dtype=torch.float64, device="cuda"))
-        self.send_lo, self.send_hi, self.recv_lo, self.recv_hi = (alloc(n) for _ in range(4))
+        if mode == "push":
+            self.recv = {(side, q): alloc(n) for side in ("lo", "hi") for q in (0, 1)}
+        else:
+            self.send_lo, self.send_hi, self.recv_lo, self.recv_hi = (alloc(n) for _ in range(4))
         self.time, self.tn = 0.0, 0
         self.t_out, self.t_end = cfg["t_out"], cfg["t_end"]
         self.dt = self.ch = 0.0
@@ -116,6 +140,15 @@ class SlabSimulation:
         p = lambda t: t.data_ptr()  # noqa: E731
         self.ctx.set_slab(p(self.send_lo) if has_lo else 0, p(self.send_hi) if has_hi else 0,
                           p(self.recv_lo) if has_lo else 0, p(self.recv_hi) if has_hi else 0, wrap_lo, wrap_hi)
+
+    def connect_push(self, has_lo: bool, has_hi: bool, push_lo, push_hi, wrap_lo: bool = False,
+                     wrap_hi: bool = False):
+        """The push exchange: push_lo/push_hi are the (parity 0, parity 1)
+        device addresses of the neighbours' buffers this slab stores into."""
+        p = lambda t: t.data_ptr()  # noqa: E731
+        rl = (p(self.recv["lo", 0]), p(self.recv["lo", 1])) if has_lo else (0, 0)
+        rh = (p(self.recv["hi", 0]), p(self.recv["hi", 1])) if has_hi else (0, 0)
+        self.ctx.set_slab_push(rl, rh, push_lo if has_lo else (0, 0), push_hi if has_hi else (0, 0), wrap_lo, wrap_hi)
 
     def stream(self):
         import torch
@@ -157,11 +190,28 @@ class LocalExchange:
     """All slabs of a grid in one process (e.g. on one GPU): halos move by
     device copies, the CFL partials by an in-process min/max."""
 
-    def __init__(self, cfg: dict, prims: Dict[str, np.ndarray], world: int, precision: int = 0):
+    def __init__(self, cfg: dict, prims: Dict[str, np.ndarray], world: int, precision: int = 0,
+                 mode: str = "copy"):
         self.periodic = int(cfg["bc"][2][0][0]) == 0
+        self.mode = mode
         self.parts = partition(cfg["n"][2], world)
-        self.ranks = [SlabSimulation(cfg, prims, k0, k1, precision) for k0, k1 in self.parts]
+        self.ranks = [SlabSimulation(cfg, prims, k0, k1, precision, mode=mode) for k0, k1 in self.parts]
         self.nb = [neighbours(r, world, self.periodic) for r in range(world)]
+        if mode == "push":
+            links = push_links(world, self.periodic)
+            for r, s in enumerate(self.ranks):
+                lo, hi = self.nb[r]
+                tgt = {}
+                for face in ("lo", "hi"):
+                    link = links[r][face]
+                    tgt[face] = ((0, 0) if link is None else
+                                 tuple(self.ranks[link[0]].recv[link[1], q].data_ptr() for q in (0, 1)))
+                s.connect_push(lo is not None, hi is not None, tgt["lo"], tgt["hi"], wrap_lo=r == 0,
+                               wrap_hi=r == world - 1)
+            for s in self.ranks:  # the initial state's boundary layers
+                s.ctx.pack_halos()
+            self._sync()
+            return
         for r, s in enumerate(self.ranks):
             lo, hi = self.nb[r]
             s.connect(lo is not None, hi is not None, wrap_lo=r == 0, wrap_hi=r == world - 1)
@@ -188,6 +238,11 @@ class LocalExchange:
         for s in self.ranks:
             s.cfl_finalize()
         for stage in range(1, self.cfg_rk() + 1):
+            if self.mode == "push":  # the previous stage of every slab has stored its layers
+                self._sync()
+                for s in self.ranks:
+                    s.ctx.hydro_stage(stage)
+                continue
             for s in self.ranks:
                 s.ctx.pack_halos()
             self._sync()
@@ -248,6 +303,69 @@ class TorchExchange:
     def cfl(self, tmin, tmax):
         self.dist.all_reduce(tmin, op=self.dist.ReduceOp.MIN)
         self.dist.all_reduce(tmax, op=self.dist.ReduceOp.MAX)
+
+
+class SymmetricHalos:
+    """The push exchange's halo buffers in symmetric memory, one process per
+    GPU: a rank's four receive buffers (low and high face, two stage
+    parities) are one symmetric allocation, so a neighbour's kernel can
+    store into them directly (peer access over NVLink).  Sections are
+    ordered (lo, 0), (lo, 1), (hi, 0), (hi, 1) of ``n`` doubles each.
+    (Not run on more than one GPU here: every GPU call of this build had
+    one.)"""
+
+    SECTION = {("lo", 0): 0, ("lo", 1): 1, ("hi", 0): 2, ("hi", 1): 3}
+
+    def __init__(self, n: int, group=None):
+        import torch
+        import torch.distributed as dist
+        import torch.distributed._symmetric_memory as symm_mem
+
+        self.n = n
+        self.buf = symm_mem.empty(4 * n, dtype=torch.float64, device="cuda")
+        self.buf.zero_()
+        self.hdl = symm_mem.rendezvous(self.buf, group if group is not None else dist.group.WORLD)
+        ptrs = self.hdl.buffer_ptrs
+        self.ptrs = list(ptrs() if callable(ptrs) else ptrs)
+
+    def local(self, side: str, q: int):
+        k = self.SECTION[side, q]
+        return self.buf[k * self.n:(k + 1) * self.n]
+
+    def peer(self, rank: int, side: str, q: int) -> int:
+        """Device address of rank's (side, parity) buffer in this process."""
+        return int(self.ptrs[rank]) + self.SECTION[side, q] * self.n * 8
+
+
+def connect_symmetric(sim: "SlabSimulation", halos: SymmetricHalos, rank: int, world: int, periodic: bool):
+    """Wire a push-mode slab to its neighbours' symmetric halo buffers and
+    store the initial boundary layers (followed by the caller's barrier)."""
+    links = push_links(world, periodic)[rank]
+    lo, hi = neighbours(rank, world, periodic)
+    sim.recv = {(side, q): halos.local(side, q) for side in ("lo", "hi") for q in (0, 1)}
+    tgt = {face: ((0, 0) if links[face] is None else
+                  tuple(halos.peer(links[face][0], links[face][1], q) for q in (0, 1))) for face in ("lo", "hi")}
+    sim.connect_push(lo is not None, hi is not None, tgt["lo"], tgt["hi"], wrap_lo=rank == 0,
+                     wrap_hi=rank == world - 1)
+    sim.ctx.pack_halos()
+
+
+def run_distributed_push_step(sim: "SlabSimulation", ex: TorchExchange) -> bool:
+    """One step of one rank with the push exchange: the CFL all-reduce, then
+    per stage a barrier (every slab finished the previous stage, so its
+    layers are in place) and the stage, whose kernel stores this slab's
+    boundary layers into the neighbours' buffers."""
+    import torch
+
+    with torch.cuda.stream(sim.stream()):
+        sim.cfl_local()
+        ex.cfl(sim.cfl_min, sim.cfl_max)
+        sim.cfl_finalize()
+        for stage in range(1, int(sim.cfg["rktype"]) + 1):
+            sim.ctx.sync()
+            ex.dist.barrier()
+            sim.ctx.hydro_stage(stage)
+    return sim.finish_step()
 
 
 def run_distributed_step(sim: SlabSimulation, ex: TorchExchange) -> bool:

@@ -212,6 +212,22 @@ int hmn_checkpoint_wait(hmn_ctx* ctx);
 size_t hmn_slab_halo_bytes(const hmn_ctx* ctx);
 int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo, const double* recv_hi,
                  int wrap_lo, int wrap_hi);
+
+/* The push exchange (instead of hmn_set_slab): recv_lo/recv_hi are this
+ * slab's halo buffers (hmn_slab_halo_bytes each) for stage parity 0 and 1,
+ * push_lo/push_hi the low and high neighbours' buffers that receive this
+ * slab's bottom and top layers (the low neighbour's recv_hi, the high
+ * neighbour's recv_lo; NULL entries on a physical face).  Each stage's
+ * kernel stores its two boundary layers straight into the neighbours'
+ * buffers while it writes them, so no pack kernel or message runs between
+ * stages; on several GPUs the push buffers are the neighbours' memory
+ * (peer access or symmetric memory).  Every slab must have finished a
+ * stage before any starts the next (the caller's barrier).  Before the
+ * first stage, and after any upload, hmn_pack_halos stores the current
+ * layers.  3-D Cartesian grids without gravity. */
+int hmn_set_slab_push(hmn_ctx* ctx, const double* const recv_lo[2], const double* const recv_hi[2],
+                      double* const push_lo[2], double* const push_hi[2], int wrap_lo, int wrap_hi);
+
 int hmn_pack_halos(hmn_ctx* ctx);
 int hmn_hydro_stage(hmn_ctx* ctx, int stage);
 int hmn_cfl_local(hmn_ctx* ctx, double time, double t_out, double t_end);

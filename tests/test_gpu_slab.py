@@ -1,7 +1,9 @@
 """Slab decomposition along z on one GPU: the slabs of one grid, each its
 own context, exchanging halos by device copies (hormone_b200.slab.
 LocalExchange), give bit for bit the undecomposed run's state and dt,
-periodic or not, with scalars, and in the mixed-precision form."""
+periodic or not, with scalars, and in the mixed-precision form; so do
+slabs whose stage kernels push their boundary layers into the neighbours'
+halo buffers (mode "push")."""
 import numpy as np
 import pytest
 
@@ -13,9 +15,9 @@ import cases
 pytestmark = pytest.mark.gpu
 
 
-def run_both(cfg, prims, world, steps, precision=0):
+def run_both(cfg, prims, world, steps, precision=0, mode="copy"):
     ref = Simulation(cfg, prims, precision=precision)
-    dec = slab.LocalExchange(cfg, prims, world, precision=precision)
+    dec = slab.LocalExchange(cfg, prims, world, precision=precision, mode=mode)
     for n in range(steps):
         ref.step()
         dec.step()
@@ -62,6 +64,44 @@ def test_riemann_with_scalars():
 def test_mixed_precision_slabs():
     cfg, prims = cases.ot3d(16)
     run_both(cfg, prims, 2, 4, precision=1)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_push_exchange_orszag_tang_periodic(world):
+    """One slab wraps onto itself; two periodic slabs are each other's low
+    and high neighbour."""
+    cfg, prims = cases.ot3d(16)
+    run_both(cfg, prims, world, 5, mode="push")
+
+
+def test_push_exchange_blast_reflective():
+    cfg, prims = cases.blast3d(14, bc=1, mag=True)
+    run_both(cfg, prims, 3, 5, mode="push")
+
+
+@pytest.mark.parametrize("nspc", [2, 5])
+def test_push_exchange_with_scalars(nspc):
+    """Scalar planes ride in the pushed layers (the 4- and 8-scalar
+    kernels)."""
+    cfg, prims = cases.riemann3d(n=(12, 10, 8), bc=(3, 1, 0), nspc=nspc)
+    run_both(cfg, prims, 2, 5, mode="push")
+
+
+@pytest.mark.parametrize("case", ["ot3d", "blast"])
+def test_push_exchange_mixed_precision(case):
+    if case == "ot3d":
+        cfg, prims = cases.ot3d(16)
+    else:
+        cfg, prims = cases.blast3d(14, bc=1, mag=True)
+    run_both(cfg, prims, 3, 4, precision=1, mode="push")
+
+
+def test_push_exchange_refuses_curvilinear_and_gravity():
+    from hormone_b200 import capi
+
+    cfg, prims = cases.spherical((16, 12, 8), mag=True, xi1s=0.2)
+    with pytest.raises(capi.HmnError):
+        slab.LocalExchange(cfg, prims, 2, mode="push")
 
 
 def test_decomposed_context_refuses_the_undecomposed_calls():

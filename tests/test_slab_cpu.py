@@ -27,6 +27,28 @@ def test_partition_and_neighbours():
     assert slab.neighbours(0, 1, True) == (None, None)
 
 
+def test_push_links_pair_faces():
+    """Push exchange: a slab's bottom layers go to its low neighbour's "hi"
+    buffers and its top layers to the high neighbour's "lo" buffers; every
+    buffer that a slab reads has exactly one writer."""
+    assert slab.push_links(1, True) == [{"lo": None, "hi": None}]
+    assert slab.push_links(3, False) == [{"lo": None, "hi": (1, "lo")}, {"lo": (0, "hi"), "hi": (2, "lo")},
+                                         {"lo": (1, "hi"), "hi": None}]
+    assert slab.push_links(2, True) == [{"lo": (1, "hi"), "hi": (1, "lo")}, {"lo": (0, "hi"), "hi": (0, "lo")}]
+    for world in (2, 3, 5):
+        for periodic in (False, True):
+            links = slab.push_links(world, periodic)
+            writers = {}
+            for r, lk in enumerate(links):
+                for face in ("lo", "hi"):
+                    if lk[face] is not None:
+                        assert lk[face] not in writers
+                        writers[lk[face]] = r
+            for r in range(world):
+                lo, hi = slab.neighbours(r, world, periodic)
+                assert writers.get((r, "lo")) == lo and writers.get((r, "hi")) == hi
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
