@@ -365,8 +365,17 @@ def _bind_slab(L):
     L.hmn_cfl_local.argtypes = [_P, _D, _D, _D]
     L.hmn_cfl_partials.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_P)]
     L.hmn_cfl_finalize.argtypes = [_P, _DP, _DP]
+    L.hmn_slab_gravity_halo_bytes.argtypes = [_P]
+    L.hmn_slab_gravity_halo_bytes.restype = ctypes.c_size_t
+    L.hmn_set_slab_gravity.argtypes = [_P, _P, _P, _P, _P]
+    L.hmn_pack_gravity_halos.argtypes = [_P]
+    L.hmn_gravity_unit.argtypes = [_P, _DP]
+    L.hmn_set_gravity_unit.argtypes = [_P, _D]
+    L.hmn_gravity_begin.argtypes = [_P, _D, _D, _I, ctypes.POINTER(_I)]
+    L.hmn_gravity_substage.argtypes = [_P]
     for n in ("hmn_set_slab", "hmn_pack_halos", "hmn_hydro_stage", "hmn_cfl_local", "hmn_cfl_partials",
-              "hmn_cfl_finalize"):
+              "hmn_cfl_finalize", "hmn_set_slab_gravity", "hmn_pack_gravity_halos", "hmn_gravity_unit",
+              "hmn_set_gravity_unit", "hmn_gravity_begin", "hmn_gravity_substage"):
         getattr(L, n).restype = _I
     L._hmn_slab_bound = True
     return L
@@ -396,6 +405,35 @@ class SlabContext(Context):
 
     def pack_halos(self):
         self._check(_bind_slab(lib()).hmn_pack_halos(self.h), "hmn_pack_halos")
+
+    # the potential's halos and the gravity sub-stages of a slab with gravity
+    def gravity_halo_bytes(self) -> int:
+        return int(_bind_slab(lib()).hmn_slab_gravity_halo_bytes(self.h))
+
+    def set_slab_gravity(self, send_lo, send_hi, recv_lo, recv_hi):
+        L = _bind_slab(lib())
+        self._check(L.hmn_set_slab_gravity(self.h, send_lo or None, send_hi or None, recv_lo or None,
+                                           recv_hi or None), "hmn_set_slab_gravity")
+
+    def pack_gravity_halos(self):
+        self._check(_bind_slab(lib()).hmn_pack_gravity_halos(self.h), "hmn_pack_gravity_halos")
+
+    def gravity_unit(self) -> float:
+        v = _D()
+        self._check(_bind_slab(lib()).hmn_gravity_unit(self.h, ctypes.byref(v)), "hmn_gravity_unit")
+        return v.value
+
+    def set_gravity_unit(self, dtg_unit: float):
+        self._check(_bind_slab(lib()).hmn_set_gravity_unit(self.h, float(dtg_unit)), "hmn_set_gravity_unit")
+
+    def gravity_begin(self, time, dt, tn) -> int:
+        n = _I()
+        self._check(_bind_slab(lib()).hmn_gravity_begin(self.h, float(time), float(dt), int(tn), ctypes.byref(n)),
+                    "hmn_gravity_begin")
+        return n.value
+
+    def gravity_substage(self):
+        self._check(_bind_slab(lib()).hmn_gravity_substage(self.h), "hmn_gravity_substage")
 
     def hydro_stage(self, stage: int):
         self._check(_bind_slab(lib()).hmn_hydro_stage(self.h, int(stage)), "hmn_hydro_stage")

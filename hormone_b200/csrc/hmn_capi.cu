@@ -57,6 +57,11 @@ struct hmn_ctx {
   const double* zrecv[2][2];
   double* zpush[2][2];
   int zpush_on, zpar;
+  double* gsend[2];          // slab decomposition with gravity: caller's potential send buffers
+  // the gravity sub-cycles planned by the last hmn_gravity_begin: cycles
+  // left, the next RK sub-stage, the cycle's step, speed and psi damping
+  int gv_left, gv_g;
+  double gv_dtgrav, gv_cgrav, gv_damp;
   double* dir[3][2];         // Dirichlet ghost values per face (device)
   double* fb;                // boundary code 10: the inner x3 face's flux (device, 9 + nspc)
   double* spcorg;            // passive scalars times density at RK stage 1
@@ -918,7 +923,7 @@ extern "C" size_t hmn_slab_halo_bytes(const hmn_ctx* ctx) {
 extern "C" int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo,
                             const double* recv_hi, int wrap_lo, int wrap_hi) {
   if (!ctx) return HMN_EINVAL;
-  if (!ctx->solve[2] || ctx->n[2] < 2 || ctx->par.gravswitch != 0) return HMN_EBADCFG;
+  if (!ctx->solve[2] || ctx->n[2] < 2 || (ctx->par.gravswitch != 0 && ctx->G.sph.on)) return HMN_EBADCFG;
   if ((recv_lo && !send_lo) || (recv_hi && !send_hi)) return HMN_EINVAL;
   ctx->zsend[0] = send_lo;
   ctx->zsend[1] = send_hi;
@@ -928,6 +933,70 @@ extern "C" int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, cons
   ctx->G.fb = recv_lo ? nullptr : ctx->fb;  // code 10 lives on the grid's inner z face only
   ctx->G.zwrap[0] = recv_lo && wrap_lo ? 1 : 0;
   ctx->G.zwrap[1] = recv_hi && wrap_hi ? 1 : 0;
+  return HMN_OK;
+}
+
+extern "C" size_t hmn_slab_gravity_halo_bytes(const hmn_ctx* ctx) {
+  if (!ctx) return 0;
+  return (size_t)ctx->n[0] * ctx->n[1] * sizeof(double);
+}
+
+// Slab decomposition with hyperbolic self-gravity: the potential's layer
+// beyond each neighbouring z face comes from the neighbour (its bottom or
+// top layer, exchanged by the caller before every gravity sub-stage and
+// once after the last) for the Laplacian and for the force of the hydro
+// stages.  After hmn_set_slab, on the faces it gave halos for.
+extern "C" int hmn_set_slab_gravity(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo,
+                                    const double* recv_hi) {
+  if (!ctx) return HMN_EINVAL;
+  if (ctx->par.gravswitch != 3 || ctx->G.sph.on || ctx->zpush_on) return HMN_EBADCFG;
+  if ((recv_lo != nullptr) != (ctx->G.zhalo[0] != nullptr) || (recv_hi != nullptr) != (ctx->G.zhalo[1] != nullptr) ||
+      (recv_lo && !send_lo) || (recv_hi && !send_hi))
+    return HMN_EINVAL;
+  ctx->gsend[0] = send_lo;
+  ctx->gsend[1] = send_hi;
+  ctx->G.ghalo[0] = recv_lo;
+  ctx->G.ghalo[1] = recv_hi;
+  drop_run_graph(ctx);
+  return HMN_OK;
+}
+
+// the potential's halo faces match the primitives' (a slab with gravity
+// exchanges both)
+static bool gravity_halos_set(const hmn_ctx* ctx) {
+  return (ctx->G.zhalo[0] == nullptr || ctx->G.ghalo[0] != nullptr) &&
+         (ctx->G.zhalo[1] == nullptr || ctx->G.ghalo[1] != nullptr);
+}
+
+extern "C" int hmn_pack_gravity_halos(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  if (ctx->par.gravswitch != 3) return HMN_EBADCFG;
+  const size_t layer = (size_t)ctx->n[0] * ctx->n[1];
+  const double* phi = ctx->gphi[ctx->gcur];
+  if (ctx->gsend[0])
+    CK(cudaMemcpyAsync(ctx->gsend[0], phi, layer * sizeof(double), cudaMemcpyDeviceToDevice, ctx->st), "pack");
+  if (ctx->gsend[1])
+    CK(cudaMemcpyAsync(ctx->gsend[1], phi + (size_t)(ctx->n[2] - 1) * layer, layer * sizeof(double),
+                       cudaMemcpyDeviceToDevice, ctx->st),
+       "pack");
+  return HMN_OK;
+}
+
+extern "C" int hmn_gravity_unit(hmn_ctx* ctx, double* dtg_unit) {
+  if (!ctx || !dtg_unit) return HMN_EINVAL;
+  *dtg_unit = ctx->dtg_unit;
+  return HMN_OK;
+}
+
+// the grid-wide dtg_unit (tools.f90:160-183 is a minimum over all cells):
+// slabs of one grid set the minimum over the slabs
+extern "C" int hmn_set_gravity_unit(hmn_ctx* ctx, double dtg_unit) {
+  if (!ctx || !(dtg_unit > 0.0)) return HMN_EINVAL;
+  ctx->dtg_unit = dtg_unit;
+  CK(cudaMemcpyAsync(&ctx->sc->dtg_unit, &ctx->dtg_unit, sizeof(double), cudaMemcpyHostToDevice, ctx->st),
+     "gravity unit");
+  CK(cudaStreamSynchronize(ctx->st), "gravity unit");
+  drop_run_graph(ctx);
   return HMN_OK;
 }
 
@@ -987,6 +1056,7 @@ extern "C" int hmn_pack_halos(hmn_ctx* ctx) {
 
 extern "C" int hmn_hydro_stage(hmn_ctx* ctx, int stage) {
   if (!ctx || stage < 1 || stage > ctx->par.rktype) return HMN_EINVAL;
+  if (ctx->par.gravswitch == 3 && !gravity_halos_set(ctx)) return HMN_EBADCFG;  // the force needs them
   return enqueue_stage(ctx, stage);
 }
 
@@ -1037,58 +1107,94 @@ static int sph_gravity_boundary(hmn_ctx* ctx) {
   return HMN_OK;
 }
 
-extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
-  if (!ctx) return HMN_EINVAL;
+// Plan the sub-cycles of gravity_hyperbolic.f90:19-60 for the step
+// [time, time + dt]: *nsub = tngrav x grktype sub-stages (0 at tn = 0, where
+// grav_init_other only sets the clock).
+extern "C" int hmn_gravity_begin(hmn_ctx* ctx, double time, double dt, int tn, int* nsub) {
+  if (!ctx || !nsub) return HMN_EINVAL;
+  *nsub = 0;
+  ctx->gv_left = 0;
   if (ctx->par.gravswitch != 3) return HMN_OK;
   if (!ctx->G.sph.on && ctx->dim != 3) return HMN_EBADCFG;  // the Cartesian solver is 3-D
-  if (tn == 0) {  // grav_init_other: only the boundary images, which the kernels form on the fly
+  if (!gravity_halos_set(ctx)) return HMN_EBADCFG;
+  if (tn == 0) {
     ctx->grvtime = time;
-    return sph_gravity_boundary(ctx);
+    return HMN_OK;
   }
   // cgrav and dtgrav of the last hmn_timestep
   int rc = fetch_scalars(ctx);
   if (rc) return rc;
   const double cgrav = ctx->sc_h->cgrav;
-  double dtgrav = ctx->sc_h->dtgrav;
+  const double dtgrav = ctx->sc_h->dtgrav;
   const int tngrav = (int)std::ceil((time + dt - ctx->grvtime) / dtgrav);  // gravity_hyperbolic.f90:33-34
   if (tngrav < 1) return HMN_OK;
-  dtgrav = (time + dt - ctx->grvtime) / (double)tngrav;
-  const double* dens = ctx->pbuf[ctx->pcur];  // density plane of the state at the gravity call
-  const double fourpiG = 4.0 * M_PI * ctx->par.G;
-  for (int l = 0; l < tngrav; l++) {
-    const double damp = std::exp(-(1.0 - ctx->cgrav_old / cgrav + ctx->par.alphagrv * ctx->par.hgcfl));
-    for (int g = 1; g <= ctx->par.grktype; g++) {
-      double faco, fact, facn;
-      rk_coeff(g, ctx->par.grktype, &faco, &fact, &facn);
-      HGArgs a;
-      memset(&a, 0, sizeof(a));
-      a.phi_in = ctx->gphi[ctx->gcur];
-      a.psi_in = ctx->gpsi[ctx->gcur];
-      a.phi_out = ctx->gphi[1 - ctx->gcur];
-      a.psi_out = ctx->gpsi[1 - ctx->gcur];
-      a.org_phi = ctx->gorg[0];
-      a.org_psi = ctx->gorg[1];
-      a.dens = dens;
-      a.plane = ctx->plane;
-      a.faco = faco;
-      a.facn = facn;
-      a.fdc = fact * dtgrav * cgrav;
-      a.fourpiG = fourpiG;
-      a.damp = damp;
-      a.stage1 = g == 1;
-      a.last = g == ctx->par.grktype;
-      a.sc = ctx->sc;
-      a.lc = ctx->hgc;
-      a.gin = ctx->gin;
-      if (ctx->G.sph.on)
-        CK(launch_hg_stage_sph(ctx->G, a, ctx->st), "hg stage");
-      else
-        CK(launch_hg_stage(ctx->G, a, blocks_for(ctx), ctx->st), "hg stage");
-      ctx->launches += 1;
-      ctx->gcur = 1 - ctx->gcur;
-    }
+  ctx->gv_dtgrav = (time + dt - ctx->grvtime) / (double)tngrav;
+  ctx->gv_cgrav = cgrav;
+  ctx->gv_left = tngrav;
+  ctx->gv_g = 1;
+  *nsub = tngrav * ctx->par.grktype;
+  return HMN_OK;
+}
+
+// The next RK sub-stage of the planned sub-cycles (hyperbolic_gravity_step,
+// gravity_hyperbolic.f90:62-110); the last sub-stage of a cycle advances the
+// gravity clock.
+extern "C" int hmn_gravity_substage(hmn_ctx* ctx) {
+  if (!ctx) return HMN_EINVAL;
+  if (ctx->gv_left < 1) return HMN_EBADCFG;
+  const int g = ctx->gv_g;
+  const double cgrav = ctx->gv_cgrav, dtgrav = ctx->gv_dtgrav;
+  if (g == 1) ctx->gv_damp = std::exp(-(1.0 - ctx->cgrav_old / cgrav + ctx->par.alphagrv * ctx->par.hgcfl));
+  double faco, fact, facn;
+  rk_coeff(g, ctx->par.grktype, &faco, &fact, &facn);
+  HGArgs a;
+  memset(&a, 0, sizeof(a));
+  a.phi_in = ctx->gphi[ctx->gcur];
+  a.psi_in = ctx->gpsi[ctx->gcur];
+  a.phi_out = ctx->gphi[1 - ctx->gcur];
+  a.psi_out = ctx->gpsi[1 - ctx->gcur];
+  a.org_phi = ctx->gorg[0];
+  a.org_psi = ctx->gorg[1];
+  a.dens = ctx->pbuf[ctx->pcur];  // density plane of the state at the gravity call
+  a.plane = ctx->plane;
+  a.faco = faco;
+  a.facn = facn;
+  a.fdc = fact * dtgrav * cgrav;
+  a.fourpiG = 4.0 * M_PI * ctx->par.G;
+  a.damp = ctx->gv_damp;
+  a.stage1 = g == 1;
+  a.last = g == ctx->par.grktype;
+  a.sc = ctx->sc;
+  a.lc = ctx->hgc;
+  a.gin = ctx->gin;
+  if (ctx->G.sph.on)
+    CK(launch_hg_stage_sph(ctx->G, a, ctx->st), "hg stage");
+  else
+    CK(launch_hg_stage(ctx->G, a, blocks_for(ctx), ctx->st), "hg stage");
+  ctx->launches += 1;
+  ctx->gcur = 1 - ctx->gcur;
+  if (g == ctx->par.grktype) {
     ctx->grvtime = ctx->grvtime + dtgrav;
     ctx->cgrav_old = cgrav;
+    ctx->gv_left -= 1;
+    ctx->gv_g = 1;
+  } else {
+    ctx->gv_g = g + 1;
+  }
+  return HMN_OK;
+}
+
+extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
+  if (!ctx) return HMN_EINVAL;
+  if (ctx->par.gravswitch != 3) return HMN_OK;
+  if (ctx->G.ghalo[0] || ctx->G.ghalo[1]) return HMN_EBADCFG;  // a slab exchanges between sub-stages
+  int nsub = 0;
+  int rc = hmn_gravity_begin(ctx, time, dt, tn, &nsub);
+  if (rc) return rc;
+  if (tn != 0 && nsub == 0) return HMN_OK;
+  for (int l = 0; l < nsub; l++) {
+    rc = hmn_gravity_substage(ctx);
+    if (rc) return rc;
   }
   return sph_gravity_boundary(ctx);
 }

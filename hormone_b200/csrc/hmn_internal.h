@@ -70,6 +70,9 @@ struct GridDev {
   // (energies rebuilt from the pressure) rather than the interior values
   const double* zhalo[2];
   int zwrap[2];
+  // the same for the gravitational potential: the one layer (nx*ny) beyond
+  // the low / high z face, from the neighbouring slab, or nullptr
+  const double* ghalo[2];
   // boundary code 9 (Dirichlet): ghost values of face [axis][inner,outer],
   // 8 + nspc planes (d, p, v1..3, b1..3, scalars) x 2 layers x face cells
   // (layer l at coordinate -2+l inner, n+l outer; the other two axes in

@@ -342,6 +342,8 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
           nb[a] = s + o;
           if (nb[a] >= 0 && nb[a] < G.n[a]) {
             ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+          } else if (a == 2 && G.ghalo[o > 0] != nullptr) {  // the neighbouring slab's layer
+            ph[o + 1] = G.ghalo[o > 0][(size_t)i + (size_t)G.n[0] * j];
           } else if (G.bc[a][0][0] == 0) {
             nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
             ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
@@ -1111,12 +1113,15 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
     cm[2] = gx.dxi[i + 2] * gy.dxi[j + 2] / gz.dx[k + 2];
     cp[2] = gx.dxi[i + 2] * gy.dxi[j + 2] / gz.dx[k + 3];
     const int ijk[3] = {i, j, k};
+    // a z neighbour in the neighbouring slab comes from its halo layer
+    const bool hlo = k == 0 && G.ghalo[0] != nullptr, hhi = k == G.n[2] - 1 && G.ghalo[1] != nullptr;
     bool use_m[3] = {true, true, true}, use_p[3] = {true, true, true};
     size_t nbm[3], nbp[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const int n = G.n[a];
       const bool per = G.bc[a][0][0] == 0;
+      const bool hm = a == 2 && hlo, hp = a == 2 && hhi;
       int m[3] = {i, j, k}, p[3] = {i, j, k};
       m[a] = ijk[a] - 1;
       p[a] = ijk[a] + 1;
@@ -1124,25 +1129,26 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
         if (m[a] < 0) m[a] += n;
         if (p[a] >= n) p[a] -= n;
       } else {
-        if (ijk[a] == n - 1) {
+        if (ijk[a] == n - 1 && !hp) {
           c0 = c0 + cp[a] * rdist(G, i, j, k) / rdist(G, p[0], p[1], p[2]);
           use_p[a] = false;
         }
-        if (ijk[a] == 0) {
+        if (ijk[a] == 0 && !hm) {
           c0 = c0 + cm[a] * rdist(G, i, j, k) / rdist(G, m[0], m[1], m[2]);
           use_m[a] = false;
         }
       }
-      nbm[a] = use_m[a] ? cidx(G, m[0], m[1], m[2]) : c;
-      nbp[a] = use_p[a] ? cidx(G, p[0], p[1], p[2]) : c;
+      nbm[a] = use_m[a] && !hm ? cidx(G, m[0], m[1], m[2]) : c;
+      nbp[a] = use_p[a] && !hp ? cidx(G, p[0], p[1], p[2]) : c;
     }
     const double cn = gx.dxi[i + 2] * gy.dxi[j + 2] * gz.dxi[k + 2];
     const double* ph = A.phi_in;
+    const size_t hc = (size_t)i + (size_t)G.n[0] * j;
     double lap = c0 * ph[c];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      if (use_m[a]) lap = lap + cm[a] * ph[nbm[a]];
-      if (use_p[a]) lap = lap + cp[a] * ph[nbp[a]];
+      if (use_m[a]) lap = lap + cm[a] * (a == 2 && hlo ? G.ghalo[0][hc] : ph[nbm[a]]);
+      if (use_p[a]) lap = lap + cp[a] * (a == 2 && hhi ? G.ghalo[1][hc] : ph[nbp[a]]);
     }
     const double lapphi = lap / cn;
     const double hgsrc = A.fourpiG * A.dens[c];

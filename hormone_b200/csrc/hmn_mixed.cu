@@ -305,6 +305,8 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
           nb[a] = s + o;
           if (nb[a] >= 0 && nb[a] < G.n[a]) {
             ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];
+          } else if (a == 2 && G.ghalo[o > 0] != nullptr) {  // the neighbouring slab's layer
+            ph[o + 1] = G.ghalo[o > 0][(size_t)i + (size_t)G.n[0] * j];
           } else if (G.bc[a][0][0] == 0) {
             nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
             ph[o + 1] = A.gphi[cidx(G, nb[0], nb[1], nb[2])];

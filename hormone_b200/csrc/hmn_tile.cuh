@@ -514,14 +514,15 @@ __device__ __forceinline__ void sph_div_weights(const GridDev& G, int i, int j, 
 // (i,j,k) along axis a, with the ghost images the boundary pass of the
 // hyperbolic solver forms: a periodic copy; on spherical grids copies at the
 // inner radius and the poles and phi ~ 1/r beyond the outer radius
-// (gravity_hyperbolic.f90:186-207, gbtype 1); on Cartesian grids the Robin
-// image phi ~ 1/r about the origin.
+// (gravity_hyperbolic.f90:186-207, gbtype 1); on Cartesian grids the
+// neighbouring z slab's layer or the Robin image phi ~ 1/r about the origin.
 template <bool SPH>
 __device__ __forceinline__ double gphi_at(const GridDev& G, const double* gphi, size_t c, int i, int j, int k,
                                           int a, int o) {
   int nb[3] = {i, j, k};
   nb[a] += o;
   if (nb[a] >= 0 && nb[a] < G.n[a]) return gphi[cidx(G, nb[0], nb[1], nb[2])];
+  if (!SPH && a == 2 && G.ghalo[o > 0] != nullptr) return G.ghalo[o > 0][(size_t)i + (size_t)G.n[0] * j];
   if (G.bc[a][0][0] == 0) {
     nb[a] = nb[a] < 0 ? G.n[a] - 1 : 0;
     return gphi[cidx(G, nb[0], nb[1], nb[2])];

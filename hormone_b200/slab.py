@@ -97,11 +97,12 @@ class SlabSimulation:
     phases that the exchange interleaves."""
 
     def __init__(self, cfg: dict, prims_global: Dict[str, np.ndarray], k0: int, k1: int, precision: int = 0,
-                 halo_alloc=None, local: bool = False, mode: str = "copy"):
+                 halo_alloc=None, local: bool = False, mode: str = "copy", grvphi=None, grvpsi=None,
+                 cgrav_old: float = 0.0):
         """prims_global: the global primitives (sliced here), or with
-        local=True the slab's own primitives.  mode "copy" allocates send and
-        receive halo buffers, "push" two receive buffers per face (one per
-        stage parity)."""
+        local=True the slab's own primitives (grvphi/grvpsi likewise, for
+        self-gravity).  mode "copy" allocates send and receive halo buffers,
+        "push" two receive buffers per face (one per stage parity)."""
         import torch
 
         self.cfg_global = cfg
@@ -112,9 +113,11 @@ class SlabSimulation:
             local = prims_global
         else:
             local = {k: (v[..., k0:k1, :, :] if k == "spc" else v[k0:k1]) for k, v in prims_global.items()}
+            grvphi = None if grvphi is None else np.ascontiguousarray(grvphi[k0:k1])
+            grvpsi = None if grvpsi is None else np.ascontiguousarray(grvpsi[k0:k1])
         st = ic.to_state(self.cfg, local)
         self.ctx = capi.SlabContext(self.cfg, self.grid, precision=precision)
-        self.ctx.upload(u=st["u"], prim=list(st["prim"]))
+        self.ctx.upload(u=st["u"], prim=list(st["prim"]), grvphi=grvphi, grvpsi=grvpsi)
         self.nspc = int(self.cfg.get("nspc", 0))
         if self.nspc:
             self.ctx.upload_scalars(st["spc"])
@@ -126,6 +129,11 @@ class SlabSimulation:
             self.recv = {(side, q): alloc(n) for side in ("lo", "hi") for q in (0, 1)}
         else:
             self.send_lo, self.send_hi, self.recv_lo, self.recv_hi = (alloc(n) for _ in range(4))
+        self.gravity = cfg["gravswitch"] == 3
+        if self.gravity:  # one layer of the potential per face
+            self.ctx.set_gravity_clock(0.0, cgrav_old)
+            m = self.ctx.gravity_halo_bytes() // 8
+            self.gsend_lo, self.gsend_hi, self.grecv_lo, self.grecv_hi = (alloc(m) for _ in range(4))
         self.time, self.tn = 0.0, 0
         self.t_out, self.t_end = cfg["t_out"], cfg["t_end"]
         self.dt = self.ch = 0.0
@@ -140,6 +148,9 @@ class SlabSimulation:
         p = lambda t: t.data_ptr()  # noqa: E731
         self.ctx.set_slab(p(self.send_lo) if has_lo else 0, p(self.send_hi) if has_hi else 0,
                           p(self.recv_lo) if has_lo else 0, p(self.recv_hi) if has_hi else 0, wrap_lo, wrap_hi)
+        if self.gravity:
+            self.ctx.set_slab_gravity(p(self.gsend_lo) if has_lo else 0, p(self.gsend_hi) if has_hi else 0,
+                                      p(self.grecv_lo) if has_lo else 0, p(self.grecv_hi) if has_hi else 0)
 
     def connect_push(self, has_lo: bool, has_hi: bool, push_lo, push_hi, wrap_lo: bool = False,
                      wrap_hi: bool = False):
@@ -177,7 +188,7 @@ class SlabSimulation:
         return False
 
     def state(self) -> Dict[str, np.ndarray]:
-        out = self.ctx.download()
+        out = self.ctx.download(gravity=self.gravity)
         if self.nspc:
             out["spc"] = self.ctx.download_scalars()
         return out
@@ -191,12 +202,14 @@ class LocalExchange:
     device copies, the CFL partials by an in-process min/max."""
 
     def __init__(self, cfg: dict, prims: Dict[str, np.ndarray], world: int, precision: int = 0,
-                 mode: str = "copy"):
+                 mode: str = "copy", grvphi=None, grvpsi=None, cgrav_old: float = 0.0):
         self.periodic = int(cfg["bc"][2][0][0]) == 0
         self.mode = mode
         self.parts = partition(cfg["n"][2], world)
-        self.ranks = [SlabSimulation(cfg, prims, k0, k1, precision, mode=mode) for k0, k1 in self.parts]
+        self.ranks = [SlabSimulation(cfg, prims, k0, k1, precision, mode=mode, grvphi=grvphi, grvpsi=grvpsi,
+                                     cgrav_old=cgrav_old) for k0, k1 in self.parts]
         self.nb = [neighbours(r, world, self.periodic) for r in range(world)]
+        self.gravity = self.ranks[0].gravity
         if mode == "push":
             links = push_links(world, self.periodic)
             for r, s in enumerate(self.ranks):
@@ -215,6 +228,25 @@ class LocalExchange:
         for r, s in enumerate(self.ranks):
             lo, hi = self.nb[r]
             s.connect(lo is not None, hi is not None, wrap_lo=r == 0, wrap_hi=r == world - 1)
+        if self.gravity:  # the grid's dtg_unit: the minimum over the slabs
+            unit = min(s.ctx.gravity_unit() for s in self.ranks)
+            for s in self.ranks:
+                s.ctx.set_gravity_unit(unit)
+
+    def _exchange_gravity(self):
+        """The potential's boundary layers to the neighbours' halos."""
+        import torch
+
+        for s in self.ranks:
+            s.ctx.pack_gravity_halos()
+        self._sync()
+        for r, s in enumerate(self.ranks):
+            lo, hi = self.nb[r]
+            if lo is not None:
+                s.grecv_lo.copy_(self.ranks[lo].gsend_hi)
+            if hi is not None:
+                s.grecv_hi.copy_(self.ranks[hi].gsend_lo)
+        torch.cuda.synchronize()
 
     def _sync(self):
         import torch
@@ -237,6 +269,14 @@ class LocalExchange:
         torch.cuda.synchronize()
         for s in self.ranks:
             s.cfl_finalize()
+        if self.gravity:  # gravity.f90 sub-stages, each after an exchange of the potential
+            nsub = {s.ctx.gravity_begin(s.time, s.dt, s.tn) for s in self.ranks}
+            assert len(nsub) == 1, nsub
+            for _ in range(nsub.pop()):
+                self._exchange_gravity()
+                for s in self.ranks:
+                    s.ctx.gravity_substage()
+            self._exchange_gravity()  # the force of the hydro stages
         for stage in range(1, self.cfg_rk() + 1):
             if self.mode == "push":  # the previous stage of every slab has stored its layers
                 self._sync()
@@ -303,6 +343,21 @@ class TorchExchange:
     def cfl(self, tmin, tmax):
         self.dist.all_reduce(tmin, op=self.dist.ReduceOp.MIN)
         self.dist.all_reduce(tmax, op=self.dist.ReduceOp.MAX)
+
+    def min_scalar(self, v: float) -> float:
+        """The minimum of a host double over the ranks."""
+        import torch
+
+        dev = "cuda" if self.dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN)
+        return float(t.item())
+
+
+def share_gravity_unit(sim: "SlabSimulation", ex: TorchExchange):
+    """Every rank's dtg_unit becomes the grid's (the minimum over slabs)."""
+    if sim.gravity:
+        sim.ctx.set_gravity_unit(ex.min_scalar(sim.ctx.gravity_unit()))
 
 
 class SymmetricHalos:
@@ -376,6 +431,13 @@ def run_distributed_step(sim: SlabSimulation, ex: TorchExchange) -> bool:
         sim.cfl_local()
         ex.cfl(sim.cfl_min, sim.cfl_max)
         sim.cfl_finalize()
+        if sim.gravity:  # share_gravity_unit ran once before the first step
+            for _ in range(sim.ctx.gravity_begin(sim.time, sim.dt, sim.tn)):
+                sim.ctx.pack_gravity_halos()
+                ex.halos(sim.gsend_lo, sim.gsend_hi, sim.grecv_lo, sim.grecv_hi)
+                sim.ctx.gravity_substage()
+            sim.ctx.pack_gravity_halos()
+            ex.halos(sim.gsend_lo, sim.gsend_hi, sim.grecv_lo, sim.grecv_hi)
         for stage in range(1, int(sim.cfg["rktype"]) + 1):
             sim.ctx.pack_halos()
             ex.halos(sim.send_lo, sim.send_hi, sim.recv_lo, sim.recv_hi)

@@ -114,8 +114,20 @@ int hmn_timestep(hmn_ctx* ctx, double time, double t_out, double t_end, double* 
 
 /* gravity (src/main/gravity.f90:18-64 -> gravity_hyperbolic.f90:19-50):
  * the hyperbolic sub-cycles from grvtime to time+dt; tn is the step index
- * (tn == 0 only sets the boundary images, grav_init_other). */
+ * (tn == 0 only sets the boundary images, grav_init_other).  Refused
+ * (HMN_EBADCFG) on a slab with gravity halos, which runs the sub-stages one
+ * by one (below). */
 int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn);
+
+/* The same split into its sub-stages (for slabs, which exchange the
+ * potential between them): hmn_gravity_begin plans the sub-cycles of
+ * [time, time+dt] from the last dt/cgrav/dtgrav and writes *nsub =
+ * tngrav x grktype (gravity_hyperbolic.f90:33-38; 0 at tn == 0, where only
+ * the clock is set); hmn_gravity_substage runs the next RK sub-stage
+ * (hyperbolic_gravity_step, gravity_hyperbolic.f90:62-110) and advances the
+ * gravity clock after the last sub-stage of a cycle. */
+int hmn_gravity_begin(hmn_ctx* ctx, double time, double dt, int tn, int* nsub);
+int hmn_gravity_substage(hmn_ctx* ctx);
 
 /* hydro_step (src/main/hydro.f90:15-52): rktype fused RK stages (boundary
  * images, slopes, HLLD fluxes, source, update, primitive check) with the dt
@@ -208,10 +220,30 @@ int hmn_checkpoint_wait(hmn_ctx* ctx);
  *   for each RK stage s: hmn_pack_halos; exchange; hmn_hydro_stage(s);
  *   hmn_phidamp.
  * hmn_timestep, hmn_hydro_step and hmn_run refuse a context with
- * neighbours (HMN_EBADCFG); gravity is not decomposed. */
+ * neighbours (HMN_EBADCFG). */
 size_t hmn_slab_halo_bytes(const hmn_ctx* ctx);
 int hmn_set_slab(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo, const double* recv_hi,
                  int wrap_lo, int wrap_hi);
+
+/* Slabs of a 3-D Cartesian grid with hyperbolic self-gravity (gravswitch 3)
+ * also exchange one layer of the potential: after hmn_set_slab, hand the
+ * context four more buffers of hmn_slab_gravity_halo_bytes (NULL on the
+ * same physical faces).  hmn_pack_gravity_halos copies the potential's
+ * lowest / highest layer into send_lo / send_hi; recv_lo / recv_hi must hold
+ * the lower / upper neighbour's send_hi / send_lo.  dtg_unit (the minimum
+ * over all cells, tools.f90:160-183) must be the grid's: set every slab's to
+ * the minimum of hmn_gravity_unit over the slabs.  A step is then
+ *   hmn_cfl_local; all-reduce; hmn_cfl_finalize;
+ *   hmn_gravity_begin(.., &nsub); nsub x { hmn_pack_gravity_halos;
+ *   exchange; hmn_gravity_substage }; hmn_pack_gravity_halos; exchange;
+ *   for each RK stage s: hmn_pack_halos; exchange; hmn_hydro_stage(s).
+ * hmn_hydro_stage and hmn_gravity_begin refuse a gravity slab without them. */
+size_t hmn_slab_gravity_halo_bytes(const hmn_ctx* ctx);
+int hmn_set_slab_gravity(hmn_ctx* ctx, double* send_lo, double* send_hi, const double* recv_lo,
+                         const double* recv_hi);
+int hmn_pack_gravity_halos(hmn_ctx* ctx);
+int hmn_gravity_unit(hmn_ctx* ctx, double* dtg_unit);
+int hmn_set_gravity_unit(hmn_ctx* ctx, double dtg_unit);
 
 /* The push exchange (instead of hmn_set_slab): recv_lo/recv_hi are this
  * slab's halo buffers (hmn_slab_halo_bytes each) for stage parity 0 and 1,

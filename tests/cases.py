@@ -95,6 +95,19 @@ def polytrope(n=16):
     return cfg, prims, phi
 
 
+def polytrope_stretched(n=16, x3min=0.18):
+    """The polytrope on a z mesh of geometrically growing widths
+    (kmesh=1, utils.f90:351-404)."""
+    ov = dict(ie=n, je=n, ke=n, mag_on=False, gamma=2.0, gravswitch=3, G=1.0, courant=0.9, kmesh=1, x3min=x3min,
+              xi1s=-2.0, xi1e=2.0, xi2s=-2.0, xi2e=2.0, xi3s=-2.0, xi3e=2.0, t_end=1.0, dt_out=1.0)
+    for a in (1, 2, 3):
+        for tag in ("is", "os", "iv", "ov"):
+            ov[f"bc{a}{tag}"] = 3
+    cfg = config.resolve("polytrope_cart", overrides=ov)
+    prims, phi = ic.polytrope_n1(cfg, G.make_grid(cfg))
+    return cfg, prims, phi
+
+
 def cell_volumes(cfg, grid):
     """dvol of metric.f90 (norm weights of tests.f90)."""
     if cfg.get("crdnt", 0) == 2:

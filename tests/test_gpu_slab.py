@@ -3,7 +3,8 @@ own context, exchanging halos by device copies (hormone_b200.slab.
 LocalExchange), give bit for bit the undecomposed run's state and dt,
 periodic or not, with scalars, and in the mixed-precision form; so do
 slabs whose stage kernels push their boundary layers into the neighbours'
-halo buffers (mode "push")."""
+halo buffers (mode "push"), and slabs with hyperbolic self-gravity, which
+also exchange the potential's boundary layers."""
 import numpy as np
 import pytest
 
@@ -15,15 +16,16 @@ import cases
 pytestmark = pytest.mark.gpu
 
 
-def run_both(cfg, prims, world, steps, precision=0, mode="copy"):
-    ref = Simulation(cfg, prims, precision=precision)
-    dec = slab.LocalExchange(cfg, prims, world, precision=precision, mode=mode)
+def run_both(cfg, prims, world, steps, precision=0, mode="copy", grvphi=None):
+    gravity = cfg["gravswitch"] == 3
+    ref = Simulation(cfg, prims, precision=precision, grvphi=grvphi)
+    dec = slab.LocalExchange(cfg, prims, world, precision=precision, mode=mode, grvphi=grvphi)
     for n in range(steps):
         ref.step()
         dec.step()
         for s in dec.ranks:
             assert s.dt == ref.dt, (n, s.dt, ref.dt)
-    a, b = ref.state(), dec.state()
+    a, b = ref.state(gravity=gravity), dec.state()
     ref.close()
     dec.close()
     for k in a:
@@ -64,6 +66,32 @@ def test_riemann_with_scalars():
 def test_mixed_precision_slabs():
     cfg, prims = cases.ot3d(16)
     run_both(cfg, prims, 2, 4, precision=1)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_polytrope_self_gravity_slabs(world):
+    """Hyperbolic self-gravity on slabs: the potential's boundary layer is
+    exchanged before every sub-stage of the sub-cycles and once more for
+    the force of the hydro stages; the potential, psi and the state match
+    the undecomposed run bit for bit."""
+    cfg, prims, phi = cases.polytrope(16)
+    run_both(cfg, prims, world, 4, grvphi=phi)
+
+
+def test_self_gravity_slabs_stretched_z():
+    """A z mesh of growing widths: each slab's own dtg_unit differs, the
+    grid's is the minimum over the slabs."""
+    cfg, prims, phi = cases.polytrope_stretched(16)
+    dec = slab.LocalExchange(cfg, prims, 2, grvphi=phi)
+    units = [s.ctx.gravity_unit() for s in dec.ranks]
+    dec.close()
+    assert units[0] == units[1]
+    run_both(cfg, prims, 2, 4, grvphi=phi)
+
+
+def test_self_gravity_slabs_mixed_precision():
+    cfg, prims, phi = cases.polytrope(16)
+    run_both(cfg, prims, 2, 3, precision=1, grvphi=phi)
 
 
 @pytest.mark.parametrize("world", [1, 2, 3])

@@ -76,7 +76,8 @@ def _worker(rank, world, port, periodic, q):
         tmin = torch.tensor([10.0 + rank], dtype=torch.float64)
         tmax = torch.tensor([10.0 + rank], dtype=torch.float64)
         ex.cfl(tmin, tmax)
-        q.put((rank, float(recv_lo[0]), float(recv_hi[0]), float(tmin), float(tmax), ex.lo, ex.hi))
+        unit = ex.min_scalar(0.5 + 0.25 * ((rank + 1) % world))  # the gravity unit's minimum over slabs
+        q.put((rank, float(recv_lo[0]), float(recv_hi[0]), float(tmin), float(tmax), ex.lo, ex.hi, unit))
     finally:
         dist.destroy_process_group()
 
@@ -93,7 +94,8 @@ def test_gloo_halo_exchange_pairs_faces(world, periodic):
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, rlo, rhi, tmin, tmax, lo, hi in res:
+    for rank, rlo, rhi, tmin, tmax, lo, hi, unit in res:
+        assert unit == 0.5
         # the low halo holds the lower neighbour's highest layers, the high
         # halo the upper neighbour's lowest layers; physical faces are untouched
         assert rlo == (100.0 * lo + 2.0 if lo is not None else -1.0)
