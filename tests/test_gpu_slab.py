@@ -148,19 +148,7 @@ def test_distributed_step_on_one_rank_over_nccl():
     """The torch.distributed driver (NCCL all-reduce of the CFL partials
     viewed in place, collectives ordered on the slab's stream) on a
     one-rank group: the same bits as the undecomposed run."""
-    import datetime
-    import os
-    import socket
-
-    import torch.distributed as dist
-
-    sock = socket.socket()
-    sock.bind(("127.0.0.1", 0))
-    port = sock.getsockname()[1]
-    sock.close()
-    os.environ["MASTER_ADDR"] = "127.0.0.1"
-    os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    dist = _one_rank_nccl()
     try:
         cfg, prims = cases.blast3d(14, bc=2, mag=True)
         ref = Simulation(cfg, prims)
@@ -170,6 +158,77 @@ def test_distributed_step_on_one_rank_over_nccl():
         for _ in range(4):
             ref.step()
             slab.run_distributed_step(sim, ex)
+            assert sim.dt == ref.dt
+        a, b = ref.state(), sim.state()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        ref.close()
+        sim.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def _one_rank_nccl():
+    import datetime
+    import os
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    return dist
+
+
+def test_distributed_gravity_step_on_one_rank_over_nccl():
+    """The distributed driver with self-gravity (the grid's dtg_unit shared
+    by an all-reduce, the potential exchanged between sub-stages) on a
+    one-rank group: the undecomposed run's bits."""
+    dist = _one_rank_nccl()
+    try:
+        cfg, prims, phi = cases.polytrope(16)
+        ref = Simulation(cfg, prims, grvphi=phi)
+        sim = slab.SlabSimulation(cfg, prims, 0, cfg["n"][2], grvphi=phi)
+        ex = slab.TorchExchange(dist, 0, 1, periodic=False)
+        sim.connect(False, False)
+        slab.share_gravity_unit(sim, ex)
+        for _ in range(4):
+            ref.step()
+            slab.run_distributed_step(sim, ex)
+            assert sim.dt == ref.dt
+        a, b = ref.state(gravity=True), sim.state()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+        ref.close()
+        sim.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_symmetric_push_step_on_one_rank():
+    """The push exchange's symmetric-memory buffers and step driver on a
+    one-rank group (a periodic grid in one slab wraps onto itself, so no
+    peer stores happen; several ranks need several GPUs)."""
+    dist = _one_rank_nccl()
+    try:
+        cfg, prims = cases.ot3d(16)
+        ref = Simulation(cfg, prims)
+        sim = slab.SlabSimulation(cfg, prims, 0, cfg["n"][2], mode="push")
+        halos = slab.SymmetricHalos(sim.halo_n)
+        assert halos.peer(0, "hi", 1) == halos.local("hi", 1).data_ptr()
+        slab.connect_symmetric(sim, halos, 0, 1, periodic=True)
+        ex = slab.TorchExchange(dist, 0, 1, periodic=True)
+        for _ in range(4):
+            ref.step()
+            slab.run_distributed_push_step(sim, ex)
             assert sim.dt == ref.dt
         a, b = ref.state(), sim.state()
         for k in a:
