@@ -83,6 +83,7 @@ def lib():
         L.hmn_launch_count.argtypes = [_P]
         L.hmn_launch_count.restype = ctypes.c_longlong
         L.hmn_sync.argtypes = [_P]
+        L.hmn_evo.argtypes = [_P, _DP]
         L.hmn_destroy.argtypes = [_P]
         L.hmn_set_gravity_clock.argtypes = [_P, _D, _D]
         L.hmn_gravity_clock.argtypes = [_P, _DP, _DP]
@@ -101,7 +102,7 @@ def lib():
                      "hmn_download", "hmn_download_pressure", "hmn_run", "hmn_last_error", "hmn_sync", "hmn_destroy",
                      "hmn_set_gravity_clock", "hmn_gravity_clock", "hmn_checkpoint_begin", "hmn_checkpoint_wait",
                      "hmn_upload_scalars", "hmn_download_scalars", "hmn_set_dirichlet", "hmn_set_metric",
-                     "hmn_set_flux_boundary"):
+                     "hmn_set_flux_boundary", "hmn_evo"):
             getattr(L, name).restype = _I
         _lib = L
     return _lib
@@ -341,6 +342,14 @@ class Context:
 
     def sync(self):
         self._check(lib().hmn_sync(self.h), "hmn_sync")
+
+    EVO = ("Mtot", "Etot", "Eitot", "Ektot", "Egtot", "Mbound", "Ebound", "Jbound", "Ebtot", "Jtot")
+
+    def evo(self) -> Dict[str, float]:
+        """hmn_evo: the ten totals of evo_output (output.f90:147-275), by name."""
+        out = (_D * 10)()
+        self._check(lib().hmn_evo(self.h, out), "hmn_evo")
+        return dict(zip(self.EVO, list(out)))
 
     def launches(self) -> int:
         return int(lib().hmn_launch_count(self.h))

@@ -77,6 +77,8 @@ struct hmn_ctx {
   double run_phifac;
   long long run_launches;    // kernel launches one replay makes
   double* sphbuf;            // spherical metric factors (SphGeo arrays)
+  double* sincbuf;           // spherical: sin of the theta centres (device, from js-2), or nullptr
+  double* evobuf;            // evo_output partials and totals (device)
   // asynchronous checkpoint: device snapshot -> pinned staging on a copy stream
   cudaStream_t cst;
   cudaEvent_t ck_snap, ck_done;
@@ -471,6 +473,8 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   if (ctx->run_exec) cudaGraphExecDestroy(ctx->run_exec);
   cudaFree(ctx->geo);
   cudaFree(ctx->sphbuf);
+  cudaFree(ctx->sincbuf);
+  cudaFree(ctx->evobuf);
   cudaFree(ctx->hgc);
   cudaFree(ctx->gin);
   free(ctx->xi1_h);
@@ -647,6 +651,14 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
   M.fac_k = ctx->n[2] == 1 ? 4.0 : 1.0;
   M.crd = 2;
   M.on = 1;
+  cudaFree(ctx->sincbuf);  // the angular-momentum weights of hmn_evo
+  ctx->sincbuf = nullptr;
+  if (mt->sinc) {
+    CK(cudaMalloc((void**)&ctx->sincbuf, (size_t)L2 * sizeof(double)), "cudaMalloc");
+    CK(cudaMemcpyAsync(ctx->sincbuf, mt->sinc, (size_t)L2 * sizeof(double), cudaMemcpyHostToDevice, ctx->st),
+       "metric");
+    CK(cudaStreamSynchronize(ctx->st), "metric");
+  }
   ctx->xi1s = xi[1];  // xi1(is-1)
   if (grav) {
     // the Laplacian's 8 planes per cell: c0, the -x/+x/-y/+y/-z/+z weights, the normalisation
@@ -1197,6 +1209,29 @@ extern "C" int hmn_gravity_step(hmn_ctx* ctx, double time, double dt, int tn) {
     if (rc) return rc;
   }
   return sph_gravity_boundary(ctx);
+}
+
+// evo_output (output.f90:147-275): the grid's totals of the current state,
+// summed per block and then over blocks in a fixed order.
+extern "C" int hmn_evo(hmn_ctx* ctx, double out[10]) {
+  if (!ctx || !out) return HMN_EINVAL;
+  const int nb = blocks_for(ctx);
+  if (!ctx->evobuf)
+    CK(cudaMalloc((void**)&ctx->evobuf, ((size_t)ctx->nsm * 8 + 1) * kEvoQ * sizeof(double)), "cudaMalloc");
+  double* tot = ctx->evobuf + (size_t)nb * kEvoQ;
+  const double* gphi = ctx->par.gravswitch == 3 ? ctx->gphi[ctx->gcur] : nullptr;
+  CK(launch_evo(ctx->G, ctx->pbuf[ctx->pcur], ctx->plane, gphi, ctx->G.sph.crd == 2 ? ctx->sincbuf : nullptr,
+                ctx->evobuf, nb, tot, ctx->st),
+     "evo");
+  ctx->launches += 2;
+  double h[kEvoQ];
+  CK(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, ctx->st), "evo");
+  CK(cudaStreamSynchronize(ctx->st), "evo");
+  // Mtot, Etot, Eitot, Ektot = 0.5 sum, Egtot, Mbound, Ebound, Jbound, Ebtot = 0.5 sum, Jtot
+  for (int q = 0; q < kEvoQ; q++) out[q] = h[q];
+  out[3] = 0.5 * h[3];
+  out[8] = 0.5 * h[8];
+  return HMN_OK;
 }
 
 extern "C" int hmn_set_gravity_clock(hmn_ctx* ctx, double grvtime, double cgrav_old) {

@@ -193,6 +193,10 @@ cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double
 cudaError_t launch_hg_stage(const GridDev& G, const HGArgs& A, int nblocks, cudaStream_t st);
 cudaError_t launch_hg_stage_sph(const GridDev& G, const HGArgs& A, cudaStream_t st);
 cudaError_t launch_advance(DevScalars* sc, cudaStream_t st);
+// evo_output totals: nblocks x kEvoQ partials in part, the kEvoQ sums in out
+constexpr int kEvoQ = 10;
+cudaError_t launch_evo(const GridDev& G, const double* P, size_t plane, const double* gphi, const double* sinc,
+                       double* part, int nblocks, double* out, cudaStream_t st);
 // batched launchers over a work list of (sim, tile) items; tile_kind selects
 // the compile-time tile (see batch_tile_kind), grid = persistent CTAs
 int batch_tile_kind(const int solve[3]);

@@ -862,6 +862,81 @@ cudaError_t launch_prim_out(const double* P, size_t plane, double phifac, double
   return cudaGetLastError();
 }
 
+// evo_output (output.f90:147-275): each block adds its cells' contributions
+// to the ten totals (mass, total, internal and twice the kinetic energy,
+// gravitational energy, bound mass, energy and angular momentum, twice the
+// magnetic energy, angular momentum); evo_final_kernel adds the blocks'
+// partials in block order, so the result does not depend on scheduling.
+// dvol follows metric.f90 as the CFL reduction forms it.
+constexpr int kEvoThreads = 256;
+
+__global__ void __launch_bounds__(kEvoThreads) evo_kernel(const GridDev G, const double* P, size_t plane,
+                                                         const double* gphi, const double* sinc, double* part) {
+  __shared__ double red[kEvoQ][kEvoThreads];
+  double acc[kEvoQ];
+#pragma unroll
+  for (int q = 0; q < kEvoQ; q++) acc[q] = 0.0;
+  const int n0 = G.n[0], n1 = G.n[1];
+  const SphGeo& M = G.sph;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < plane; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % n0), j = (int)((c / n0) % n1), k = (int)(c / ((size_t)n0 * n1));
+    const double dxi1 = G.g[0].dxi[i + 2], dxi2 = G.g[1].dxi[j + 2], dxi3 = G.g[2].dxi[k + 2];
+    double dvol;
+    if (M.on && M.crd == 1)
+      dvol = 0.5 * M.ar2[i + 2] * dxi2 * dxi3 * M.fac_j;
+    else if (M.on)
+      dvol = M.vr[i + 2] * M.cd[j + 2] * dxi3 * M.fac_j * M.fac_k;
+    else
+      dvol = dxi1 * dxi2 * dxi3;
+    const double d = P[c], v1 = P[PV * plane + c], v2 = P[(PV + 1) * plane + c], v3 = P[(PV + 2) * plane + c];
+    const double e = P[PE * plane + c], eint = P[PEINT * plane + c];
+    const double b1 = P[PB * plane + c], b2 = P[(PB + 1) * plane + c], b3 = P[(PB + 2) * plane + c];
+    acc[0] = acc[0] + d * dvol;
+    acc[1] = acc[1] + e * dvol;
+    acc[2] = acc[2] + eint * dvol;
+    acc[3] = acc[3] + d * (v1 * v1 + v2 * v2 + v3 * v3) * dvol;
+    acc[8] = acc[8] + (b1 * b1 + b2 * b2 + b3 * b3) * dvol;
+    double jl = 0.0;
+    if (M.on && M.crd == 1) jl = d * G.g[0].x[i + 2] * v2 * dvol;
+    if (M.on && M.crd == 2 && sinc) jl = d * G.g[0].x[i + 2] * sinc[j + 2] * v3 * dvol;
+    acc[9] = acc[9] + jl;
+    if (gphi) {  // totphi = grvphi (no external potential on this path)
+      const double ph = gphi[c], tot = ph;
+      acc[4] = acc[4] + d * (tot - 0.5 * ph) * dvol;
+      if (tot + (e - eint) / d <= 0.0) {
+        acc[5] = acc[5] + d * dvol;
+        acc[6] = acc[6] + (e + d * (tot - 0.5 * ph)) * dvol;
+        acc[7] = acc[7] + jl;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kEvoQ; q++) red[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int h = kEvoThreads / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+#pragma unroll
+      for (int q = 0; q < kEvoQ; q++) red[q][threadIdx.x] = red[q][threadIdx.x] + red[q][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x < kEvoQ) part[(size_t)blockIdx.x * kEvoQ + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void evo_final_kernel(const double* part, int nblocks, double* out) {
+  const int q = threadIdx.x;
+  if (q >= kEvoQ) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; b++) s = s + part[(size_t)b * kEvoQ + q];
+  out[q] = s;
+}
+
+cudaError_t launch_evo(const GridDev& G, const double* P, size_t plane, const double* gphi, const double* sinc,
+                       double* part, int nblocks, double* out, cudaStream_t st) {
+  evo_kernel<<<nblocks, kEvoThreads, 0, st>>>(G, P, plane, gphi, sinc, part);
+  evo_final_kernel<<<1, 32, 0, st>>>(part, nblocks, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
   advance_kernel<<<1, 32, 0, st>>>(sc);
   return cudaGetLastError();

@@ -124,6 +124,25 @@ class Simulation:
         self.tn += n
         return self.time >= self.t_end
 
+    def evo(self) -> Dict[str, float]:
+        """One line of evo_output (output.f90:147-275): tn, time and the
+        totals the reference writes for this set-up (gravity entries with
+        self-gravity, Ebtot with fields, Jtot on curvilinear grids of two or
+        more dimensions), doubled with equatorial symmetry."""
+        tot = self.ctx.evo()
+        c = self.cfg
+        keys = ["Mtot", "Etot", "Eitot", "Ektot"]
+        if c["gravswitch"] >= 1:
+            keys += ["Egtot", "Mbound", "Ebound", "Jbound"]
+        if c["mag_on"]:
+            keys.append("Ebtot")
+        if c["dim"] >= 2 and c.get("crdnt", 0) >= 1:
+            keys.append("Jtot")
+        f = 2.0 if c.get("eq_sym", False) else 1.0
+        out = {"tn": self.tn, "time": self.time}
+        out.update({k: f * tot[k] for k in keys})
+        return out
+
     def state(self, gravity: bool = False) -> Dict[str, np.ndarray]:
         out = self.ctx.download(gravity=gravity)
         if self.nspc:

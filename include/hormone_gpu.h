@@ -272,6 +272,14 @@ int hmn_cfl_finalize(hmn_ctx* ctx, double* dt, double* ch);
  * *time and *steps are updated. */
 int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, int* steps);
 
+/* evo_output (src/main/output.f90:147-275): the totals of the current state
+ * over the grid, out[0..9] = Mtot, Etot, Eitot, Ektot, Egtot, Mbound,
+ * Ebound, Jbound, Ebtot, Jtot (the gravity entries with gravswitch 3,
+ * Jbound/Jtot on cylindrical and spherical grids, else 0).  Summed per
+ * block and then over blocks in a fixed order: deterministic, but not the
+ * reference's sequential order.  The eq_sym doubling is the caller's. */
+int hmn_evo(hmn_ctx* ctx, double out[10]);
+
 /* First error recorded by any kernel: code and the cell (0-based). */
 int hmn_last_error(hmn_ctx* ctx, int* code, int* i, int* j, int* k, int* sim);
 
