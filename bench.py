@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--boxes", type=int, default=512)
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--policy", choices=["fifo", "sjf"], default="fifo", help="serve admission order")
+    ap.add_argument("--live-cells", type=int, default=0, help="serve: cap on the admitted cells (0: none)")
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--poly-steps", type=int, default=2000, help="timed steps of the polytrope workload")
     ap.add_argument("--decomp", choices=["replicas", "slab"], default="replicas",
@@ -882,7 +884,8 @@ def run_serve(args, rank=0, world=1, local_rank=0):
     if dist:
         dist.barrier()
     with ClockSampler(local_rank) as clk:
-        stats = serve.serve(reqs, b, chunk=8, keep_results=False)
+        stats = serve.serve(reqs, b, chunk=8, keep_results=False, policy=args.policy,
+                            live_cells=args.live_cells or None)
     b.close()
     if dist:
         allst = [None] * world
@@ -902,7 +905,8 @@ def run_serve(args, rank=0, world=1, local_rank=0):
             "steps": summ["batch_steps"], "warmup": 0, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "mixed", "data": "synthetic",
             "config": {"workload": f"serve-{args.requests}-requests-poisson-{args.rate}/s",
-                       "pool_bytes": int(free * 0.6), "parallelism": f"requests sharded over {world} rank(s)"},
+                       "pool_bytes": int(free * 0.6), "parallelism": f"requests sharded over {world} rank(s)",
+                       "admission": args.policy, "live_cells_cap": args.live_cells or None},
             "serve": summ, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 

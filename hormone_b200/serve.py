@@ -3,8 +3,9 @@
 Requests arrive over time (a seeded Poisson stream in the benchmark).  The
 server admits each arrived request into the running batch as soon as the
 batch's device pool has room for its footprint (first come, first served,
-with smaller requests allowed to pass a head-of-line request that does not
-fit), advances all admitted simulations together a few steps at a time (each
+or shortest estimated work first under a cap on the live cells, with
+smaller requests allowed to pass a head-of-line request that does not fit),
+advances all admitted simulations together a few steps at a time (each
 on its own clock), and retires every simulation that reached its end time:
 its result is copied back, its pool memory is freed for waiting requests.
 Reported: time-to-solution per request (completion minus arrival, wall
@@ -109,11 +110,29 @@ class ServeStats:
                 "max_concurrent": self.max_live, "batch_steps": self.batch_steps}
 
 
+def estimated_work(cfg: dict) -> float:
+    """Zone-updates a request needs, up to a constant: its cells times its
+    steps, which grow with t_end and, through the CFL condition on the
+    finest width, with the cells along its longest axis."""
+    n = [int(v) for v in cfg["n"]]
+    return float(np.prod(n)) * max(n) * float(cfg["t_end"])
+
+
 def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], float] = time.perf_counter,
-          keep_results: bool = True, realtime: bool = True) -> ServeStats:
+          keep_results: bool = True, realtime: bool = True, policy: str = "fifo",
+          live_cells: Optional[int] = None) -> ServeStats:
     """Run the stream through `batch` (a hormone_b200.batch.Batch or any
     object with add/step/poll/download/remove).  With realtime=False arrival
-    times are ignored (every request is available at once)."""
+    times are ignored (every request is available at once).
+
+    policy "fifo" admits arrived requests in arrival order; "sjf" in order of
+    estimated work (shortest first, arrival order among equals).  live_cells
+    caps the cells of the admitted simulations (a request larger than the
+    cap still runs when nothing else does): every batch step advances every
+    live simulation, so a small request admitted beside many large ones
+    waits for as many of their steps as it needs itself."""
+    if policy not in ("fifo", "sjf"):
+        raise ValueError(f"unknown admission policy {policy!r}")
     stats = ServeStats()
     pending = sorted(requests, key=lambda r: r.arrival)
     waiting: List[Request] = []
@@ -125,8 +144,11 @@ def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], fl
         while i < len(pending) and (not realtime or pending[i].arrival <= now):
             waiting.append(pending[i])
             i += 1
-        # admission: FIFO, letting smaller requests pass one that does not fit yet
+        if policy == "sjf":
+            waiting.sort(key=lambda r: estimated_work(r.cfg))  # stable: arrival order among equals
+        # admission in policy order, letting smaller requests pass one that does not fit yet
         still = []
+        live = sum(r.cells for r in running.values())
         for r in waiting:
             cap = getattr(batch, "capacity", None)
             if cap is not None and cap(r.cfg) is False:  # can never fit: fail it instead of waiting forever
@@ -135,12 +157,16 @@ def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], fl
                 stats.failed += 1
                 stats.failures.append((r.rid, r.kind, r.cells, r.error, 0))
                 continue
+            if live_cells is not None and running and live + r.cells > live_cells:
+                still.append(r)
+                continue
             slot = batch.add(r.cfg, r.prims)
             if slot is None:
                 still.append(r)
                 continue
             r.t_admit = clock() - t0
             running[slot] = r
+            live += r.cells
         waiting = still
         stats.max_live = max(stats.max_live, len(running))
         if not running:

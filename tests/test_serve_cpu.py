@@ -78,3 +78,49 @@ def test_request_larger_than_the_pool_fails_instead_of_blocking():
     fake = FakeBatch(pool=1000)
     stats = serve.serve(reqs, fake, chunk=1, realtime=False)
     assert stats.failed == 3 and stats.completed == 0
+
+
+class TimedFake(FakeBatch):
+    """A batch whose step costs time in proportion to the live cells (every
+    step advances every live simulation), on a clock of its own."""
+
+    def __init__(self, pool):
+        super().__init__(pool)
+        self.t = 0.0
+        self.peak_cells = 0
+
+    def add(self, cfg, prims):
+        s = super().add(cfg, prims)
+        if s is not None and len(self.sims) > 1:
+            self.peak_cells = max(self.peak_cells, self.used)
+        return s
+
+    def step(self, n):
+        self.t += n * self.used * 1e-6
+        super().step(n)
+
+
+def test_shortest_first_under_a_cell_cap_cuts_the_median_latency():
+    """Admitting by estimated work under a cap on the live cells finishes the
+    small requests before the large ones run: the median time-to-solution
+    falls, every request still completes with the same steps, and the cap
+    holds whenever more than one simulation is live."""
+    res = {}
+    for policy, cap in (("fifo", None), ("sjf", 3000)):
+        reqs = serve.make_requests(40, rate=1e9, seed=4, max_cells=4096, min_cells=64)
+        fake = TimedFake(pool=10 ** 6)
+        stats = serve.serve(reqs, fake, chunk=2, realtime=False, clock=lambda: fake.t, policy=policy,
+                            live_cells=cap)
+        assert stats.completed == 40 and stats.failed == 0
+        assert all(r.steps == -(-r.cells // 100) for r in reqs)
+        if cap is not None:
+            assert fake.peak_cells <= cap
+        res[policy] = stats.summary()
+    assert res["sjf"]["p50_s"] < 0.5 * res["fifo"]["p50_s"], res
+
+
+def test_unknown_policy_is_refused():
+    import pytest
+
+    with pytest.raises(ValueError):
+        serve.serve([], FakeBatch(pool=10), policy="lifo")
