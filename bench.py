@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--boxes", type=int, default=512)
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=50.0)
-    ap.add_argument("--policy", choices=["fifo", "sjf"], default="fifo", help="serve admission order")
+    ap.add_argument("--policy", choices=["fifo", "sjf", "priority"], default="priority",
+                    help="serve admission and stepping order")
     ap.add_argument("--live-cells", type=int, default=0, help="serve: cap on the admitted cells (0: none)")
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--poly-steps", type=int, default=2000, help="timed steps of the polytrope workload")

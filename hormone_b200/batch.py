@@ -27,6 +27,7 @@ def _bind(L):
                                 capi._DPP, _D, _D, ctypes.POINTER(_I)]
     L.hmn_batch_remove.argtypes = [_P, _I]
     L.hmn_batch_step.argtypes = [_P, _I]
+    L.hmn_batch_set_held.argtypes = [_P, ctypes.POINTER(_I)]
     L.hmn_batch_poll.argtypes = [_P, capi._DP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]
     L.hmn_batch_download.argtypes = [_P, _I, capi._DP, capi._DPP]
     L.hmn_batch_set_schedule.argtypes = [_P, _I, _I, _I]
@@ -37,7 +38,8 @@ def _bind(L):
     L.hmn_batch_stream.restype = _P
     L.hmn_batch_destroy.argtypes = [_P]
     for n in ("hmn_batch_create", "hmn_batch_add", "hmn_batch_remove", "hmn_batch_step", "hmn_batch_poll",
-              "hmn_batch_download", "hmn_batch_set_schedule", "hmn_batch_sync", "hmn_batch_destroy"):
+              "hmn_batch_download", "hmn_batch_set_schedule", "hmn_batch_sync", "hmn_batch_destroy",
+              "hmn_batch_set_held"):
         getattr(L, n).restype = _I
     L._hmn_batch_bound = True
     return L
@@ -117,6 +119,16 @@ class Batch:
         rc = capi.lib().hmn_batch_step(self.h, int(nsteps))
         if rc != 0:
             raise capi.HmnError(rc, "hmn_batch_step")
+
+    def set_held(self, slots):
+        """Leave the simulations in `slots` out of the following steps (and
+        release every other one)."""
+        held = np.zeros(self.max_sims, dtype=np.int32)
+        for s in slots:
+            held[int(s)] = 1
+        rc = capi.lib().hmn_batch_set_held(self.h, held.ctypes.data_as(ctypes.POINTER(_I)))
+        if rc != 0:
+            raise capi.HmnError(rc, "hmn_batch_set_held")
 
     def poll(self):
         n = self.max_sims

@@ -371,6 +371,28 @@ static int pull(hmn_batch* b) {
   return HMN_OK;
 }
 
+// Hold (held[s] = 1) or release simulations: a held simulation is left out
+// of every step (its clock, state and CFL partials stay as they are) until
+// it is released, so a scheduler can advance some simulations alone.
+extern "C" int hmn_batch_set_held(hmn_batch* b, const int* held) {
+  if (!b || !held) return HMN_EINVAL;
+  int rc = pull(b);
+  if (rc) return rc;
+  bool changed = false;
+  for (int s = 0; s < b->max_sims; s++) {
+    const int h = b->slots[s].used && held[s] ? 1 : 0;
+    if (b->h_sims[s].held != h) changed = true;
+    b->h_sims[s].held = h;
+  }
+  if (!changed) return HMN_OK;
+  BCK(cudaMemcpyAsync(b->d_sims, b->h_sims.data(), (size_t)b->max_sims * sizeof(SimDesc), cudaMemcpyHostToDevice,
+                      b->st),
+      "descriptor");
+  BCK(cudaStreamSynchronize(b->st), "sync");
+  b->dirty = true;
+  return HMN_OK;
+}
+
 static int rebuild(hmn_batch* b) {
   // work list: active, unfinished simulations grouped by (tile kind, mag, glm)
   std::vector<int2> items;
@@ -381,7 +403,9 @@ static int rebuild(hmn_batch* b) {
       Klass k{kind, mag, glm, (int)items.size(), 0, 0};
       for (int s = 0; s < b->max_sims; s++) {
         const SlotInfo& si = b->slots[s];
-        if (!si.used || si.kind != kind || si.mag != mag || si.glm != glm || b->h_sims[s].sc.done) continue;
+        if (!si.used || si.kind != kind || si.mag != mag || si.glm != glm || b->h_sims[s].sc.done ||
+            b->h_sims[s].held)
+          continue;
         for (int t = 0; t < si.ntiles; t++) items.push_back(make_int2(s, t));
       }
       k.count = (int)items.size() - k.first;

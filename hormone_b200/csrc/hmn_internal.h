@@ -157,6 +157,7 @@ struct SimDesc {
   int pcur;           // P buffer of the current state
   int nvar, limiter, rktype, glm;
   int active;         // 0 for a free slot
+  int held;           // 1: left out of the steps until released (hmn_batch_set_held)
   double gamma, gm1;
   double damp;        // phidamp factor exp(-alpha9wave*courant)
   double phifac;      // pending phidamp factor for the next stage 1

@@ -1034,7 +1034,7 @@ __global__ void __launch_bounds__(TL::NT) batch_cfl_kernel(SimDesc* sims, const 
 
 __global__ void batch_finalize_kernel(SimDesc* sims, int nsims) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsims || !sims[s].active || sims[s].sc.done) return;
+  if (s >= nsims || !sims[s].active || sims[s].sc.done || sims[s].held) return;
   finalize_dt(&sims[s].sc);
 }
 
@@ -1044,7 +1044,7 @@ __global__ void batch_advance_kernel(SimDesc* sims, int nsims) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsims) return;
   SimDesc& S = sims[s];
-  if (!S.active || S.sc.done) return;
+  if (!S.active || S.sc.done || S.held) return;
   S.sc.time = S.sc.time + S.sc.dt;
   S.sc.tn = S.sc.tn + 1;
   S.pcur = (S.pcur + S.rktype) & 1;

@@ -120,7 +120,7 @@ def estimated_work(cfg: dict) -> float:
 
 def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], float] = time.perf_counter,
           keep_results: bool = True, realtime: bool = True, policy: str = "fifo",
-          live_cells: Optional[int] = None) -> ServeStats:
+          live_cells: Optional[int] = None, boost: int = 8, short_frac: float = 0.05) -> ServeStats:
     """Run the stream through `batch` (a hormone_b200.batch.Batch or any
     object with add/step/poll/download/remove).  With realtime=False arrival
     times are ignored (every request is available at once).
@@ -130,8 +130,16 @@ def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], fl
     caps the cells of the admitted simulations (a request larger than the
     cap still runs when nothing else does): every batch step advances every
     live simulation, so a small request admitted beside many large ones
-    waits for as many of their steps as it needs itself."""
-    if policy not in ("fifo", "sjf"):
+    waits for as many of their steps as it needs itself.
+
+    policy "priority" admits in arrival order and, after every `chunk`
+    steps of all live simulations, holds the large ones (more cells than
+    short_frac of the largest live one) and advances the small ones alone
+    for boost x chunk more steps: a small request no longer pays for the
+    large ones' cells at every one of its steps.  (Needs a batch with
+    set_held.)  Every simulation still takes exactly its own steps, so the
+    results do not depend on the policy."""
+    if policy not in ("fifo", "sjf", "priority"):
         raise ValueError(f"unknown admission policy {policy!r}")
     stats = ServeStats()
     pending = sorted(requests, key=lambda r: r.arrival)
@@ -175,6 +183,14 @@ def serve(requests: List[Request], batch, chunk: int = 8, clock: Callable[[], fl
             continue
         batch.step(chunk)
         stats.batch_steps += chunk
+        if policy == "priority" and len(running) > 1:
+            top = max(r.cells for r in running.values())
+            held = [s for s, r in running.items() if r.cells > short_frac * top]
+            if len(held) < len(running):
+                batch.set_held(held)
+                batch.step(boost * chunk)
+                batch.set_held([])
+                stats.batch_steps += boost * chunk
         _, tn, done, err = batch.poll()
         for slot in [s for s in running if done[s] or err[s]]:
             r = running.pop(slot)

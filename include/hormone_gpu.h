@@ -319,9 +319,17 @@ int hmn_batch_add(hmn_batch* b, const hmn_grid* grid, const hmn_params* params, 
 /* Release a simulation's slot and pool memory. */
 int hmn_batch_remove(hmn_batch* b, int sim);
 
-/* Advance every admitted, unfinished simulation by up to nsteps steps
- * (a simulation stops at its t_end).  Asynchronous. */
+/* Advance every admitted, unfinished simulation that is not held by up to
+ * nsteps steps (a simulation stops at its t_end).  Asynchronous. */
 int hmn_batch_step(hmn_batch* b, int nsteps);
+
+/* held[s] != 0 (one int per slot, max_sims of them) leaves simulation s out
+ * of the following steps: its clock and state stay as they are until a
+ * later call releases it (held[s] = 0).  A scheduler uses it to advance
+ * small simulations alone between full steps; each simulation still takes
+ * exactly its own sequence of steps.  No reference counterpart (the
+ * reference runs one simulation per process). */
+int hmn_batch_set_held(hmn_batch* b, const int* held);
 
 /* Clock, step count, done flag and error code of every slot (arrays of
  * max_sims entries; any may be NULL).  Synchronises. */
