@@ -366,8 +366,8 @@ class SymmetricHalos:
     parities) are one symmetric allocation, so a neighbour's kernel can
     store into them directly (peer access over NVLink).  Sections are
     ordered (lo, 0), (lo, 1), (hi, 0), (hi, 1) of ``n`` doubles each.
-    (Not run on more than one GPU here: every GPU call of this build had
-    one.)"""
+    (Exercised on a one-rank group only; peer stores between GPUs are
+    untested.)"""
 
     SECTION = {("lo", 0): 0, ("lo", 1): 1, ("hi", 0): 2, ("hi", 1): 3}
 
