@@ -301,6 +301,15 @@ class LocalExchange:
     def cfg_rk(self) -> int:
         return int(self.ranks[0].cfg["rktype"])
 
+    def evo(self) -> Dict[str, float]:
+        """The evo_output totals of the whole grid: each slab's hmn_evo
+        totals added in slab order (output.f90:235-244 all-reduces them)."""
+        out: Dict[str, float] = {}
+        for s in self.ranks:
+            for k, v in s.ctx.evo().items():
+                out[k] = out.get(k, 0.0) + v
+        return out
+
     def state(self) -> Dict[str, np.ndarray]:
         """The global state assembled from the slabs (z is the slowest axis)."""
         parts = [s.state() for s in self.ranks]
@@ -343,6 +352,17 @@ class TorchExchange:
     def cfl(self, tmin, tmax):
         self.dist.all_reduce(tmin, op=self.dist.ReduceOp.MIN)
         self.dist.all_reduce(tmax, op=self.dist.ReduceOp.MAX)
+
+    def evo(self, sim: "SlabSimulation") -> Dict[str, float]:
+        """The evo_output totals of the whole grid: this slab's hmn_evo
+        totals summed over the ranks (output.f90:235-244)."""
+        import torch
+
+        tot = sim.ctx.evo()
+        dev = "cuda" if self.dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([tot[k] for k in tot], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return dict(zip(tot, t.tolist()))
 
     def min_scalar(self, v: float) -> float:
         """The minimum of a host double over the ranks."""

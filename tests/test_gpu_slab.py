@@ -94,6 +94,23 @@ def test_self_gravity_slabs_mixed_precision():
     run_both(cfg, prims, 2, 3, precision=1, grvphi=phi)
 
 
+@pytest.mark.parametrize("make", [lambda: cases.ot3d(16) + (None,), lambda: cases.polytrope(16)])
+def test_evo_totals_over_slabs(make):
+    """The evo_output totals summed over 3 slabs equal the undecomposed
+    grid's to rounding (both sum per block; the slabs add their totals)."""
+    cfg, prims, phi = make()
+    ref = Simulation(cfg, prims, grvphi=phi)
+    dec = slab.LocalExchange(cfg, prims, 3, grvphi=phi)
+    for _ in range(3):
+        ref.step()
+        dec.step()
+    a, b = ref.ctx.evo(), dec.evo()
+    ref.close()
+    dec.close()
+    for k in a:
+        assert abs(a[k] - b[k]) <= 1e-12 * max(abs(a[k]), 1e-300) + 1e-14 * abs(a["Etot"]), (k, a[k], b[k])
+
+
 @pytest.mark.parametrize("world", [1, 2, 3])
 def test_push_exchange_orszag_tang_periodic(world):
     """One slab wraps onto itself; two periodic slabs are each other's low
@@ -204,6 +221,7 @@ def test_distributed_gravity_step_on_one_rank_over_nccl():
             ref.step()
             slab.run_distributed_step(sim, ex)
             assert sim.dt == ref.dt
+        assert ex.evo(sim) == sim.ctx.evo()  # one rank: the sum is its own totals
         a, b = ref.state(gravity=True), sim.state()
         for k in a:
             assert np.array_equal(a[k], b[k]), k
