@@ -492,22 +492,26 @@ extern "C" int hmn_batch_poll(hmn_batch* b, double* time, int* tn, int* done, in
   if (!b) return HMN_EINVAL;
   int rc = pull(b);
   if (rc) return rc;
-  bool newly_done = false;
+  bool any_done = false;
   for (int s = 0; s < b->max_sims; s++) {
     const SimDesc& S = b->h_sims[s];
     if (time) time[s] = S.sc.time;
     if (tn) tn[s] = S.sc.tn;
     if (done) done[s] = b->slots[s].used ? S.sc.done : 0;
     if (err) err[s] = S.sc.err_code;
-    if (b->slots[s].used && S.sc.done) newly_done = true;
+    if (b->slots[s].used && S.sc.done) any_done = true;
   }
-  // drop finished simulations from the work list at the next step
-  if (newly_done) {
+  // drop finished simulations from the work list at the next step: the list
+  // is rebuilt only when its tile count differs from that of the used,
+  // unfinished and not held simulations (the set rebuild() lists), so a
+  // finished simulation left in its slot does not force a rebuild and graph
+  // re-capture at every poll
+  if (any_done) {
     size_t live = 0;
     for (const Klass& k : b->classes) live += k.count;
     size_t want = 0;
     for (int s = 0; s < b->max_sims; s++)
-      if (b->slots[s].used && !b->h_sims[s].sc.done) want += b->slots[s].ntiles;
+      if (b->slots[s].used && !b->h_sims[s].sc.done && !b->h_sims[s].held) want += b->slots[s].ntiles;
     if (want != live) b->dirty = true;
   }
   return HMN_OK;

@@ -4,7 +4,7 @@
 // unit is compiled with --fmad=false so nothing is fused).
 //
 // Reference routines (paths in the HORMONE tree):
-//   minmod / modified_mc   src/main/fluxlimiter.f90:94-129
+//   minmod / modified_mc   src/main/fluxlimiter.f90:40-56, 58-75
 //   get_eint               src/main/eos.f90:846-866
 //   get_cf                 src/main/eos.f90:351-365
 //   eos_p_cs (ideal gas)   src/main/eos.f90:195-242
@@ -23,7 +23,7 @@ __device__ __forceinline__ T fmin2(T a, T b) { return a < b ? a : b; }
 template <typename T>
 __device__ __forceinline__ T fmax2(T a, T b) { return a > b ? a : b; }
 
-// Generalised minmod with theta = 1.4 on inverse spacings (fluxlimiter.f90:94-110).
+// Generalised minmod with theta = 1.4 on inverse spacings (fluxlimiter.f90:40-56).
 // i0 = 1/dx(c), i1 = 1/dx(c+1), isum = i0 + i1.
 __device__ __forceinline__ double lim_minmod(double u0, double u1, double u2, double i0, double i1, double isum) {
   double x = 1.4 * (u2 - u1) * i1;
@@ -36,7 +36,7 @@ __device__ __forceinline__ double lim_minmod(double u0, double u1, double u2, do
   return s * fmax2(0.0, m);
 }
 
-// Modified MC (fluxlimiter.f90:112-129).  Grid factors precomputed per cell:
+// Modified MC (fluxlimiter.f90:58-75).  Grid factors precomputed per cell:
 // cf = (x(c+1)-x(c))/(xi(c)-x(c)), cb = (x(c)-x(c-1))/(x(c)-xi(c-1)),
 // ga = x(c+1)-x(c), gb = x(c)-x(c-1).
 __device__ __forceinline__ double lim_mmc(double u0, double u1, double u2, double cf, double cb, double ga,

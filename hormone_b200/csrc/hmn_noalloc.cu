@@ -8,8 +8,17 @@
 // Such callers cannot create an hmn_ctx (hmn_create allocates).  This entry point takes
 // the conserved state already on the device and writes dt, ch and a status
 // word to caller-owned device memory; the only other device memory it touches
-// is the file-scope scratch array below, which every GPU that loads the
-// library holds until the process exits.
+// is the file-scope scratch array below.  The CUDA runtime loads this
+// library's device code on a GPU lazily, at its first use there, and that
+// load is when the array is allocated; from then on the GPU holds it until
+// the process exits.  So the first call on each device allocates (it loads
+// the code and looks up the array's address) and belongs in the caller's
+// start-up, before the point after which it may not allocate.
+//
+// Every call copies the caller's host arrays of cell widths into the
+// scratch with cudaMemcpyAsync.  Host arrays are usually pageable, and a
+// pageable copy cannot be recorded into a CUDA graph, so the entry point is
+// not to be called while its stream is being captured.
 //
 // Scratch layout (doubles): the cell widths dxi of the three axes (at most
 // kNoallocMaxAxis+4 values each), then one (min dti, max cf) pair per block
@@ -40,8 +49,7 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoallocWords];
 // Device address of g_noalloc_scratch per device.  In host code the symbol
 // name is only a host-side stand-in, so the first call on each device looks
 // the address up with cudaGetSymbolAddress (that device current) and later
-// calls reuse it.  Make that first call on a device before any stream
-// capture begins.
+// calls reuse it.
 constexpr int kMaxDevices = 64;
 static double* g_scratch_ptr[kMaxDevices] = {nullptr};
 
@@ -173,6 +181,10 @@ extern "C" int hmn_timestep_noalloc(const hmn_grid* grid, const hmn_params* par,
                                     double t_out, double t_end, double* out_dev, void* stream) {
   if (!grid || !par || !u_dev || !out_dev) return HMN_EINVAL;
   if (par->gravswitch != 0) return HMN_EBADCFG;  // the gravity wave speed needs the context's state
+  if (grid->ghost != 0) {                        // u_dev is read as packed interior planes
+    fprintf(stderr, "hmn_timestep_noalloc: u_dev must be packed (grid->ghost = 0, got %d)\n", grid->ghost);
+    return HMN_EINVAL;
+  }
   NoallocGrid G;
   size_t plane = 1;
   for (int a = 0; a < 3; a++) {

@@ -362,10 +362,14 @@ int hmn_batch_destroy(hmn_batch* b);
  * per GPU that loads the library: at most 4096 cells per axis (larger
  * grids return HMN_EINVAL), gravswitch must be 0, and the grid is taken
  * as Cartesian (a curvilinear grid's timestep goes through hmn_timestep,
- * which has its metric).  The first call on a
- * device looks up the array's device address; make it before any stream
- * capture.  Calls that overlap on the GPU share the array and race: the
- * caller must order them. */
+ * which has its metric).  u_dev must be packed: grid->ghost other than 0
+ * returns HMN_EINVAL.  The first call on a device allocates: the CUDA
+ * runtime loads the library's device code there (and with it the array)
+ * and the call looks up the array's address, so make it at start-up.
+ * Every call copies grid->dxi from host memory on `stream`, so it must not
+ * be called while that stream is being captured into a CUDA graph.  Calls
+ * that overlap on the GPU share the array and race: the caller must order
+ * them. */
 int hmn_timestep_noalloc(const hmn_grid* grid, const hmn_params* params, const double* u_dev, double time,
                          double t_out, double t_end, double* out_dev, void* stream);
 

@@ -20,7 +20,7 @@
  *                   (cylindrical R, phi, z without a solved phi)
  *   metric          src/main/metric.f90:26-51 (Cartesian), :53-100
  *                   (cylindrical), :102-151 (spherical)
- *   limiters        src/main/fluxlimiter.f90:94-129
+ *   limiters        src/main/fluxlimiter.f90:40-56 (minmod), 58-75 (modified_mc)
  *   slopes          src/main/interpolation.f90:49-484
  *   face fluxes     src/main/numflux.f90:46-563
  *   HLLD + GLM      src/main/hlldflux.f90:19-179
@@ -712,7 +712,7 @@ static void boundarycondition(Oracle *o) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* limiters: fluxlimiter.f90:94-129                                           */
+/* limiters: fluxlimiter.f90:40-56 (minmod), 58-75 (modified_mc)            */
 
 static inline double minmod(const double u[3], const double dx[2]) {
   double x = 1.4 * (u[2] - u[1]) * dx[1];

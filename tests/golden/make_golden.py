@@ -3,7 +3,8 @@
 Reads ``tests/<simtype>[_flat].bin`` of the reference tree (the files that
 src/main/tests.f90:46-182 compares a finished test run against) with
 ``hormone_b200.binio.readbin`` and writes ``<simtype>[_flat].npz`` beside this
-script.  Run once where the reference tree is present:
+script.  Run once where the reference tree is present, giving its root as the
+argument or in the environment variable HORMONE_REF:
 
     python tests/golden/make_golden.py /path/to/HORMONE
 """
@@ -36,4 +37,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HORMONE_REF")
+    if not root:
+        sys.exit("usage: make_golden.py <HORMONE tree> (or set HORMONE_REF)")
+    main(root)

@@ -10,7 +10,7 @@ This file is collected last so that, if it fails, a run stopping at the
 first failure has already run every other test.  It checks the result against
 hmn_timestep (the allocating entry point) bit for bit, on two calls in a row
 (the second sees the state one step later and reuses the same scratch), and
-that oversize grids and negative-energy states are reported."""
+that oversize grids, ghosted layouts and negative-energy states are reported."""
 import ctypes
 
 import numpy as np
@@ -80,4 +80,9 @@ def test_noalloc_reports_negative_energy_and_rejects_oversize_grids():
     gb, keepb = capi.grid_struct(big, G.make_grid(big))
     rc = L.hmn_timestep_noalloc(ctypes.byref(gb), ctypes.byref(capi.params_struct(big)), _ptr(u_dev), 0.0, 1.0, 1.0,
                                 _ptr(out), ctypes.c_void_p(stream.cuda_stream))
+    assert rc == capi.HMN_EINVAL
+    gg, keepg = capi.grid_struct(cfg, G.make_grid(cfg))
+    gg.ghost = 2  # the state is read as packed planes; a ghosted layout is refused
+    rc = L.hmn_timestep_noalloc(ctypes.byref(gg), ctypes.byref(ps), _ptr(u_dev), 0.0, 1.0, 1.0, _ptr(out),
+                                ctypes.c_void_p(stream.cuda_stream))
     assert rc == capi.HMN_EINVAL
