@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhormone_b200.so")
-SOURCES = ["hmn_kernels.cu", "hmn_capi.cu", "hmn_noalloc.cu", "hmn_mixed.cu", "hmn_batch.cu"]
+SOURCES = ["hmn_kernels.cu", "hmn_march.cu", "hmn_capi.cu", "hmn_noalloc.cu", "hmn_mixed.cu", "hmn_batch.cu"]
 # per-source precision flags: the FP64 path is bit-compatible (no fused
 # multiply-add); the mixed-precision stage uses fast single-precision math
 FLAGS = {"hmn_mixed.cu": ["-use_fast_math"]}
@@ -29,25 +29,35 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def _mtime(path: str) -> float:
+    return os.path.getmtime(path) if os.path.exists(path) else -1.0
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "hormone_gpu.h")]
-    if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
-        return LIB
-    objs, procs = [], []
+    """Compile the translation units whose object is older than their source
+    or any header (all of them with force), in parallel, and link the library."""
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if not f.endswith(".cu")] + \
+        [os.path.join(HERE, "..", "include", "hormone_gpu.h")]
+    newest_header = max(_mtime(h) for h in headers)
     bdir = os.path.join(HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
+    objs, procs = [], []
     for src in SOURCES:  # translation units compile in parallel
+        path = os.path.join(CSRC, src)
         obj = os.path.join(bdir, src.replace(".cu", ".o"))
+        objs.append(obj)
+        if not force and _mtime(obj) >= max(_mtime(path), newest_header):
+            continue
         cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", *FLAGS.get(src, DEFAULT_FLAGS), "-lineinfo", "-Xcompiler",
-               "-fPIC,-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
+               "-fPIC,-ffp-contract=off", "-c", path, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((src, subprocess.Popen(cmd)))
-        objs.append(obj)
     failed = [src for src, p in procs if p.wait() != 0]
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
-    subprocess.run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], check=True)
+    if procs or _mtime(LIB) < max(_mtime(o) for o in objs):
+        subprocess.run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], check=True)
     return LIB
 
 

@@ -174,6 +174,12 @@ void stage_tile(const int solve[3], int precision, int nspc, int tile[3]);
 // tm: tensor maps of A.pin for TMA staging (3-D tiles; nullptr stages with plain loads)
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st);
+// the FP64 stage of a 3-D Cartesian grid without passive scalars as a march
+// along z (hmn_march.cu); cudaErrorNotSupported for every other grid
+cudaError_t launch_stage_march(const GridDev& G, const StageArgs& A, bool mag, bool glm, cudaStream_t st);
+bool march_enabled();
+// its decomposition: z planes per chunk, column tiles along x and y, chunks
+void march_chunks(const int n[3], int* lz, int* ntx, int* nty, int* nch);
 // mixed precision (hmn_mixed.cu): FP32 Riemann solver, FP64 reconstruction and accumulation
 cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                                cudaStream_t st);

@@ -774,6 +774,10 @@ static cudaError_t launch_scalar_tiles(const GridDev& G, const StageArgs& A, boo
 
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st) {
+  {
+    const cudaError_t e = launch_stage_march(G, A, mag, glm, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
   if (A.push[0] != nullptr || A.push[1] != nullptr) return launch_stage_push(G, A, mag, glm, st);
   if (G.sph.on) return launch_stage_spherical(G, A, mag, glm, st);
   const int* t = A.tile;
