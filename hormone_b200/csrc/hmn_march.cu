@@ -145,16 +145,45 @@ __device__ __forceinline__ void slopes_with(const double* pm, const double* p0, 
   }
 }
 
+// The slopes with IEEE division, out of line: the rare path of slopes_of.
+template <bool MAG, int LIM, int QS>
+__device__ __noinline__ void slopes_ieee(const double* pm, const double* p0, const double* pp, const AxisGeo* g,
+                                         int cg, double* out) {
+  PlainDiv pd;
+  double sl[NS];
+  slopes_with<MAG, LIM, QS>(pm, p0, pp, *g, cg, sl, pd);
+#pragma unroll
+  for (int q = 0; q < NS; q++) out[q] = sl[q];
+}
+
 // The slopes with every quotient formed by FastDiv, recomputed with IEEE
 // division where FastDiv could not vouch for one (bitwise the same result).
+// One out-of-line copy serves every call site, so that warps in different
+// phases of the march share instruction cache lines.
+template <bool MAG, int LIM, int QS>
+__device__ __noinline__ void slopes_fast(const double* pm, const double* p0, const double* pp, const AxisGeo* g,
+                                         int cg, double* out) {
+  FastDiv fd;
+  double sl[NS];
+  slopes_with<MAG, LIM, QS>(pm, p0, pp, *g, cg, sl, fd);
+  if (fd.bad) {
+    slopes_ieee<MAG, LIM, QS>(pm, p0, pp, g, cg, out);
+    return;
+  }
+#pragma unroll
+  for (int q = 0; q < NS; q++) out[q] = sl[q];
+}
 template <bool MAG, int LIM, int QS>
 __device__ __forceinline__ void slopes_of(const double* pm, const double* p0, const double* pp, const AxisGeo& g,
                                           int cg, double sl[NS]) {
-  FastDiv fd;
-  slopes_with<MAG, LIM, QS>(pm, p0, pp, g, cg, sl, fd);
-  if (fd.bad) {
-    PlainDiv pd;
-    slopes_with<MAG, LIM, QS>(pm, p0, pp, g, cg, sl, pd);
+  if constexpr (LIM == 0) {
+#pragma unroll
+    for (int q = 0; q < NS; q++) sl[q] = 0.0;
+  } else {
+    double tmp[NS];
+    slopes_fast<MAG, LIM, QS>(pm, p0, pp, &g, cg, tmp);
+#pragma unroll
+    for (int q = 0; q < NS; q++) sl[q] = tmp[q];
   }
 }
 
@@ -210,17 +239,39 @@ __device__ __forceinline__ bool face_flux_with(PL pl, PR pr, SL sl, SR sr, doubl
   return true;
 }
 
+// The face flux with IEEE division, out of line: the rare path of
+// face_flux.  pl/pr: staged quantity 0 of the cells (stride QS); sl/sr:
+// slope 0 (strides ssl, ssr).
+template <bool MAG, int QS>
+__device__ __noinline__ bool face_flux_ieee(const double* pl, const double* pr, const double* sl, int ssl,
+                                            const double* sr, int ssr, double dx1, double dx2, int cn, int c1, int c2,
+                                            double gamma, double gm1, double ch, double* out) {
+  PlainDiv pd;
+  double fl[9];
+  const bool ok = face_flux_with<MAG>([&](int q) { return pl[q * QS]; }, [&](int q) { return pr[q * QS]; },
+                                      [&](int q) { return sl[q * ssl]; }, [&](int q) { return sr[q * ssr]; }, dx1,
+                                      dx2, cn, c1, c2, gamma, gm1, ch, fl, pd);
+#pragma unroll
+  for (int q = 0; q < 9; q++) out[q] = fl[q];
+  return ok;
+}
+
 // The face flux with every quotient formed by FastDiv, recomputed with IEEE
-// division where FastDiv could not vouch for one (bitwise the same result).
-template <bool MAG, class PL, class PR, class SL, class SR>
-__device__ __forceinline__ bool face_flux(PL pl, PR pr, SL sl, SR sr, double dx1, double dx2, int cn, int c1, int c2,
-                                          double gamma, double gm1, double ch, double fl[9]) {
+// division where FastDiv could not vouch for one (bitwise the same result);
+// one out-of-line copy for the x, y and z faces.  Arguments as
+// face_flux_ieee.
+template <bool MAG, int QS>
+__device__ __noinline__ bool face_flux_fast(const double* pl, const double* pr, const double* sl, int ssl,
+                                            const double* sr, int ssr, double dx1, double dx2, int cn, int c1, int c2,
+                                            double gamma, double gm1, double ch, double* out) {
   FastDiv fd;
-  bool ok = face_flux_with<MAG>(pl, pr, sl, sr, dx1, dx2, cn, c1, c2, gamma, gm1, ch, fl, fd);
-  if (fd.bad) {
-    PlainDiv pd;
-    ok = face_flux_with<MAG>(pl, pr, sl, sr, dx1, dx2, cn, c1, c2, gamma, gm1, ch, fl, pd);
-  }
+  double fl[9];
+  const bool ok = face_flux_with<MAG>([&](int q) { return pl[q * QS]; }, [&](int q) { return pr[q * QS]; },
+                                      [&](int q) { return sl[q * ssl]; }, [&](int q) { return sr[q * ssr]; }, dx1,
+                                      dx2, cn, c1, c2, gamma, gm1, ch, fl, fd);
+  if (fd.bad) return face_flux_ieee<MAG, QS>(pl, pr, sl, ssl, sr, ssr, dx1, dx2, cn, c1, c2, gamma, gm1, ch, out);
+#pragma unroll
+  for (int q = 0; q < 9; q++) out[q] = fl[q];
   return ok;
 }
 
@@ -300,10 +351,11 @@ __device__ __forceinline__ bool z_face(const double* Wk, const double* Wk1, cons
                                        double fz[9]) {
   constexpr int QS = MT::NPL;
   const double dx1 = gz.hr[k + 2], dx2 = gz.hl[k + 3];
-  double fl[9];
-  const bool ok = face_flux<MAG>([&](int q) { return Wk[q * QS]; }, [&](int q) { return Wk1[q * QS]; },
-                                 [&](int q) { return sm.SZ[q][t]; }, [&](int q) { return szn[q]; }, dx1, dx2, 2, 0, 1,
-                                 A.gamma, A.gm1, ch, fl);
+  double fl[9], sr[NS];
+#pragma unroll
+  for (int q = 0; q < NS; q++) sr[q] = szn[q];
+  const bool ok =
+      face_flux_fast<MAG, QS>(Wk, Wk1, &sm.SZ[0][t], MT::NC, sr, 1, dx1, dx2, 2, 0, 1, A.gamma, A.gm1, ch, fl);
   // rotate back into the conserved slots (numflux.f90:531-543)
   fz[ICNT] = fl[0];
   fz[IMO1 + 2] = fl[1];
@@ -451,9 +503,7 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
       const double* SLp = &sm.S[0][sL];
       const double* SRp = &sm.S[0][sR];
       constexpr int SS = MT::NSXY;
-      if (!face_flux<MAG>([&](int q) { return PL[q * QS]; }, [&](int q) { return PR[q * QS]; },
-                          [&](int q) { return SLp[q * SS]; }, [&](int q) { return SRp[q * SS]; }, dx1, dx2, cn, c1, c2,
-                          A.gamma, A.gm1, ch, fl)) {
+      if (!face_flux_fast<MAG, QS>(PL, PR, SLp, SS, SRp, SS, dx1, dx2, cn, c1, c2, A.gamma, A.gm1, ch, fl)) {
         int gi[3] = {x0 + fi, y0 + fj, k};
         gi[ax] = gL;
         record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);
