@@ -32,7 +32,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "zone-updates/s"
-WORKLOAD = "orszag-tang-3d-256^3-fp64"
 
 
 def parse():
@@ -42,8 +41,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=256)
-    ap.add_argument("--cpu-size", type=int, default=128, help="edge of the box the CPU legs time")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-size", type=int, default=0, help="edge of the box the CPU legs time (0: --size)")
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--no-extra", action="store_true", help="skip the compact kh_batch and serve legs")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
@@ -163,6 +163,25 @@ def profiled_traffic(prefix="stage_kernel_ot3d"):
     return profiled_value("dram_bytes_per_cell", prefix)
 
 
+def profile_source(prefix):
+    """The committed ncu summary the profiled figures come from, and the
+    commit of the kernel it captured (its line 'captured_at_commit: X')."""
+    pdir = os.path.join(ROOT, "profiles")
+    for fn in sorted(os.listdir(pdir)) if os.path.isdir(pdir) else []:
+        if fn.startswith(prefix) and fn.endswith(".md"):
+            m = re.search(r"captured_at_commit:\s*([0-9a-f]+)", open(os.path.join(pdir, fn)).read())
+            return {"file": f"profiles/{fn}", "commit": m.group(1) if m else None}
+    return None
+
+
+def ot_line_config(n, world):
+    """config of the Orszag-Tang line, the same for the GPU and the reference arm."""
+    return {"workload": f"orszag-tang-3d-{n}^3-fp64", "grid": [n, n, n], "cells_per_gpu": n ** 3,
+            "limiter": "modified_mc", "rktype": 3, "courant": 0.9,
+            "l2": f"inputs larger than L2 (9 x 8 B x {n}^3 = {9 * 8 * n ** 3 / 1e9:.2f} GB per RK buffer)",
+            "parallelism": f"replicas{world}"}
+
+
 # ---------------------------------------------------------------------------
 def cpu_leg(n, steps, warm=1):
     """The oracle (C restatement, OpenMP over all host cores) on an n^3 box of
@@ -188,27 +207,31 @@ def run_reference(args, rank):
         return
     import oracle.oracle as orc  # noqa: F401  (builds liboracle.so if needed)
 
-    n = args.cpu_size
+    # the GPU arm's grid and workload; the CPU steps are the sample: at most
+    # --steps of them (about 3 s each at 256^3 on 16 cores), one untimed
+    n = args.size
+    steps = max(3, min(args.steps, 20))
     from oracle.oracle import Oracle
 
     cfg = ot_config(n)
     o = Oracle(cfg)
     o.set_prims(ot_prims(cfg, 20261203))
     o.start()
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 1)):
         o.step()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         o.step()
     el = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    v = n ** 3 * args.steps / el
-    sample = (f"{n}^3 box of the same 3-D Orszag-Tang workload, {args.steps} full steps; CPU restatement of "
-              f"HORMONE's FP64 step (the Fortran reference cannot be compiled here), OpenMP over {cores} threads")
+    v = n ** 3 * steps / el
+    sample = (f"{n}^3 box of the same 3-D Orszag-Tang workload, {steps} full steps after {min(args.warmup, 1)} "
+              f"untimed; CPU restatement of HORMONE's FP64 step (the Fortran reference cannot be compiled here), "
+              f"OpenMP over {cores} threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": n ** 3, "grid": [n, n, n], "note": "bounded CPU sample"},
+            "config": ot_line_config(n, args.gpus),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -364,13 +387,26 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes = (2 + 3 + 3) * nvar * 8 / 3 * cells  # per stage launch, averaged over the 3 stages
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
-    tpc = profiled_traffic()
+    prof = "march_stage_ot3d"  # the ncu summary of the stage kernel this grid runs on
+    tpc = profiled_traffic(prof)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": (tpc * cells) if tpc else None, "kernel": "stage_kernel",
+                "traffic": (tpc * cells) if tpc else None, "kernel": "march_stage_kernel",
                 "alg_bytes_per_launch": alg_bytes, "launch_ms": stage_ms, "peak_kind": peak_kind,
-                "fp64_pipe": profiled_value("fp64_pipe_frac"),
-                "note": "FP64-issue-bound stencil: frac is of measured HBM copy bandwidth; fp64_pipe is ncu's "
-                        "FP64 pipe utilisation of the same kernel (profiles/)"}
+                "traffic_source": profile_source(prof),
+                "note": "FP64-issue-bound stencil: frac is of measured HBM copy bandwidth; the instruction "
+                        "bounds below use per-cell instruction counts from the ncu summary in traffic_source "
+                        "(counts per cell do not depend on timing) and this run's launch time and SM clock"}
+    # the bounds the stage actually meets: issue slots (one warp instruction
+    # per cycle per SM sub-partition) and the FP64 pipe (a warp instruction
+    # takes it for two cycles: 16 FP64 lanes per sub-partition)
+    winst, fpinst = profiled_value("warp_inst_per_cell", prof), profiled_value("fp64_warp_inst_per_cell", prof)
+    nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    clk_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    slots = stage_ms * 1e-3 * nsm * 4 * clk_hz
+    if winst:
+        roofline["issue_frac"] = winst * cells / slots
+    if fpinst:
+        roofline["fp64_pipe_frac"] = 2 * fpinst * cells / slots
 
     # end to end through the drop-in C ABI with pinned host buffers: the
     # conserved state U goes up (hmn_upload derives the primitives from it on
@@ -408,24 +444,106 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_mixed:
         mixed = mixed_leg(args, cfg, prims, sim, rank, world, dist)
 
+    sim.close()
+    extra = {}
+    if rank == 0 and world == 1 and not args.no_extra:
+        extra = extra_legs(args, value, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, el = cpu_leg(args.cpu_size, args.cpu_steps)
+        cn = args.cpu_size or n
+        v, cores, el = cpu_leg(cn, args.cpu_steps)
         cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-               "sample": f"{args.cpu_size}^3 box of the same workload, {args.cpu_steps} full steps "
+               "sample": f"{cn}^3 box of the same workload, {args.cpu_steps} full steps after one untimed "
                          f"({el:.1f} s) of the CPU restatement, OpenMP"}
-    sim.close()
     if rank == 0:
+        config = ot_line_config(n, world)
+        config["precision"] = "fp64 bit-compatible (no FMA)"
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "grid": [n, n, n], "cells_per_gpu": cells, "limiter": "modified_mc",
-                           "rktype": 3, "courant": 0.9, "precision": "fp64 bit-compatible (no FMA)",
-                           "l2": f"inputs larger than L2 (9 x 8 B x {n}^3 = {9 * 8 * n ** 3 / 1e9:.2f} GB per RK buffer)",
-                           "parallelism": f"replicas{world}"},
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "mixed": mixed,
                 "clocks": clocks}
+        line.update(extra)
         print(json.dumps(line), flush=True)
+
+
+def kh_boxes(nboxes, seed=20261203):
+    """(cfg, density ratio, Bx) of the periodic Kelvin-Helmholtz boxes of the
+    batched benchmark: edges round(128 * 4^u), u ~ U[0, 1], seeded."""
+    import numpy as np
+
+    from hormone_b200 import config
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    boxes = []
+    for _ in range(nboxes):
+        n = int(round(128 * 4 ** rng.uniform()))
+        ratio, bx = float(rng.uniform(1, 4)), float(rng.uniform(0, 0.1))
+        ov = dict(ie=n, je=n, ke=1, mag_on=True, gamma=1.6666666666666667, t_end=2.0, dt_out=2.0,
+                  xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5)
+        boxes.append((config.resolve("kh_batch", overrides=ov), ratio, bx))
+    return boxes
+
+
+def batch_leg(boxes, steps, warmup, precision):
+    """`steps` steps of every box in one batch (persistent launches, autotuned
+    schedule, CUDA graph), timed on the batch's stream: zone-updates/s."""
+    import numpy as np
+    import torch
+
+    from hormone_b200 import autotune
+    from hormone_b200.batch import Batch, footprint
+
+    sched = autotune.tune(boxes[:32], precision=precision, steps=2, cache=None)
+    b = Batch(sum(footprint(c) for c, _ in boxes) + (1 << 26), max_sims=len(boxes) + 1, precision=precision)
+    for c, p in boxes:
+        assert b.add(c, p) is not None
+    autotune.apply(b, sched)
+    stream = torch.cuda.ExternalStream(b.stream_ptr())
+    b.step(warmup)
+    b.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    b.close()
+    cells = sum(int(np.prod(c["n"])) for c, _ in boxes)
+    return {"value": cells * steps / (ms * 1e-3), "ms_per_step": ms / steps, "cells": cells}
+
+
+def extra_legs(args, plain_fp64, local_rank):
+    """The batched and served forms on compact versions of their benchmarks,
+    each in FP64 and in the mixed form, with the ratios of the mixed form to
+    the plain FP64 form (the Orszag-Tang value of this line) and to the same
+    form in FP64."""
+    import torch
+
+    from hormone_b200 import grid as G, ic, serve
+    from hormone_b200.batch import Batch
+
+    boxes = [(c, ic.kelvin_helmholtz(c, G.make_grid(c), r, bx)) for c, r, bx in kh_boxes(64)]
+    kb = {p: batch_leg(boxes, 20, 3, p) for p in (0, 1)}
+    kh = {"workload": "kh-batch-64-boxes-128^2..512^2: the first 64 boxes of the 512-box set, 20 steps after 3",
+          "cells": kb[0]["cells"], "fp64": kb[0]["value"], "mixed": kb[1]["value"],
+          "ms_per_step": {"fp64": kb[0]["ms_per_step"], "mixed": kb[1]["ms_per_step"]},
+          "mixed_over_fp64_batch": kb[1]["value"] / kb[0]["value"],
+          "mixed_over_plain_fp64": kb[1]["value"] / plain_fp64}
+    sv = {}
+    for p in (0, 1):
+        reqs = serve.make_requests(32, rate=50.0, seed=20261203)
+        free, _ = torch.cuda.mem_get_info()
+        b = Batch(int(free * 0.6), max_sims=1024, precision=p)
+        st = serve.serve(reqs, b, chunk=8, keep_results=False, policy="priority").summary()
+        b.close()
+        sv[p] = st
+    srv = {"workload": "serve-32-requests-poisson-50/s: the first 32 requests of the seeded 4096-request stream",
+           "fp64": {k: sv[0][k] for k in ("zone_updates_per_s", "p50_s", "p99_s", "completed", "failed")},
+           "mixed": {k: sv[1][k] for k in ("zone_updates_per_s", "p50_s", "p99_s", "completed", "failed")},
+           "mixed_over_fp64_served": sv[1]["zone_updates_per_s"] / sv[0]["zone_updates_per_s"],
+           "mixed_over_plain_fp64": sv[1]["zone_updates_per_s"] / plain_fp64}
+    return {"kh_batch": kh, "serve": srv}
 
 
 def run_slab(args, rank, world, local_rank):
@@ -500,15 +618,7 @@ def run_kh_batch(args, rank=0, world=1, local_rank=0):
     if world > 1:
         import torch.distributed as dist
 
-    rng = np.random.Generator(np.random.PCG64(20261203))
-    boxes = []
-    for b in range(args.boxes):
-        n = int(round(128 * 4 ** rng.uniform()))
-        ratio, bx = float(rng.uniform(1, 4)), float(rng.uniform(0, 0.1))
-        ov = dict(ie=n, je=n, ke=1, mag_on=True, gamma=1.6666666666666667, t_end=2.0, dt_out=2.0,
-                  xi1s=-0.5, xi1e=0.5, xi2s=-0.5, xi2e=0.5)
-        cfg = config.resolve("kh_batch", overrides=ov)
-        boxes.append((cfg, ratio, bx))
+    boxes = kh_boxes(args.boxes)
     total_cells = sum(int(np.prod(c["n"])) for c, _, _ in boxes)
     mine = shard.my_share([footprint(c) for c, _, _ in boxes], rank, world)
     boxes = [(c, ic.kelvin_helmholtz(c, G.make_grid(c), r, b)) for i, (c, r, b) in enumerate(boxes) if i in set(mine)]
