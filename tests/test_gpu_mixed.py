@@ -77,22 +77,41 @@ def l1_rel(a, b):
     return float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
 
 
-# Density L1 of a whole run against the FP64 result.  Over a whole run the
-# difference is set by the scheme's slope-zeroing switch, not by the size of
-# the FP32 rounding: the FP64 scheme itself, started from a state perturbed
-# by 1e-9, ends Brio-Wu (1024 cells, t=0.1) 3e-5 away in L1(rho)
-# (tests/test_oracle_sensitivity.py), and a perturbation of 1e-14 ends 5e-3
-# away by t=0.5 on Orszag-Tang.  The bounds below are that sensitivity with a
-# margin; the per-step bound of 1e-6 is test_mixed_one_step_error.
-@pytest.mark.parametrize("name,tol", [("briowushock_x", 2e-3), ("sodshock_x", 2e-3), ("briowushock_y", 2e-3),
-                                      ("orszagtang_xy", 2e-2), ("sedov_default", 2e-3)])
-def test_mixed_whole_run_against_fp64(name, tol):
+def run_noisy_fp64(cfg, prims, seed=5, eps=2.0 ** -24):
+    """The FP64 form with an FP32-sized relative perturbation (uniform in
+    [-eps, eps], seeded) of every conserved value after every step: the
+    flow's own response to noise of the size the mixed form's FP32 fluxes
+    carry."""
+    rng = np.random.default_rng(seed)
+    s = Simulation(cfg, prims, precision=0)
+    while True:
+        end = s.step()
+        if end:
+            break
+        u = s.state()["u"]
+        s.ctx.upload(u=u * (1.0 + eps * rng.uniform(-1.0, 1.0, u.shape)))  # primitives derived from the new u
+        if s.mag_glm:
+            s.ctx.phidamp()  # the upload dropped the step's pending phidamp factor; set it again
+    st = s.state()
+    s.close()
+    return st
+
+
+# Density L1 of a whole run against the FP64 result, bounded by twice that of
+# the FP64 form with FP32-sized noise injected every step (both measured
+# here).  Over a whole run the difference is set by the scheme's
+# slope-zeroing switch, a discontinuous function of the state, not by the
+# size of the rounding; the per-step bound of 1e-6 is
+# test_mixed_one_step_error.
+@pytest.mark.parametrize("name", ["briowushock_x", "sodshock_x", "briowushock_y", "orszagtang_xy", "sedov_default"])
+def test_mixed_whole_run_against_fp64(name):
     cfg, prims = cases.golden_case(name)
     a = run_to_end(cfg, prims, 0)
     b = run_to_end(cfg, prims, 1)
-    l1 = l1_rel(b["d"], a["d"])
-    print(f"{name}: L1(rho) mixed vs fp64 = {l1:.3e}")
-    assert l1 <= tol, l1
+    c = run_noisy_fp64(cfg, prims)
+    l1, l1n = l1_rel(b["d"], a["d"]), l1_rel(c["d"], a["d"])
+    print(f"{name}: L1(rho) mixed vs fp64 = {l1:.3e}; fp64 with fp32-sized noise vs fp64 = {l1n:.3e}")
+    assert l1 <= 2.0 * l1n, (l1, l1n)
 
 
 def test_mixed_brio_wu_1024_cells():
