@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <cstdlib>
 
+#include "hmn_face.cuh"
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
 #include "hmn_tile.cuh"
@@ -75,61 +76,24 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
     const int rp = TL::pidx(lp[0], lp[1], lp[2]);
     const int cg = lc[AX] + t0[AX];  // global coordinate along AX
     double sl[NS];
-    if (A.limiter == 0) {
-#pragma unroll
-      for (int q = 0; q < NS; q++) sl[q] = 0.0;
-      if constexpr (TL::SP > 0)
-        for (int n = 0; n < A.nspc; n++) sm.S[NS + n][w] = 0.0;
-    } else {
-      constexpr int qmap[NS] = {Q_D, Q_E, Q_M + 0, Q_M + 1, Q_M + 2, Q_B + 0, Q_B + 1, Q_B + 2};
-      const double hl = g.hl[cg + 2], hr = g.hr[cg + 2];
-      double L[NS], R[NS];
-      if (A.limiter == 1) {
-        const double i0 = g.idx[cg + 2], i1 = g.idx[cg + 3], is = g.isum[cg + 2];
-#pragma unroll
-        for (int q = 0; q < nsl; q++) {
-          const double u0 = sm.P[qmap[q]][rm], u1 = sm.P[qmap[q]][r], u2 = sm.P[qmap[q]][rp];
-          const double du = lim_minmod(u0, u1, u2, i0, i1, is);
-          sl[q] = du;
-          L[q] = u1 - hl * du;
-          R[q] = u1 + hr * du;
-        }
-      } else {
-        const double cf = g.mcf[cg + 2], cb = g.mcb[cg + 2], ga = g.ga[cg + 2], gb = g.gb[cg + 2];
-#pragma unroll
-        for (int q = 0; q < nsl; q++) {
-          const double u0 = sm.P[qmap[q]][rm], u1 = sm.P[qmap[q]][r], u2 = sm.P[qmap[q]][rp];
-          const double du = lim_mmc(u0, u1, u2, cf, cb, ga, gb);
-          sl[q] = du;
-          L[q] = u1 - hl * du;
-          R[q] = u1 + hr * du;
-        }
-      }
-#pragma unroll
-      for (int q = nsl; q < NS; q++) sl[q] = 0.0;
-      // passive-scalar slopes (interpolation.f90:135-141), not zeroed below
-      if constexpr (TL::SP > 0) {
-        for (int n = 0; n < A.nspc; n++) {
+    if (A.limiter == 1)
+      slopes_of<MAG, 1, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, sl);
+    else if (A.limiter == 2)
+      slopes_of<MAG, 2, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, sl);
+    else
+      slopes_of<MAG, 0, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, sl);
+    // passive-scalar slopes (interpolation.f90:135-141), not zeroed by the eint check
+    if constexpr (TL::SP > 0) {
+      for (int n = 0; n < A.nspc; n++) {
+        double du = 0.0;
+        if (A.limiter != 0) {
           const double u0 = sm.P[NQ + n][rm], u1 = sm.P[NQ + n][r], u2 = sm.P[NQ + n][rp];
-          double du;
           if (A.limiter == 1)
             du = lim_minmod(u0, u1, u2, g.idx[cg + 2], g.idx[cg + 3], g.isum[cg + 2]);
           else
             du = lim_mmc(u0, u1, u2, g.mcf[cg + 2], g.mcb[cg + 2], g.ga[cg + 2], g.gb[cg + 2]);
-          sm.S[NS + n][w] = du;
         }
-      }
-      // admissibility of the face internal energies (interpolation.f90:147-163)
-      double eintl = L[S_E] - 0.5 * (L[S_M] * L[S_M] + L[S_M + 1] * L[S_M + 1] + L[S_M + 2] * L[S_M + 2]) / L[S_D];
-      double eintr = R[S_E] - 0.5 * (R[S_M] * R[S_M] + R[S_M + 1] * R[S_M + 1] + R[S_M + 2] * R[S_M + 2]) / R[S_D];
-      if (MAG) {
-        eintl = eintl - 0.5 * (L[S_B] * L[S_B] + L[S_B + 1] * L[S_B + 1] + L[S_B + 2] * L[S_B + 2]);
-        eintr = eintr - 0.5 * (R[S_B] * R[S_B] + R[S_B + 1] * R[S_B + 1] + R[S_B + 2] * R[S_B + 2]);
-      }
-      const double em = sm.P[Q_EINT][rm], e0 = sm.P[Q_EINT][r], ep = sm.P[Q_EINT][rp];
-      if (eintl >= fmax2(em, e0) || eintl <= fmin2(em, e0) || eintr >= fmax2(e0, ep) || eintr <= fmin2(e0, ep)) {
-#pragma unroll
-        for (int q = 0; q < NS; q++) sl[q] = 0.0;
+        sm.S[NS + n][w] = du;
       }
     }
 #pragma unroll
@@ -153,47 +117,12 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
     const int gL = t0[AX] + f - 1;
     const double dx1 = g.hr[gL + 2];  // xi(i)-x(i)
     const double dx2 = g.hl[gL + 3];  // x(i+1)-xi(i)
-    const double dl = sm.P[Q_D][rL] + dx1 * sm.S[S_D][sL];
-    const double dr = sm.P[Q_D][rR] - dx2 * sm.S[S_D][sR];
-    const double el = sm.P[Q_E][rL] + dx1 * sm.S[S_E][sL];
-    const double er = sm.P[Q_E][rR] - dx2 * sm.S[S_E][sR];
-    const double v1l = (sm.P[Q_M + cn][rL] + dx1 * sm.S[S_M + cn][sL]) / dl;
-    const double v1r = (sm.P[Q_M + cn][rR] - dx2 * sm.S[S_M + cn][sR]) / dr;
-    const double v2l = (sm.P[Q_M + c1][rL] + dx1 * sm.S[S_M + c1][sL]) / dl;
-    const double v2r = (sm.P[Q_M + c1][rR] - dx2 * sm.S[S_M + c1][sR]) / dr;
-    const double v3l = (sm.P[Q_M + c2][rL] + dx1 * sm.S[S_M + c2][sL]) / dl;
-    const double v3r = (sm.P[Q_M + c2][rR] - dx2 * sm.S[S_M + c2][sR]) / dr;
-    double b1l = 0.0, b1r = 0.0, b2l = 0.0, b2r = 0.0, b3l = 0.0, b3r = 0.0, phil = 0.0, phir = 0.0;
-    if (MAG) {
-      b1l = sm.P[Q_B + cn][rL] + dx1 * sm.S[S_B + cn][sL];
-      b1r = sm.P[Q_B + cn][rR] - dx2 * sm.S[S_B + cn][sR];
-      b2l = sm.P[Q_B + c1][rL] + dx1 * sm.S[S_B + c1][sL];
-      b2r = sm.P[Q_B + c1][rR] - dx2 * sm.S[S_B + c1][sR];
-      b3l = sm.P[Q_B + c2][rL] + dx1 * sm.S[S_B + c2][sL];
-      b3r = sm.P[Q_B + c2][rR] - dx2 * sm.S[S_B + c2][sR];
-      // phi is never reconstructed: its slope is identically zero (allocations.f90)
-      phil = sm.P[Q_PHI][rL] + dx1 * 0.0;
-      phir = sm.P[Q_PHI][rR] - dx2 * 0.0;
-    }
-    const double eil = get_eint<MAG>(el, dl, v1l, v2l, v3l, b1l, b2l, b3l);
-    const double eir = get_eint<MAG>(er, dr, v1r, v2r, v3r, b1r, b2r, b3r);
     double fl[9];
-    if (eil <= 0.0 || dl <= 0.0 || eir <= 0.0 || dr <= 0.0) {
+    if (!face_flux_fast<MAG, TL::NR>(&sm.P[0][rL], &sm.P[0][rR], &sm.S[0][sL], TL::NSB, &sm.S[0][sR], TL::NSB, dx1,
+                                     dx2, cn, c1, c2, A.gamma, A.gm1, ch, fl)) {
       int gi[3] = {t0[0] + fx, t0[1] + fy, t0[2] + fz};
       gi[AX] = gL;
       record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);  // numflux.f90:117 -> error_flux
-#pragma unroll
-      for (int q = 0; q < 9; q++) fl[q] = 0.0;
-    } else {
-      // eos_p_cs (eos.f90:209-219) with erad = 0
-      const double ptl0 = A.gm1 * eil, ptr0 = A.gm1 * eir;
-      const double csl = sqrt(A.gamma * ptl0 / dl), csr = sqrt(A.gamma * ptr0 / dr);
-      const double ptl = ptl0 + 0.5 * (b1l * b1l + b2l * b2l + b3l * b3l);
-      const double ptr = ptr0 + 0.5 * (b1r * b1r + b2r * b2r + b3r * b3r);
-      const double cfl = get_cf(dl, csl, b1l, b2l, b3l);
-      const double cfr = get_cf(dr, csr, b1r, b2r, b3r);
-      hlld(fl, cfl, cfr, v1l, v1r, v2l, v2r, v3l, v3r, dl, dr, el, er, ptl, ptr, b1l, b1r, b2l, b2r, b3l, b3r, phil,
-           phir, ch);
     }
     // rotate back into the conserved slots (numflux.f90:186-198, 359-371, 531-543)
     sm.F[ICNT][w] = fl[0];
@@ -373,7 +302,19 @@ __device__ __forceinline__ void stage_tile_exact(const GridDev& G, const StageAr
   }
   // primitive + pressure of the new state (rungekutta.f90:205-229, eos.f90:805-842)
   const double d = un[0];
-  const double v1 = un[1] / d, v2 = un[2] / d, v3 = un[3] / d;
+  double v1, v2, v3;
+  {
+    FastDiv fd;
+    const double rd = fd.rec(d);
+    v1 = fd.div(un[1], d, rd);
+    v2 = fd.div(un[2], d, rd);
+    v3 = fd.div(un[3], d, rd);
+    if (fd.bad) {
+      v1 = un[1] / d;
+      v2 = un[2] / d;
+      v3 = un[3] / d;
+    }
+  }
   const double b1 = MAG ? un[5] : 0.0, b2 = MAG ? un[6] : 0.0, b3 = MAG ? un[7] : 0.0;
   const double eint = get_eint<MAG>(un[4], d, v1, v2, v3, b1, b2, b3);
   double* Po = A.pout;
