@@ -42,6 +42,17 @@ __device__ __forceinline__ double rcp_approx(double b) {
   return y;
 }
 
+// 1/b within about one ulp, without branches (two Newton-Raphson steps from
+// the approximation); for the mixed-precision form, which is not bound to
+// IEEE quotients.  A zero b gives NaN where IEEE gives infinity.
+__device__ __forceinline__ double rcp_nr(double b) {
+  double y = rcp_approx(b);
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  return __fma_rn(y, e, y);
+}
+
 // RN(1/b); sets bad where b is out of range or has an all-ones significand
 __device__ __forceinline__ double recip_rn(double b, bool& bad) {
   const unsigned lo = (unsigned)__double2loint(b), hi = (unsigned)__double2hiint(b);

@@ -185,6 +185,9 @@ __device__ __forceinline__ bool z_face(const double* Wk, const double* Wk1, cons
   return ok;
 }
 
+// Ask for the line of p to be brought into L2 (no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.L2 [%0];" ::"l"(p)); }
+
 template <bool MAG, bool GLM, int LIM, class MT, bool PUSH>
 __global__ void __launch_bounds__(MT::NT, MT::MINB)
     march_stage_kernel(const __grid_constant__ GridDev G, const __grid_constant__ StageArgs A, int LZ, int ntx,
@@ -252,6 +255,29 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
     const double* Wk = &sm.W[slot(k)][0][0];
     const double* Wk1 = &sm.W[slot(k + 1)][0][0];
     const double* Wk2 = &sm.W[slot(k + 2)][0][0];
+    // ---- prefetch into L2 what phase 3 reads from HBM: the owners' U of
+    // cell k, the other threads' cells of plane k+3 (interior cells only)
+    if (live) {
+      const size_t c = cidx(G, x0 + oi, y0 + oj, k);
+#pragma unroll
+      for (int q = 0; q < nv; q++) {
+        prefetch_l2(A.uorg + q * pl + c);
+        if (A.ucur != A.uorg) prefetch_l2(A.ucur + q * pl + c);
+      }
+    } else if (!owner && k + 3 <= kend + 1 && k + 3 < G.n[2]) {
+      for (int w = h; w < MT::NPL; w += NH) {
+        int i, j;
+        MT::cell_of(w, i, j);
+        const int gi = x0 + i, gj = y0 + j;
+        const bool col = i >= 0 && i < T0 && j >= 0 && j < T1;
+        const bool ring = k + 3 < kend && ((i >= -2 && i < T0 + 2 && j >= 0 && j < T1) ||
+                                           (i >= 0 && i < T0 && j >= -2 && j < T1 + 2));
+        if (!(col || ring) || gi < 0 || gi >= G.n[0] || gj < 0 || gj >= G.n[1]) continue;
+        const size_t c = cidx(G, gi, gj, k + 3);
+#pragma unroll
+        for (int q = 0; q < NP; q++) prefetch_l2(A.pin + q * pl + c);
+      }
+    }
     // ---- phase 1: slopes --------------------------------------------------------
     // owners: the z slope of their column, then one x-y slope cell each (the
     // last NC of the list); the other threads: the rest of the list

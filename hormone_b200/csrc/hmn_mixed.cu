@@ -4,7 +4,9 @@
 // stage_kernel (hmn_kernels.cu), with the arithmetic split by what needs
 // double precision:
 //   * reconstruction in FP64, with the limiters' divisions by grid spacings
-//     replaced by products with precomputed reciprocals;
+//     replaced by products with precomputed reciprocals, and the FP64
+//     reciprocals of densities by two Newton-Raphson steps from the
+//     approximate reciprocal (within about one ulp, no branch);
 //   * pressure recovery eint = E - kinetic - magnetic in FP64, in the cells
 //     and on both sides of every face (high Mach / low beta cancellation);
 //   * the HLLD Riemann solver, the EOS and the fast speeds in FP32
@@ -21,6 +23,7 @@
 #include <cstdint>
 #include <cstring>
 
+#include "hmn_div.cuh"
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
 #include "hmn_tile.cuh"
@@ -120,7 +123,7 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
           R[q] = u1 + hr * du;
         }
       }
-      const double rdl = 1.0 / L[S_D], rdr = 1.0 / R[S_D];
+      const double rdl = rcp_nr(L[S_D]), rdr = rcp_nr(R[S_D]);
       double eintl = L[S_E] - 0.5 * (L[S_M] * L[S_M] + L[S_M + 1] * L[S_M + 1] + L[S_M + 2] * L[S_M + 2]) * rdl;
       double eintr = R[S_E] - 0.5 * (R[S_M] * R[S_M] + R[S_M + 1] * R[S_M + 1] + R[S_M + 2] * R[S_M + 2]) * rdr;
       if (MAG) {
@@ -157,7 +160,7 @@ __device__ __forceinline__ void axis_pass_mixed(const GridDev& G, const StageArg
     const double dr = sm.P[Q_D][rR] - dx2 * (double)sm.S[S_D][sR];
     const double el = sm.P[Q_E][rL] + dx1 * (double)sm.S[S_E][sL];
     const double er = sm.P[Q_E][rR] - dx2 * (double)sm.S[S_E][sR];
-    const double rdl = 1.0 / dl, rdr = 1.0 / dr;
+    const double rdl = rcp_nr(dl), rdr = rcp_nr(dr);
     const double v1l = (sm.P[Q_M + cn][rL] + dx1 * (double)sm.S[S_M + cn][sL]) * rdl;
     const double v1r = (sm.P[Q_M + cn][rR] - dx2 * (double)sm.S[S_M + cn][sR]) * rdr;
     const double v2l = (sm.P[Q_M + c1][rL] + dx1 * (double)sm.S[S_M + c1][sL]) * rdl;
@@ -340,7 +343,8 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
     A.uout[q * pl + c] = val;
   }
   const double d = un[0];
-  const double v1 = un[1] / d, v2 = un[2] / d, v3 = un[3] / d;
+  const double rd = rcp_nr(d);
+  const double v1 = un[1] * rd, v2 = un[2] * rd, v3 = un[3] * rd;
   const double b1 = MAG ? un[5] : 0.0, b2 = MAG ? un[6] : 0.0, b3 = MAG ? un[7] : 0.0;
   const double eint = get_eint<MAG>(un[4], d, v1, v2, v3, b1, b2, b3);
   double* Po = A.pout;
