@@ -443,6 +443,13 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     G.g[a].risum = base + 14 * L;
   }
   memcpy(G.bc, ctx->bc, sizeof(G.bc));
+  G.idx_rn = 1;
+  for (int a = 0; a < 3; a++)
+    for (int s = 2; s < ctx->n[a] + 3; s++) {
+      const double dx = grid->dx[a][s], m = std::fabs(dx);
+      if (!(grid->idx[a][s] == 1.0 / dx) || !(m >= std::ldexp(1.0, -500)) || !(m < std::ldexp(1.0, 501)))
+        G.idx_rn = 0;
+    }
   stage_tile(ctx->solve, par->precision, par->nspc, ctx->tile);
   for (int a = 0; a < 3; a++) ctx->tiles[a] = (ctx->n[a] + ctx->tile[a] - 1) / ctx->tile[a];
   setup_tma(ctx);

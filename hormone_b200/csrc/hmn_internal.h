@@ -82,6 +82,10 @@ struct GridDev {
   // (9 conserved slots, then the scalars), or nullptr
   const double* fb;
   SphGeo sph;
+  // 1 where, for every cell index c of the three axes, idx(c) = RN(1/dx(c))
+  // and dx(c) lies in [2^-500, 2^501) (checked on the host): the quotients
+  // by dx may then be corrected from idx without forming the reciprocal
+  int idx_rn;
 };
 
 // Device-resident scalars of one simulation: the CFL reduction slots, the

@@ -1116,24 +1116,13 @@ __device__ __forceinline__ double rdist(const GridDev& G, int i, int j, int k) {
 
 // one thread per cell of an x row segment; rows by (blockIdx.y, blockIdx.z)
 // = (j, k), so no index division
-__global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HGArgs A) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
-  if (i < G.n[0]) {
-    const size_t c = cidx(G, i, j, k);
-    const AxisGeo &gx = G.g[0], &gy = G.g[1], &gz = G.g[2];
-    double c0 = -((gx.idx[i + 2] + gx.idx[i + 3]) * gy.dxi[j + 2] * gz.dxi[k + 2] +
-                  (gy.idx[j + 2] + gy.idx[j + 3]) * gx.dxi[i + 2] * gz.dxi[k + 2] +
-                  (gz.idx[k + 2] + gz.idx[k + 3]) * gx.dxi[i + 2] * gy.dxi[j + 2]);
-    double cm[3], cp[3];
-    cm[0] = gy.dxi[j + 2] * gz.dxi[k + 2] / gx.dx[i + 2];
-    cp[0] = gy.dxi[j + 2] * gz.dxi[k + 2] / gx.dx[i + 3];
-    cm[1] = gx.dxi[i + 2] * gz.dxi[k + 2] / gy.dx[j + 2];
-    cp[1] = gx.dxi[i + 2] * gz.dxi[k + 2] / gy.dx[j + 3];
-    cm[2] = gx.dxi[i + 2] * gy.dxi[j + 2] / gz.dx[k + 2];
-    cp[2] = gx.dxi[i + 2] * gy.dxi[j + 2] / gz.dx[k + 3];
-    const int ijk[3] = {i, j, k};
-    // a z neighbour in the neighbouring slab comes from its halo layer
+// The Laplacian numerator of a cell on a face of the grid (or of a slab):
+// the Robin image phi ~ 1/r folded into the diagonal on a free face, the
+// periodic neighbour, or the neighbouring slab's layer (hg_stage_kernel).
+__device__ __forceinline__ double hg_boundary_lap(const GridDev& G, int i, int j, int k, size_t c, double c0,
+                                                  const double cm[3], const double cp[3], const double* ph) {
+  const int ijk[3] = {i, j, k};
+  // a z neighbour in the neighbouring slab comes from its halo layer
     const bool hlo = k == 0 && G.ghalo[0] != nullptr, hhi = k == G.n[2] - 1 && G.ghalo[1] != nullptr;
     bool use_m[3] = {true, true, true}, use_p[3] = {true, true, true};
     size_t nbm[3], nbp[3];
@@ -1161,8 +1150,6 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
       nbm[a] = use_m[a] && !hm ? cidx(G, m[0], m[1], m[2]) : c;
       nbp[a] = use_p[a] && !hp ? cidx(G, p[0], p[1], p[2]) : c;
     }
-    const double cn = gx.dxi[i + 2] * gy.dxi[j + 2] * gz.dxi[k + 2];
-    const double* ph = A.phi_in;
     const size_t hc = (size_t)i + (size_t)G.n[0] * j;
     double lap = c0 * ph[c];
 #pragma unroll
@@ -1170,7 +1157,63 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
       if (use_m[a]) lap = lap + cm[a] * (a == 2 && hlo ? G.ghalo[0][hc] : ph[nbm[a]]);
       if (use_p[a]) lap = lap + cp[a] * (a == 2 && hhi ? G.ghalo[1][hc] : ph[nbp[a]]);
     }
-    const double lapphi = lap / cn;
+    return lap;
+}
+
+__global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HGArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i < G.n[0]) {
+    const size_t c = cidx(G, i, j, k);
+    const AxisGeo &gx = G.g[0], &gy = G.g[1], &gz = G.g[2];
+    double c0 = -((gx.idx[i + 2] + gx.idx[i + 3]) * gy.dxi[j + 2] * gz.dxi[k + 2] +
+                  (gy.idx[j + 2] + gy.idx[j + 3]) * gx.dxi[i + 2] * gz.dxi[k + 2] +
+                  (gz.idx[k + 2] + gz.idx[k + 3]) * gx.dxi[i + 2] * gy.dxi[j + 2]);
+    double cm[3], cp[3];
+    // neighbour weights: area over centre spacing, each quotient corrected
+    // from idx = RN(1/dx) where the host vouched for it (FastDiv), else
+    // IEEE division -- the same bits either way
+    const double ayz = gy.dxi[j + 2] * gz.dxi[k + 2], axz = gx.dxi[i + 2] * gz.dxi[k + 2];
+    const double axy = gx.dxi[i + 2] * gy.dxi[j + 2];
+    bool slow = !G.idx_rn;
+    if (!slow) {
+      cm[0] = div_rn(ayz, gx.dx[i + 2], gx.idx[i + 2], slow);
+      cp[0] = div_rn(ayz, gx.dx[i + 3], gx.idx[i + 3], slow);
+      cm[1] = div_rn(axz, gy.dx[j + 2], gy.idx[j + 2], slow);
+      cp[1] = div_rn(axz, gy.dx[j + 3], gy.idx[j + 3], slow);
+      cm[2] = div_rn(axy, gz.dx[k + 2], gz.idx[k + 2], slow);
+      cp[2] = div_rn(axy, gz.dx[k + 3], gz.idx[k + 3], slow);
+    }
+    if (slow) {
+      cm[0] = ayz / gx.dx[i + 2];
+      cp[0] = ayz / gx.dx[i + 3];
+      cm[1] = axz / gy.dx[j + 2];
+      cp[1] = axz / gy.dx[j + 3];
+      cm[2] = axy / gz.dx[k + 2];
+      cp[2] = axy / gz.dx[k + 3];
+    }
+    const double cn = gx.dxi[i + 2] * gy.dxi[j + 2] * gz.dxi[k + 2];
+    const double* ph = A.phi_in;
+    double lap;
+    const size_t nx = (size_t)G.n[0], nxy = nx * (size_t)G.n[1];
+    if (i > 0 && i < G.n[0] - 1 && j > 0 && j < G.n[1] - 1 && k > 0 && k < G.n[2] - 1) {
+      // interior cell: every neighbour is a cell of this grid
+      lap = c0 * ph[c];
+      lap = lap + cm[0] * ph[c - 1];
+      lap = lap + cp[0] * ph[c + 1];
+      lap = lap + cm[1] * ph[c - nx];
+      lap = lap + cp[1] * ph[c + nx];
+      lap = lap + cm[2] * ph[c - nxy];
+      lap = lap + cp[2] * ph[c + nxy];
+    } else {
+      lap = hg_boundary_lap(G, i, j, k, c, c0, cm, cp, ph);
+    }
+    double lapphi;
+    {
+      FastDiv fd;
+      lapphi = fd.div(lap, cn, fd.rec(cn));
+      if (fd.bad) lapphi = lap / cn;
+    }
     const double hgsrc = A.fourpiG * A.dens[c];
     double o1, o2;
     const double phi0 = ph[c], psi0 = A.psi_in[c];
