@@ -72,6 +72,7 @@ struct hmn_ctx {
   double xi1s;
   // hmn_run's device loop as a CUDA graph of kRunGraphSteps steps, valid for
   // the primitive-buffer parity and phidamp factor it was captured with
+  unsigned int* small_bar;   // grid barrier of the persistent small-grid loop (2 words, lazily)
   cudaGraphExec_t run_exec;
   int run_pcur;
   double run_phifac;
@@ -469,6 +470,7 @@ extern "C" int hmn_destroy(hmn_ctx* ctx) {
   for (int b = 0; b < 3; b++) cudaFree(ctx->buf[b]);
   for (int b = 0; b < 2; b++) cudaFree(ctx->pbuf[b]);
   cudaFree(ctx->spcorg);
+  cudaFree(ctx->small_bar);
   for (int a = 0; a < 3; a++)
     for (int io = 0; io < 2; io++) cudaFree(ctx->dir[a][io]);
   cudaFree(ctx->fb);
@@ -815,6 +817,46 @@ static void rk_coeff(int iter, int type, double* faco, double* fact, double* fac
 
 // RK stage s (1..rktype) of the current step; the last stage also does the
 // step's buffer bookkeeping
+// The arguments of RK stage s (1-based) on the state in primitive buffer
+// pcur: buffer roles, RK coefficients, scalars (hydro.f90:35-41).
+static StageArgs stage_args(hmn_ctx* ctx, int s, int pcur) {
+  const int rk = ctx->par.rktype;
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  rk_coeff(s, rk, &a.faco, &a.fact, &a.facn);
+  a.uorg = ctx->buf[0];
+  a.pin = ctx->pbuf[pcur];
+  a.pout = ctx->pbuf[1 - pcur];
+  if (s == 1) {
+    a.phifac = ctx->phifac;
+    a.ucur = ctx->buf[0];
+    a.uout = ctx->buf[1];
+  } else if (s == 2) {
+    a.ucur = ctx->buf[1];
+    a.uout = rk == 2 ? ctx->buf[0] : ctx->buf[2];
+    a.phifac = 1.0;
+  } else {
+    a.ucur = ctx->buf[2];
+    a.uout = ctx->buf[0];
+    a.phifac = 1.0;
+  }
+  a.gphi = ctx->par.gravswitch == 3 ? ctx->gphi[ctx->gcur] : nullptr;
+  a.sc = ctx->sc;
+  a.plane = ctx->plane;
+  a.gamma = ctx->par.gamma;
+  a.gm1 = ctx->par.gamma - 1.0;
+  a.limiter = ctx->par.limiter;
+  a.nvar = ctx->nvar;
+  for (int d = 0; d < 3; d++) {
+    a.tile[d] = ctx->tile[d];
+    a.tiles[d] = ctx->tiles[d];
+  }
+  a.stage = s;
+  a.nspc = ctx->par.nspc;
+  a.spcorg = ctx->spcorg;
+  return a;
+}
+
 static int enqueue_stage(hmn_ctx* ctx, int s) {
   const int rk = ctx->par.rktype;
   for (int a = 0; a < 3; a++)
@@ -822,49 +864,14 @@ static int enqueue_stage(hmn_ctx* ctx, int s) {
       if (ctx->solve[a] && (ctx->bc[a][io][0] >= 9 || ctx->bc[a][io][1] >= 9) && !ctx->G.dir[a][io])
         return HMN_EBADCFG;  // codes 9 and 10 need hmn_set_dirichlet first
   if (ctx->solve[2] && ctx->bc[2][0][0] == 10 && !ctx->fb) return HMN_EBADCFG;  // and hmn_set_flux_boundary
-  double* A = ctx->buf[0];
-  double* B = ctx->buf[1];
-  double* C = ctx->buf[2];
   {
-    StageArgs a;
-    memset(&a, 0, sizeof(a));
-    rk_coeff(s, rk, &a.faco, &a.fact, &a.facn);
-    a.uorg = A;
-    a.pin = ctx->pbuf[ctx->pcur];
-    a.pout = ctx->pbuf[1 - ctx->pcur];
-    if (s == 1) {
-      a.phifac = ctx->phifac;
-      a.ucur = A;
-      a.uout = B;
-    } else if (s == 2) {
-      a.ucur = B;
-      a.uout = rk == 2 ? A : C;
-      a.phifac = 1.0;
-    } else {
-      a.ucur = C;
-      a.uout = A;
-      a.phifac = 1.0;
-    }
-    a.gphi = ctx->par.gravswitch == 3 ? ctx->gphi[ctx->gcur] : nullptr;
-    a.sc = ctx->sc;
-    a.plane = ctx->plane;
-    a.gamma = ctx->par.gamma;
-    a.gm1 = ctx->par.gamma - 1.0;
-    a.limiter = ctx->par.limiter;
-    a.nvar = ctx->nvar;
-    for (int d = 0; d < 3; d++) {
-      a.tile[d] = ctx->tile[d];
-      a.tiles[d] = ctx->tiles[d];
-    }
-    a.stage = s;
+    StageArgs a = stage_args(ctx, s, ctx->pcur);
     if (ctx->zpush_on) {  // read the halos of this parity, store into the other
       ctx->G.zhalo[0] = ctx->zrecv[0][ctx->zpar];
       ctx->G.zhalo[1] = ctx->zrecv[1][ctx->zpar];
       a.push[0] = ctx->zpush[0][ctx->zpar ^ 1];
       a.push[1] = ctx->zpush[1][ctx->zpar ^ 1];
     }
-    a.nspc = ctx->par.nspc;
-    a.spcorg = ctx->spcorg;
     const TmaMaps* tm = ctx->tma_ok ? &ctx->tmaps[ctx->pcur] : nullptr;
     if (ctx->par.precision == 1)
       CK(launch_stage_mixed(ctx->G, a, ctx->mag, ctx->glm, tm, ctx->st), "stage");
@@ -1462,6 +1469,68 @@ static int enqueue_step(hmn_ctx* ctx) {
   return HMN_OK;
 }
 
+// Grids of at most this many cells step in one persistent launch
+// (hmn_small.cu) instead of a chain of six launches per step.
+constexpr size_t kSmallCells = 65536;
+
+static bool small_run_ok(hmn_ctx* ctx) {
+  const char* e = getenv("HMN_SMALL");  // HMN_SMALL=0 keeps the per-phase launches
+  if (e && e[0] == '0') return false;
+  return ctx->par.precision == 0 && ctx->par.nspc == 0 && (ctx->par.rktype == 2 || ctx->par.rktype == 3) &&
+         !ctx->zpush_on && ctx->plane <= kSmallCells && small_run_supported(ctx->tile, ctx->G.sph.on != 0);
+}
+
+// Up to max_steps steps of the device loop in persistent launches of at
+// most 4096 steps each; the clock, dt and end test stay on the device.
+static int run_small(hmn_ctx* ctx, int max_steps) {
+  for (int a = 0; a < 3; a++)
+    for (int io = 0; io < 2; io++)
+      if (ctx->solve[a] && (ctx->bc[a][io][0] >= 9 || ctx->bc[a][io][1] >= 9) && !ctx->G.dir[a][io])
+        return HMN_EBADCFG;  // codes 9 and 10 need hmn_set_dirichlet first
+  if (ctx->solve[2] && ctx->bc[2][0][0] == 10 && !ctx->fb) return HMN_EBADCFG;
+  if (!ctx->small_bar) {
+    CK(cudaMalloc((void**)&ctx->small_bar, 2 * sizeof(unsigned int)), "barrier");
+    CK(cudaMemsetAsync(ctx->small_bar, 0, 2 * sizeof(unsigned int), ctx->st), "barrier");
+  }
+  const int rk = ctx->par.rktype;
+  SmallRun R;
+  memset(&R, 0, sizeof(R));
+  for (int p = 0; p < 2; p++)
+    for (int s = 1; s <= rk; s++) R.st[p][s - 1] = stage_args(ctx, s, (ctx->pcur + p + s - 1) & 1);
+  R.sc = ctx->sc;
+  R.bar = ctx->small_bar;
+  R.damp = ctx->glm ? std::exp(-ctx->par.alpha9wave * ctx->par.courant) : 1.0;
+  R.phifac0 = ctx->phifac;
+  R.rk = rk;
+  R.ntiles = ctx->tiles[0] * ctx->tiles[1] * ctx->tiles[2];
+  const int tn0 = ctx->sc_h->tn, pcur0 = ctx->pcur;
+  int left = max_steps;
+  while (left > 0) {
+    R.nsteps = left < 4096 ? left : 4096;
+    const int tn_before = ctx->sc_h->tn;
+    int grid = 0;
+    CK(launch_small_run(ctx->G, R, ctx->mag != 0, ctx->glm != 0, ctx->G.sph.on != 0, ctx->tile, ctx->st, &grid),
+       "small run");
+    ctx->launches += 1;
+    const int rc = fetch_scalars(ctx);
+    if (rc) {
+      ctx->pcur = (pcur0 + rk * (ctx->sc_h->tn - tn0)) & 1;
+      return rc;
+    }
+    const int ran = ctx->sc_h->tn - tn_before;
+    if (ran > 0) R.phifac0 = R.damp;  // the next launch's first step follows a step of this one
+    // the parity of the primitive buffer moves with the steps that ran
+    for (int p = 0; p < 2; p++)
+      for (int s = 1; s <= rk; s++)
+        R.st[p][s - 1] = stage_args(ctx, s, (pcur0 + rk * (ctx->sc_h->tn - tn0) + p + s - 1) & 1);
+    if (ctx->sc_h->err_code || ctx->sc_h->done || ran < R.nsteps) break;
+    left -= R.nsteps;
+  }
+  ctx->pcur = (pcur0 + rk * (ctx->sc_h->tn - tn0)) & 1;
+  if (ctx->sc_h->tn > tn0) ctx->phifac = R.damp;
+  return HMN_OK;
+}
+
 // kRunGraphSteps steps of the device loop as one graph launch.  Steps are
 // launch-bound on small grids (a few microseconds of work per kernel); the
 // graph removes the per-launch host cost.  The step count is even so that
@@ -1528,6 +1597,13 @@ extern "C" int hmn_run(hmn_ctx* ctx, double* time, double t_end, int max_steps, 
   if (rc) return rc;
   const int tn0 = ctx->sc_h->tn;
   const int pcur0 = ctx->pcur;
+  if (small_run_ok(ctx)) {
+    rc = run_small(ctx, max_steps);
+    if (rc) return rc;
+    *time = ctx->sc_h->time;
+    if (steps) *steps = ctx->sc_h->tn - tn0;
+    return HMN_OK;
+  }
   int done = 0;
   const bool graphs = ctx->par.rktype != 1;  // rktype 1 swaps buffers on the host after each step
   const int chunk = graphs ? kRunGraphSteps : 1;

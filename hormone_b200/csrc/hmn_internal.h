@@ -128,6 +128,17 @@ struct StageArgs {
   double* push[2];
 };
 
+// Several whole steps of a small grid in one persistent launch
+// (hmn_small.cu: small_run_kernel).
+struct SmallRun {
+  StageArgs st[2][3];   // [primitive buffer of the step's state][RK stage - 1]
+  DevScalars* sc;
+  unsigned int* bar;    // grid barrier: arrivals, generation (zero before the first use)
+  double phifac0;       // pending phidamp factor for the first step's stage 1
+  double damp;          // the factor of every later step's stage 1 (1 without GLM)
+  int nsteps, ntiles, rk;
+};
+
 // Arguments of one hyperbolic-gravity RK stage (hmn_kernels.cu: hg_stage_kernel).
 struct HGArgs {
   const double* phi_in;
@@ -184,6 +195,11 @@ cudaError_t launch_stage_march(const GridDev& G, const StageArgs& A, bool mag, b
 bool march_enabled();
 // its decomposition: z planes per chunk, column tiles along x and y, chunks
 void march_chunks(const int n[3], int* lz, int* ntx, int* nty, int* nch);
+// up to R.nsteps steps of a small grid in one cooperative launch of at most
+// one CTA per tile (hmn_small.cu); *grid receives the CTA count
+int small_run_supported(const int tile[3], bool sph);
+cudaError_t launch_small_run(const GridDev& G, const SmallRun& R, bool mag, bool glm, bool sph, const int tile[3],
+                             cudaStream_t st, int* grid);
 // mixed precision (hmn_mixed.cu): FP32 Riemann solver, FP64 reconstruction and accumulation
 cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                                cudaStream_t st);
