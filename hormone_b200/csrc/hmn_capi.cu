@@ -73,6 +73,8 @@ struct hmn_ctx {
   // hmn_run's device loop as a CUDA graph of kRunGraphSteps steps, valid for
   // the primitive-buffer parity and phidamp factor it was captured with
   unsigned int* small_bar;   // grid barrier of the persistent small-grid loop (2 words, lazily)
+  int hg_uni, hg_urcn_ok;    // uniform Cartesian grid: the gravity stage's constant Laplacian weights
+  double hg_c0, hg_cm[3], hg_cp[3], hg_cn, hg_rcn;
   cudaGraphExec_t run_exec;
   int run_pcur;
   double run_phifac;
@@ -444,6 +446,33 @@ extern "C" int hmn_create(const hmn_grid* grid, const hmn_params* par, hmn_ctx**
     G.g[a].risum = base + 14 * L;
   }
   memcpy(G.bc, ctx->bc, sizeof(G.bc));
+  // a Cartesian grid uniform along every axis gives every cell the same
+  // Laplacian weights in the gravity stage: form them once, in the kernel's
+  // operation order (hg_stage_kernel)
+  ctx->hg_uni = 1;
+  for (int a = 0; a < 3; a++) {
+    const int n = ctx->n[a];
+    for (int s = 2; s <= n + 2; s++)
+      if (grid->dx[a][s] != grid->dx[a][2] || grid->idx[a][s] != grid->idx[a][2]) ctx->hg_uni = 0;
+    for (int s = 2; s <= n + 1; s++)
+      if (grid->dxi[a][s] != grid->dxi[a][2]) ctx->hg_uni = 0;
+  }
+  if (ctx->hg_uni) {
+    const double dxi0 = grid->dxi[0][2], dxi1 = grid->dxi[1][2], dxi2 = grid->dxi[2][2];
+    const double i0 = grid->idx[0][2], i1 = grid->idx[1][2], i2 = grid->idx[2][2];
+    ctx->hg_c0 = -((i0 + i0) * dxi1 * dxi2 + (i1 + i1) * dxi0 * dxi2 + (i2 + i2) * dxi0 * dxi1);
+    const double ayz = dxi1 * dxi2, axz = dxi0 * dxi2, axy = dxi0 * dxi1;
+    ctx->hg_cm[0] = ayz / grid->dx[0][2];
+    ctx->hg_cp[0] = ayz / grid->dx[0][3];
+    ctx->hg_cm[1] = axz / grid->dx[1][2];
+    ctx->hg_cp[1] = axz / grid->dx[1][3];
+    ctx->hg_cm[2] = axy / grid->dx[2][2];
+    ctx->hg_cp[2] = axy / grid->dx[2][3];
+    ctx->hg_cn = dxi0 * dxi1 * dxi2;
+    ctx->hg_rcn = 1.0 / ctx->hg_cn;
+    const double m = std::fabs(ctx->hg_cn);
+    ctx->hg_urcn_ok = m >= std::ldexp(1.0, -500) && m < std::ldexp(1.0, 501);
+  }
   G.idx_rn = 1;
   for (int a = 0; a < 3; a++)
     for (int s = 2; s < ctx->n[a] + 3; s++) {
@@ -1193,6 +1222,15 @@ extern "C" int hmn_gravity_substage(hmn_ctx* ctx) {
   a.sc = ctx->sc;
   a.lc = ctx->hgc;
   a.gin = ctx->gin;
+  a.uni = ctx->hg_uni && !ctx->G.sph.on;
+  a.urcn_ok = ctx->hg_urcn_ok;
+  a.uc0 = ctx->hg_c0;
+  for (int d = 0; d < 3; d++) {
+    a.ucm[d] = ctx->hg_cm[d];
+    a.ucp[d] = ctx->hg_cp[d];
+  }
+  a.ucn = ctx->hg_cn;
+  a.urcn = ctx->hg_rcn;
   if (ctx->G.sph.on)
     CK(launch_hg_stage_sph(ctx->G, a, ctx->st), "hg stage");
   else

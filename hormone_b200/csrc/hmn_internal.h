@@ -159,6 +159,12 @@ struct HGArgs {
   // the potential beyond r = xi1s as the last boundary pass left it
   const double* lc;
   const double* gin;
+  // Cartesian grids uniform along every axis: the Laplacian weights every
+  // cell would form (c0, the -/+ neighbour weights of each axis, the cell
+  // volume cn) and RN(1/cn), formed once on the host with the same IEEE
+  // operations; urcn_ok where cn lies in [2^-500, 2^501)
+  int uni, urcn_ok;
+  double uc0, ucm[3], ucp[3], ucn, urcn;
 };
 
 // One simulation of a batch, resident in device memory.  Every field the

@@ -742,10 +742,19 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
   if (i < G.n[0]) {
     const size_t c = cidx(G, i, j, k);
     const AxisGeo &gx = G.g[0], &gy = G.g[1], &gz = G.g[2];
-    double c0 = -((gx.idx[i + 2] + gx.idx[i + 3]) * gy.dxi[j + 2] * gz.dxi[k + 2] +
-                  (gy.idx[j + 2] + gy.idx[j + 3]) * gx.dxi[i + 2] * gz.dxi[k + 2] +
-                  (gz.idx[k + 2] + gz.idx[k + 3]) * gx.dxi[i + 2] * gy.dxi[j + 2]);
-    double cm[3], cp[3];
+    double c0, cm[3], cp[3], cn;
+    if (A.uni) {  // every cell's weights are these (formed on the host in this order)
+      c0 = A.uc0;
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        cm[a] = A.ucm[a];
+        cp[a] = A.ucp[a];
+      }
+      cn = A.ucn;
+    } else {
+    c0 = -((gx.idx[i + 2] + gx.idx[i + 3]) * gy.dxi[j + 2] * gz.dxi[k + 2] +
+           (gy.idx[j + 2] + gy.idx[j + 3]) * gx.dxi[i + 2] * gz.dxi[k + 2] +
+           (gz.idx[k + 2] + gz.idx[k + 3]) * gx.dxi[i + 2] * gy.dxi[j + 2]);
     // neighbour weights: area over centre spacing, each quotient corrected
     // from idx = RN(1/dx) where the host vouched for it (FastDiv), else
     // IEEE division -- the same bits either way
@@ -768,7 +777,8 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
       cm[2] = axy / gz.dx[k + 2];
       cp[2] = axy / gz.dx[k + 3];
     }
-    const double cn = gx.dxi[i + 2] * gy.dxi[j + 2] * gz.dxi[k + 2];
+    cn = gx.dxi[i + 2] * gy.dxi[j + 2] * gz.dxi[k + 2];
+    }
     const double* ph = A.phi_in;
     double lap;
     const size_t nx = (size_t)G.n[0], nxy = nx * (size_t)G.n[1];
@@ -785,7 +795,11 @@ __global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HG
       lap = hg_boundary_lap(G, i, j, k, c, c0, cm, cp, ph);
     }
     double lapphi;
-    {
+    if (A.uni && A.urcn_ok) {
+      bool bad = false;
+      lapphi = div_rn(lap, cn, A.urcn, bad);
+      if (bad) lapphi = lap / cn;
+    } else {
       FastDiv fd;
       lapphi = fd.div(lap, cn, fd.rec(cn));
       if (fd.bad) lapphi = lap / cn;
