@@ -268,6 +268,21 @@ __device__ __forceinline__ void stage_tile_mixed(const GridDev& G, const StageAr
     t0[a] = ti * TT[a];
     T[a] = min(TT[a], G.n[a] - t0[a]);
   }
+  {  // ask L2 for the U this thread's epilogue reads, while the axis passes run
+    const int tid0 = threadIdx.x;
+    if (tid0 < TL::NC) {
+      const int cx = tid0 % TL::TX, cy = (tid0 / TL::TX) % TL::TY, cz = tid0 / (TL::TX * TL::TY);
+      if (cx < T[0] && cy < T[1] && cz < T[2]) {
+        const size_t c = cidx(G, t0[0] + cx, t0[1] + cy, t0[2] + cz);
+        constexpr int nvp = MAG ? (GLM ? 9 : 8) : 5;
+#pragma unroll
+        for (int q = 0; q < nvp; q++) {
+          asm volatile("prefetch.L2 [%0];" ::"l"(A.uorg + q * A.plane + c));
+          if (A.ucur != A.uorg) asm volatile("prefetch.L2 [%0];" ::"l"(A.ucur + q * A.plane + c));
+        }
+      }
+    }
+  }
   stage_region<MAG, GLM, TL>(G, A, sm.P, &sm.bar, tm, t0, T);
   double acc[9];
 #pragma unroll
