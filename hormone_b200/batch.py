@@ -31,6 +31,7 @@ def _bind(L):
     L.hmn_batch_poll.argtypes = [_P, capi._DP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]
     L.hmn_batch_download.argtypes = [_P, _I, capi._DP, capi._DPP]
     L.hmn_batch_set_schedule.argtypes = [_P, _I, _I, _I]
+    L.hmn_batch_set_sweep.argtypes = [_P, _I, _I]
     L.hmn_batch_launch_count.argtypes = [_P]
     L.hmn_batch_launch_count.restype = ctypes.c_longlong
     L.hmn_batch_sync.argtypes = [_P]
@@ -38,8 +39,8 @@ def _bind(L):
     L.hmn_batch_stream.restype = _P
     L.hmn_batch_destroy.argtypes = [_P]
     for n in ("hmn_batch_create", "hmn_batch_add", "hmn_batch_remove", "hmn_batch_step", "hmn_batch_poll",
-              "hmn_batch_download", "hmn_batch_set_schedule", "hmn_batch_sync", "hmn_batch_destroy",
-              "hmn_batch_set_held"):
+              "hmn_batch_download", "hmn_batch_set_schedule", "hmn_batch_set_sweep", "hmn_batch_sync",
+              "hmn_batch_destroy", "hmn_batch_set_held"):
         getattr(L, n).restype = _I
     L._hmn_batch_bound = True
     return L
@@ -160,6 +161,14 @@ class Batch:
         rc = capi.lib().hmn_batch_set_schedule(self.h, int(kind), int(tile_id), int(blocks_per_sm))
         if rc != 0:
             raise capi.HmnError(rc, "hmn_batch_set_schedule")
+
+    def set_sweep(self, kind: int, sweep: int):
+        """Work-list order and CTA split of kind's stage launches: 0 static
+        (slot order), 1 interleaved across simulations, 2 dynamic (largest
+        simulations first, CTAs take items from a shared counter)."""
+        rc = capi.lib().hmn_batch_set_sweep(self.h, int(kind), int(sweep))
+        if rc != 0:
+            raise capi.HmnError(rc, "hmn_batch_set_sweep")
 
     def sync(self):
         capi.lib().hmn_batch_sync(self.h)

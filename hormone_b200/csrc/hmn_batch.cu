@@ -39,6 +39,7 @@ struct Klass {
   bool mag, glm;
   int first, count;  // range in the item list
   int grid;          // persistent CTAs of the stage launches
+  bool dynamic;      // stage launches take items from the shared counter
 };
 
 constexpr size_t kAlign = 256;
@@ -64,6 +65,8 @@ struct hmn_batch {
   int nsm = 148;
   int blocks_per_sm[3] = {0, 0, 0};  // per tile kind; 0: occupancy-derived persistent grid
   int tile_id[3] = {0, 2, 4};         // tile of each kind (batch_tile_variants)
+  int sweep[3] = {HMN_SWEEP_STATIC, HMN_SWEEP_STATIC, HMN_SWEEP_STATIC};  // item order and split per kind
+  int* d_queue = nullptr;             // {next item, CTAs finished} of a dynamic stage launch
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;
   double* stage_h = nullptr;
@@ -143,6 +146,8 @@ extern "C" int hmn_batch_create(size_t pool_bytes, int max_sims, int precision, 
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->pool, b->pool_bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_sims, (size_t)max_sims * sizeof(SimDesc));
   if (e == cudaSuccess) e = cudaMemset(b->d_sims, 0, (size_t)max_sims * sizeof(SimDesc));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_queue, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_queue, 0, 2 * sizeof(int));
   if (e != cudaSuccess) {
     int rc = cuda_fail(e, "batch create");
     hmn_batch_destroy(b);
@@ -163,6 +168,7 @@ extern "C" int hmn_batch_destroy(hmn_batch* b) {
   cudaFree(b->pool);
   cudaFree(b->d_sims);
   cudaFree(b->d_items);
+  cudaFree(b->d_queue);
   if (b->stage_h) cudaFreeHost(b->stage_h);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
@@ -400,13 +406,28 @@ static int rebuild(hmn_batch* b) {
   for (int kind = 0; kind < 3; kind++)  // the tile kinds of batch_tile_kind
     for (int m = 0; m < 3; m++) {
       const bool mag = m > 0, glm = m == 2;
-      Klass k{kind, mag, glm, (int)items.size(), 0, 0};
+      const int sweep = b->sweep[kind];
+      Klass k{kind, mag, glm, (int)items.size(), 0, 0, sweep == HMN_SWEEP_DYNAMIC};
+      std::vector<int> sims;
+      int most = 0;
       for (int s = 0; s < b->max_sims; s++) {
         const SlotInfo& si = b->slots[s];
         if (!si.used || si.kind != kind || si.mag != mag || si.glm != glm || b->h_sims[s].sc.done ||
             b->h_sims[s].held)
           continue;
-        for (int t = 0; t < si.ntiles; t++) items.push_back(make_int2(s, t));
+        sims.push_back(s);
+        most = std::max(most, si.ntiles);
+      }
+      if (sweep == HMN_SWEEP_INTERLEAVED) {  // tile t of every simulation, then tile t + 1
+        for (int t = 0; t < most; t++)
+          for (int s : sims)
+            if (t < b->slots[s].ntiles) items.push_back(make_int2(s, t));
+      } else {
+        if (sweep == HMN_SWEEP_DYNAMIC)  // the largest simulations first
+          std::stable_sort(sims.begin(), sims.end(),
+                           [b](int x, int y) { return b->slots[x].ntiles > b->slots[y].ntiles; });
+        for (int s : sims)
+          for (int t = 0; t < b->slots[s].ntiles; t++) items.push_back(make_int2(s, t));
       }
       k.count = (int)items.size() - k.first;
       if (k.count) {
@@ -449,7 +470,7 @@ static int enqueue_step(hmn_batch* b, long long* nlaunch) {
     for (const Klass& k : b->classes) {
       BCK(launch_batch_stage(b->d_sims, b->d_items + k.first, k.count, b->tile_id[k.kind], k.mag, k.glm, s,
                              b->rktype,
-                             b->precision, k.grid, b->st),
+                             b->precision, k.grid, k.dynamic ? b->d_queue : nullptr, b->st),
           "batch stage");
       (*nlaunch)++;
     }
@@ -570,6 +591,15 @@ extern "C" int hmn_batch_set_schedule(hmn_batch* b, int kind, int tile_id, int b
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+  return HMN_OK;
+}
+
+extern "C" int hmn_batch_set_sweep(hmn_batch* b, int kind, int sweep) {
+  if (!b || kind < 0 || kind > 2 || sweep < HMN_SWEEP_STATIC || sweep > HMN_SWEEP_DYNAMIC) return HMN_EINVAL;
+  BCK(cudaStreamSynchronize(b->st), "sync");
+  if (sweep == b->sweep[kind]) return HMN_OK;
+  b->sweep[kind] = sweep;
+  b->dirty = true;  // the next step rebuilds the work list and its graph
   return HMN_OK;
 }
 

@@ -231,7 +231,9 @@ constexpr int kEvoQ = 10;
 cudaError_t launch_evo(const GridDev& G, const double* P, size_t plane, const double* gphi, const double* sinc,
                        double* part, int nblocks, double* out, cudaStream_t st);
 // batched launchers over a work list of (sim, tile) items; tile_kind selects
-// the compile-time tile (see batch_tile_kind), grid = persistent CTAs
+// the compile-time tile (see batch_tile_kind), grid = persistent CTAs; the
+// stage launchers' queue is null for the static item split or a self-
+// resetting {next item, CTAs finished} counter pair (hmn_queue.cuh)
 int batch_tile_kind(const int solve[3]);
 int batch_tile_variants(int kind, int* tile_ids);
 void batch_tile_shape(int tile_id, int tile[3]);
@@ -239,10 +241,10 @@ cudaError_t launch_batch_cfl(SimDesc* sims, const int2* items, int nitems, int k
                              cudaStream_t st);
 cudaError_t launch_batch_finalize(SimDesc* sims, int nsims, cudaStream_t st);
 cudaError_t launch_batch_stage(SimDesc* sims, const int2* items, int nitems, int kind, bool mag, bool glm,
-                               int stage, int rk, int precision, int grid, cudaStream_t st);
+                               int stage, int rk, int precision, int grid, int* queue, cudaStream_t st);
 cudaError_t launch_batch_advance(SimDesc* sims, int nsims, cudaStream_t st);
 int batch_stage_blocks_per_sm(int kind, bool mag, bool glm, int precision);
 cudaError_t launch_batch_stage_mixed(SimDesc* sims, const int2* items, int nitems, int kind, bool mag, bool glm,
-                                     int stage, int rk, int grid, cudaStream_t st);
+                                     int stage, int rk, int grid, int* queue, cudaStream_t st);
 int batch_stage_mixed_blocks_per_sm(int kind, bool mag, bool glm);
 }  // namespace hmn

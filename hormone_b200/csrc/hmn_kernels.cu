@@ -34,6 +34,7 @@
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
 #include "hmn_stage.cuh"
+#include "hmn_queue.cuh"
 #include "hmn_tile.cuh"
 
 namespace hmn {
@@ -507,19 +508,19 @@ void batch_tile_shape(int tid, int tile[3]) {
   for (int a = 0; a < 3; a++) tile[a] = shapes[tid][a];
 }
 
-template <bool MAG, bool GLM, class TL>
+template <bool MAG, bool GLM, class TL, bool DYN>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel(SimDesc* sims, const int2* items, int nitems,
-                                                                        int stage, int rk) {
+                                                                        int stage, int rk, int* queue) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+  for_each_item<DYN>(nitems, queue, [&](int it) {
     const int2 w = items[it];
     SimDesc& S = sims[w.x];
-    if (!S.active || S.sc.done) continue;
+    if (!S.active || S.sc.done) return;
     const StageArgs A = batch_stage_args(S, stage, rk);
     stage_tile_exact<MAG, GLM, TL>(S.G, A, sm, w.y, nullptr);
     __syncthreads();
-  }
+  });
 }
 
 template <bool MAG, class TL>
@@ -584,8 +585,11 @@ template <bool MAG, bool GLM, class TL>
 static cudaError_t batch_attr_t() {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel<MAG, GLM, TL>,
+    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel<MAG, GLM, TL, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemT<TL>));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(batch_stage_kernel<MAG, GLM, TL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(SmemT<TL>));
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -594,30 +598,36 @@ static cudaError_t batch_attr_t() {
 
 template <bool MAG, bool GLM, class TL>
 static cudaError_t launch_batch_stage_t(SimDesc* sims, const int2* items, int nitems, int stage, int rk, int grid,
-                                        cudaStream_t st) {
+                                        int* queue, cudaStream_t st) {
   cudaError_t e = batch_attr_t<MAG, GLM, TL>();
   if (e != cudaSuccess) return e;
-  batch_stage_kernel<MAG, GLM, TL><<<grid, TL::NT, sizeof(SmemT<TL>), st>>>(sims, items, nitems, stage, rk);
+  if (queue)
+    batch_stage_kernel<MAG, GLM, TL, true>
+        <<<grid, TL::NT, sizeof(SmemT<TL>), st>>>(sims, items, nitems, stage, rk, queue);
+  else
+    batch_stage_kernel<MAG, GLM, TL, false>
+        <<<grid, TL::NT, sizeof(SmemT<TL>), st>>>(sims, items, nitems, stage, rk, nullptr);
   return cudaGetLastError();
 }
 
 template <class TL>
 static cudaError_t launch_batch_stage_tl(SimDesc* sims, const int2* items, int nitems, bool mag, bool glm, int stage,
-                                         int rk, int grid, cudaStream_t st) {
-  if (mag && glm) return launch_batch_stage_t<true, true, TL>(sims, items, nitems, stage, rk, grid, st);
-  if (mag) return launch_batch_stage_t<true, false, TL>(sims, items, nitems, stage, rk, grid, st);
-  return launch_batch_stage_t<false, false, TL>(sims, items, nitems, stage, rk, grid, st);
+                                         int rk, int grid, int* queue, cudaStream_t st) {
+  if (mag && glm) return launch_batch_stage_t<true, true, TL>(sims, items, nitems, stage, rk, grid, queue, st);
+  if (mag) return launch_batch_stage_t<true, false, TL>(sims, items, nitems, stage, rk, grid, queue, st);
+  return launch_batch_stage_t<false, false, TL>(sims, items, nitems, stage, rk, grid, queue, st);
 }
 
 cudaError_t launch_batch_stage(SimDesc* sims, const int2* items, int nitems, int tid, bool mag, bool glm, int stage,
-                               int rk, int precision, int grid, cudaStream_t st) {
-  if (precision == 1) return launch_batch_stage_mixed(sims, items, nitems, tid, mag, glm, stage, rk, grid, st);
+                               int rk, int precision, int grid, int* queue, cudaStream_t st) {
+  if (precision == 1)
+    return launch_batch_stage_mixed(sims, items, nitems, tid, mag, glm, stage, rk, grid, queue, st);
   switch (tid) {
-    case 0: return launch_batch_stage_tl<T3D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 1: return launch_batch_stage_tl<T3D4>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 2: return launch_batch_stage_tl<T2D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 3: return launch_batch_stage_tl<T2D8>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 4: return launch_batch_stage_tl<T1D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 0: return launch_batch_stage_tl<T3D>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 1: return launch_batch_stage_tl<T3D4>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 2: return launch_batch_stage_tl<T2D>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 3: return launch_batch_stage_tl<T2D8>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 4: return launch_batch_stage_tl<T1D>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -626,7 +636,8 @@ template <bool MAG, bool GLM, class TL>
 static int occupancy_t() {
   int n = 0;
   batch_attr_t<MAG, GLM, TL>();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_stage_kernel<MAG, GLM, TL>, TL::NT, sizeof(SmemT<TL>));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_stage_kernel<MAG, GLM, TL, true>, TL::NT,
+                                                sizeof(SmemT<TL>));  // the static split's shared memory is no larger
   return n > 0 ? n : 1;
 }
 

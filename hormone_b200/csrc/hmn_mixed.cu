@@ -26,6 +26,7 @@
 #include "hmn_div.cuh"
 #include "hmn_internal.h"
 #include "hmn_math.cuh"
+#include "hmn_queue.cuh"
 #include "hmn_tile.cuh"
 
 namespace hmn {
@@ -516,19 +517,20 @@ cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, b
 }
 
 // batched form (see batch_stage_kernel in hmn_kernels.cu)
-template <bool MAG, bool GLM, class TL>
+template <bool MAG, bool GLM, class TL, bool DYN>
 __global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel_mixed(SimDesc* sims, const int2* items,
-                                                                              int nitems, int stage, int rk) {
+                                                                              int nitems, int stage, int rk,
+                                                                              int* queue) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   SmemMixed<TL>& sm = *reinterpret_cast<SmemMixed<TL>*>(smem_raw);
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+  for_each_item<DYN>(nitems, queue, [&](int it) {
     const int2 w = items[it];
     SimDesc& S = sims[w.x];
-    if (!S.active || S.sc.done) continue;
+    if (!S.active || S.sc.done) return;
     const StageArgs A = batch_stage_args(S, stage, rk);
     stage_tile_mixed<MAG, GLM, TL>(S.G, A, sm, w.y, nullptr);
     __syncthreads();
-  }
+  });
 }
 
 using M3D = Tile<8, 8, 8, 640, 1>;
@@ -541,8 +543,11 @@ template <bool MAG, bool GLM, class TL>
 static cudaError_t bm_attr_t() {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel_mixed<MAG, GLM, TL>,
+    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel_mixed<MAG, GLM, TL, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemMixed<TL>));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(batch_stage_kernel_mixed<MAG, GLM, TL, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemMixed<TL>));
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -551,29 +556,34 @@ static cudaError_t bm_attr_t() {
 
 template <bool MAG, bool GLM, class TL>
 static cudaError_t launch_bm_t(SimDesc* sims, const int2* items, int nitems, int stage, int rk, int grid,
-                               cudaStream_t st) {
+                               int* queue, cudaStream_t st) {
   cudaError_t e = bm_attr_t<MAG, GLM, TL>();
   if (e != cudaSuccess) return e;
-  batch_stage_kernel_mixed<MAG, GLM, TL><<<grid, TL::NT, sizeof(SmemMixed<TL>), st>>>(sims, items, nitems, stage, rk);
+  if (queue)
+    batch_stage_kernel_mixed<MAG, GLM, TL, true>
+        <<<grid, TL::NT, sizeof(SmemMixed<TL>), st>>>(sims, items, nitems, stage, rk, queue);
+  else
+    batch_stage_kernel_mixed<MAG, GLM, TL, false>
+        <<<grid, TL::NT, sizeof(SmemMixed<TL>), st>>>(sims, items, nitems, stage, rk, nullptr);
   return cudaGetLastError();
 }
 
 template <class TL>
 static cudaError_t launch_bm_tl(SimDesc* sims, const int2* items, int nitems, bool mag, bool glm, int stage, int rk,
-                                int grid, cudaStream_t st) {
-  if (mag && glm) return launch_bm_t<true, true, TL>(sims, items, nitems, stage, rk, grid, st);
-  if (mag) return launch_bm_t<true, false, TL>(sims, items, nitems, stage, rk, grid, st);
-  return launch_bm_t<false, false, TL>(sims, items, nitems, stage, rk, grid, st);
+                                int grid, int* queue, cudaStream_t st) {
+  if (mag && glm) return launch_bm_t<true, true, TL>(sims, items, nitems, stage, rk, grid, queue, st);
+  if (mag) return launch_bm_t<true, false, TL>(sims, items, nitems, stage, rk, grid, queue, st);
+  return launch_bm_t<false, false, TL>(sims, items, nitems, stage, rk, grid, queue, st);
 }
 
 cudaError_t launch_batch_stage_mixed(SimDesc* sims, const int2* items, int nitems, int tid, bool mag, bool glm,
-                                     int stage, int rk, int grid, cudaStream_t st) {
+                                     int stage, int rk, int grid, int* queue, cudaStream_t st) {
   switch (tid) {
-    case 0: return launch_bm_tl<M3D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 1: return launch_bm_tl<M3D4>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 2: return launch_bm_tl<M2D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 3: return launch_bm_tl<M2D8>(sims, items, nitems, mag, glm, stage, rk, grid, st);
-    case 4: return launch_bm_tl<M1D>(sims, items, nitems, mag, glm, stage, rk, grid, st);
+    case 0: return launch_bm_tl<M3D>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 1: return launch_bm_tl<M3D4>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 2: return launch_bm_tl<M2D>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 3: return launch_bm_tl<M2D8>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
+    case 4: return launch_bm_tl<M1D>(sims, items, nitems, mag, glm, stage, rk, grid, queue, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -582,8 +592,8 @@ template <bool MAG, bool GLM, class TL>
 static int occ_m() {
   int n = 0;
   bm_attr_t<MAG, GLM, TL>();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_stage_kernel_mixed<MAG, GLM, TL>, TL::NT,
-                                                sizeof(SmemMixed<TL>));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_stage_kernel_mixed<MAG, GLM, TL, true>, TL::NT,
+                                                sizeof(SmemMixed<TL>));  // the static split's is no larger
   return n > 0 ? n : 1;
 }
 

@@ -346,6 +346,20 @@ int hmn_batch_download(hmn_batch* b, int sim, double* u, double* const prim[9]);
  * it; results do not depend on it. */
 int hmn_batch_set_schedule(hmn_batch* b, int kind, int tile_id, int blocks_per_sm);
 
+/* Sweep schedule of one grid kind's stage launches: the order of the
+ * (simulation, tile) work list and how the persistent CTAs split it.
+ *   HMN_SWEEP_STATIC       simulations in slot order, each one's tiles x
+ *                          fastest; CTA b takes items b, b + grid, ...
+ *   HMN_SWEEP_INTERLEAVED  tile t of every simulation, then tile t + 1;
+ *                          static split
+ *   HMN_SWEEP_DYNAMIC      the largest simulations first; CTAs take the
+ *                          next item from a shared counter
+ * The autotuner sets it; results do not depend on it. */
+#define HMN_SWEEP_STATIC 0
+#define HMN_SWEEP_INTERLEAVED 1
+#define HMN_SWEEP_DYNAMIC 2
+int hmn_batch_set_sweep(hmn_batch* b, int kind, int sweep);
+
 long long hmn_batch_launch_count(hmn_batch* b);
 int hmn_batch_sync(hmn_batch* b);
 void* hmn_batch_stream(hmn_batch* b);

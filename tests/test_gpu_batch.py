@@ -1,7 +1,7 @@
 """Batched simulations (hmn_batch_*): every simulation in a batch gives the
 same bits as the same simulation run alone, whatever else is in the batch,
-whatever tile and persistent-grid schedule, and admission follows the pool's
-free memory."""
+whatever tile, persistent-grid size and sweep schedule, and admission follows
+the pool's free memory."""
 import numpy as np
 import pytest
 
@@ -66,18 +66,37 @@ def test_batch_matches_each_simulation_alone(precision):
     b.close()
 
 
-def test_schedule_does_not_change_results():
-    sims = mix()[:4]
+SCHEDULES = (  # kind -> (tile_id, blocks_per_sm, sweep): every tile, grid size and sweep at least once
+    {0: (0, 0, 0), 1: (2, 0, 0), 2: (4, 0, 0)},
+    {0: (1, 1, 1), 1: (3, 2, 1), 2: (4, 4, 1)},
+    {0: (0, 4, 2), 1: (2, 1, 2), 2: (4, 2, 2)},
+    {0: (1, 2, 2), 1: (3, 4, 2), 2: (4, 1, 0)},
+)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_schedule_does_not_change_results(precision):
+    """Tile shape, grid size and sweep (static, interleaved, dynamic) give
+    the same bits, also when the schedule changes between steps (the work
+    list and graph are rebuilt) and over many replays of one graph (the
+    dynamic queue resets itself after every launch)."""
+    sims = mix()[:5]  # 2-D, 3-D and 1-D kinds
     outs = []
-    for sched in ({0: (0, 0), 1: (2, 0)}, {0: (1, 1), 1: (3, 2)}):
-        b = Batch(sum(footprint(c) for c, _ in sims) + (1 << 20), max_sims=8)
+    for i, sched in enumerate(SCHEDULES):
+        b = Batch(sum(footprint(c) for c, _ in sims) + (1 << 20), max_sims=8, precision=precision)
         slots = [b.add(c, p) for c, p in sims]
         autotune.apply(b, sched)
-        b.step(5)
-        outs.append([b.download(s)["u"] for s in slots])
+        b.step(2)
+        autotune.apply(b, SCHEDULES[(i + 1) % len(SCHEDULES)])
+        b.step(6)
+        t, tn, done, err = b.poll()
+        outs.append([(tn[s], t[s], b.download(s)) for s in slots])
         b.close()
-    for x, y in zip(*outs):
-        assert np.array_equal(x, y)
+    for other in outs[1:]:
+        for (tn0, t0, x), (tn1, t1, y) in zip(outs[0], other):
+            assert tn0 == tn1 and t0 == t1
+            for k in ("u", "d", "v1", "v2", "v3", "e", "b1", "b2", "b3"):
+                assert np.array_equal(x[k], y[k]), k
 
 
 def test_admission_by_footprint_and_slot_reuse():
@@ -94,11 +113,26 @@ def test_admission_by_footprint_and_slot_reuse():
     b.close()
 
 
-def test_autotuner_picks_a_valid_schedule(tmp_path):
+def test_autotuner_times_every_candidate_and_keeps_the_fastest(tmp_path):
+    import json
+
     sims = mix()[:3]
-    best = autotune.tune(sims, steps=2, cache=str(tmp_path / "tune.json"))
+    path = tmp_path / "tune.json"
+    best = autotune.tune(sims, steps=2, cache=str(path))
     assert set(best) == {1}
-    tid, g = best[1]
-    assert tid in autotune.TILE_VARIANTS[1] and g in autotune.GRID_SIZES
-    again = autotune.tune(sims, steps=2, cache=str(tmp_path / "tune.json"))  # served from the cache
+    entry = next(iter(json.loads(path.read_text()).values()))
+    timed = {tuple(c[:3]): c[3] for c in entry["candidates"]}
+    assert set(timed) == set(autotune.candidates(1))  # tiles x grid sizes x sweeps
+    assert all(ms > 0 for ms in timed.values())
+    assert timed[best[1]] == min(timed.values()) == entry["ms_per_step"]
+    again = autotune.tune(sims, steps=2, cache=str(path))  # served from the cache
     assert again == best
+    # the chosen schedule gives each simulation's own bits
+    b = Batch(sum(footprint(c) for c, _ in sims) + (1 << 20), max_sims=4)
+    slots = [b.add(c, p) for c, p in sims]
+    autotune.apply(b, best)
+    b.run_all(chunk=4)
+    for s, (c, p) in zip(slots, sims):
+        ref = alone(c, p)
+        assert np.array_equal(b.download(s)["u"], ref["u"])
+    b.close()
