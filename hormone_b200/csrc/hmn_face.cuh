@@ -69,32 +69,35 @@ __device__ __forceinline__ void slopes_with(const double* pm, const double* p0, 
 }
 
 // The slopes with IEEE division, out of line: the rare path of slopes_of.
+// Slope q goes to out[q * os].
 template <bool MAG, int LIM, int QS>
 __device__ __noinline__ void slopes_ieee(const double* pm, const double* p0, const double* pp, const AxisGeo* g,
-                                         int cg, double* out) {
+                                         int cg, double* out, int os) {
   PlainDiv pd;
   double sl[NS];
   slopes_with<MAG, LIM, QS>(pm, p0, pp, *g, cg, sl, pd);
 #pragma unroll
-  for (int q = 0; q < NS; q++) out[q] = sl[q];
+  for (int q = 0; q < NS; q++) out[q * os] = sl[q];
 }
 
 // The slopes with every quotient formed by FastDiv, recomputed with IEEE
 // division where FastDiv could not vouch for one (bitwise the same result).
 // One out-of-line copy serves every call site, so that warps in different
-// phases of the march share instruction cache lines.
+// phases of the march share instruction cache lines.  Slope q goes to
+// out[q * os]: a caller that keeps slopes in shared memory passes its slot
+// there, and nothing goes through the stack.
 template <bool MAG, int LIM, int QS>
 __device__ __noinline__ void slopes_fast(const double* pm, const double* p0, const double* pp, const AxisGeo* g,
-                                         int cg, double* out) {
+                                         int cg, double* out, int os) {
   FastDiv fd;
   double sl[NS];
   slopes_with<MAG, LIM, QS>(pm, p0, pp, *g, cg, sl, fd);
   if (fd.bad) {
-    slopes_ieee<MAG, LIM, QS>(pm, p0, pp, g, cg, out);
+    slopes_ieee<MAG, LIM, QS>(pm, p0, pp, g, cg, out, os);
     return;
   }
 #pragma unroll
-  for (int q = 0; q < NS; q++) out[q] = sl[q];
+  for (int q = 0; q < NS; q++) out[q * os] = sl[q];
 }
 template <bool MAG, int LIM, int QS>
 __device__ __forceinline__ void slopes_of(const double* pm, const double* p0, const double* pp, const AxisGeo& g,
@@ -104,9 +107,21 @@ __device__ __forceinline__ void slopes_of(const double* pm, const double* p0, co
     for (int q = 0; q < NS; q++) sl[q] = 0.0;
   } else {
     double tmp[NS];
-    slopes_fast<MAG, LIM, QS>(pm, p0, pp, &g, cg, tmp);
+    slopes_fast<MAG, LIM, QS>(pm, p0, pp, &g, cg, tmp, 1);
 #pragma unroll
     for (int q = 0; q < NS; q++) sl[q] = tmp[q];
+  }
+}
+
+// slopes_of written straight to out[q * os] (shared memory).
+template <bool MAG, int LIM, int QS>
+__device__ __forceinline__ void slopes_to(const double* pm, const double* p0, const double* pp, const AxisGeo& g,
+                                          int cg, double* out, int os) {
+  if constexpr (LIM == 0) {
+#pragma unroll
+    for (int q = 0; q < NS; q++) out[q * os] = 0.0;
+  } else {
+    slopes_fast<MAG, LIM, QS>(pm, p0, pp, &g, cg, out, os);
   }
 }
 
@@ -162,39 +177,59 @@ __device__ __forceinline__ bool face_flux_with(PL pl, PR pr, SL sl, SR sr, doubl
   return true;
 }
 
+// Store a face flux: with os == 0, fl in the solver's order to out[0..8];
+// otherwise rotated back into the conserved slots (numflux.f90:186-198,
+// 359-371, 531-543), slot v to out[v * os].
+__device__ __forceinline__ void put_flux(const double fl[9], int cn, int c1, int c2, double* out, int os) {
+  if (os == 0) {
+#pragma unroll
+    for (int q = 0; q < 9; q++) out[q] = fl[q];
+    return;
+  }
+  out[ICNT * os] = fl[0];
+  out[(IMO1 + cn) * os] = fl[1];
+  out[(IMO1 + c1) * os] = fl[2];
+  out[(IMO1 + c2) * os] = fl[3];
+  out[IENE * os] = fl[4];
+  out[(IMG1 + cn) * os] = fl[5];
+  out[(IMG1 + c1) * os] = fl[6];
+  out[(IMG1 + c2) * os] = fl[7];
+  out[I9WV * os] = fl[8];
+}
+
 // The face flux with IEEE division, out of line: the rare path of
 // face_flux.  pl/pr: staged quantity 0 of the cells (stride QS); sl/sr:
-// slope 0 (strides ssl, ssr).
+// slope 0 (strides ssl, ssr); out/os as put_flux.
 template <bool MAG, int QS>
 __device__ __noinline__ bool face_flux_ieee(const double* pl, const double* pr, const double* sl, int ssl,
                                             const double* sr, int ssr, double dx1, double dx2, int cn, int c1, int c2,
-                                            double gamma, double gm1, double ch, double* out) {
+                                            double gamma, double gm1, double ch, double* out, int os) {
   PlainDiv pd;
   double fl[9];
   const bool ok = face_flux_with<MAG>([&](int q) { return pl[q * QS]; }, [&](int q) { return pr[q * QS]; },
                                       [&](int q) { return sl[q * ssl]; }, [&](int q) { return sr[q * ssr]; }, dx1,
                                       dx2, cn, c1, c2, gamma, gm1, ch, fl, pd);
-#pragma unroll
-  for (int q = 0; q < 9; q++) out[q] = fl[q];
+  put_flux(fl, cn, c1, c2, out, os);
   return ok;
 }
 
 // The face flux with every quotient formed by FastDiv, recomputed with IEEE
 // division where FastDiv could not vouch for one (bitwise the same result);
 // one out-of-line copy for the x, y and z faces.  Arguments as
-// face_flux_ieee.
+// face_flux_ieee.  A caller that keeps fluxes in shared memory passes its
+// slot and stride, and nothing goes through the stack.
 template <bool MAG, int QS>
 __device__ __noinline__ bool face_flux_fast(const double* pl, const double* pr, const double* sl, int ssl,
                                             const double* sr, int ssr, double dx1, double dx2, int cn, int c1, int c2,
-                                            double gamma, double gm1, double ch, double* out) {
+                                            double gamma, double gm1, double ch, double* out, int os) {
   FastDiv fd;
   double fl[9];
   const bool ok = face_flux_with<MAG>([&](int q) { return pl[q * QS]; }, [&](int q) { return pr[q * QS]; },
                                       [&](int q) { return sl[q * ssl]; }, [&](int q) { return sr[q * ssr]; }, dx1,
                                       dx2, cn, c1, c2, gamma, gm1, ch, fl, fd);
-  if (fd.bad) return face_flux_ieee<MAG, QS>(pl, pr, sl, ssl, sr, ssr, dx1, dx2, cn, c1, c2, gamma, gm1, ch, out);
-#pragma unroll
-  for (int q = 0; q < 9; q++) out[q] = fl[q];
+  if (fd.bad)
+    return face_flux_ieee<MAG, QS>(pl, pr, sl, ssl, sr, ssr, dx1, dx2, cn, c1, c2, gamma, gm1, ch, out, os);
+  put_flux(fl, cn, c1, c2, out, os);
   return ok;
 }
 

@@ -160,29 +160,17 @@ __device__ __forceinline__ void cart_gravity(const GridDev& G, const StageArgs& 
 
 // z flux of the face above the column's cell (k+1/2) from the window: the
 // left state from plane k with the z slope the column keeps in SZ, the
-// right one from plane k+1 with its slope in registers.
+// right one from plane k+1 with its slope in the thread's array sr (which
+// the slope call filled in place: it is handed on, not copied).  The flux
+// lands in fz already rotated into the conserved slots (put_flux with unit
+// stride; numflux.f90:531-543).
 template <bool MAG, class MT>
 __device__ __forceinline__ bool z_face(const double* Wk, const double* Wk1, const MarchSmem<MT>& sm, int t,
-                                       const double szn[NS], const AxisGeo& gz, int k, const StageArgs& A, double ch,
+                                       const double* sr, const AxisGeo& gz, int k, const StageArgs& A, double ch,
                                        double fz[9]) {
   constexpr int QS = MT::NPL;
   const double dx1 = gz.hr[k + 2], dx2 = gz.hl[k + 3];
-  double fl[9], sr[NS];
-#pragma unroll
-  for (int q = 0; q < NS; q++) sr[q] = szn[q];
-  const bool ok =
-      face_flux_fast<MAG, QS>(Wk, Wk1, &sm.SZ[0][t], MT::NC, sr, 1, dx1, dx2, 2, 0, 1, A.gamma, A.gm1, ch, fl);
-  // rotate back into the conserved slots (numflux.f90:531-543)
-  fz[ICNT] = fl[0];
-  fz[IMO1 + 2] = fl[1];
-  fz[IMO1 + 0] = fl[2];
-  fz[IMO1 + 1] = fl[3];
-  fz[IENE] = fl[4];
-  fz[IMG1 + 2] = fl[5];
-  fz[IMG1 + 0] = fl[6];
-  fz[IMG1 + 1] = fl[7];
-  fz[I9WV] = fl[8];
-  return ok;
+  return face_flux_fast<MAG, QS>(Wk, Wk1, &sm.SZ[0][t], MT::NC, sr, 1, dx1, dx2, 2, 0, 1, A.gamma, A.gm1, ch, fz, 1);
 }
 
 // Ask for the line of p to be brought into L2 (no register, no wait).
@@ -222,8 +210,8 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
   __syncthreads();
   double szn[NS];  // the z slope of the plane above the one being finished
   if (live)
-    slopes_of<MAG, LIM, QS>(&sm.W[slot(k0 - 2)][0][orr], &sm.W[slot(k0 - 1)][0][orr], &sm.W[slot(k0)][0][orr], gz,
-                            k0 - 1, szn);
+    slopes_to<MAG, LIM, QS>(&sm.W[slot(k0 - 2)][0][orr], &sm.W[slot(k0 - 1)][0][orr], &sm.W[slot(k0)][0][orr], gz,
+                            k0 - 1, szn, 1);
   __syncthreads();
   stage_plane<MAG, GLM, MT>(G, A, sm.W[slot(k0 + 1)], k0 + 1, k0 + 1 < kend, x0, y0, T0, T1, tid, NT);
   __syncthreads();
@@ -231,8 +219,8 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
 #pragma unroll
     for (int q = 0; q < NS; q++) sm.SZ[q][tid] = szn[q];  // the slope of k0-1 is the face's left slope
     double szk[NS];
-    slopes_of<MAG, LIM, QS>(&sm.W[slot(k0 - 1)][0][orr], &sm.W[slot(k0)][0][orr], &sm.W[slot(k0 + 1)][0][orr], gz,
-                            k0, szk);
+    slopes_to<MAG, LIM, QS>(&sm.W[slot(k0 - 1)][0][orr], &sm.W[slot(k0)][0][orr], &sm.W[slot(k0 + 1)][0][orr], gz,
+                            k0, szk, 1);
     double fz[9];
     if (!z_face<MAG, MT>(&sm.W[slot(k0 - 1)][0][orr], &sm.W[slot(k0)][0][orr], sm, tid, szk, gz, k0 - 1, A, ch, fz))
       record_error(A.sc, kENEG_EINT, x0 + oi, y0 + oj, k0 - 1);
@@ -281,7 +269,7 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
     // ---- phase 1: slopes --------------------------------------------------------
     // owners: the z slope of their column, then one x-y slope cell each (the
     // last NC of the list); the other threads: the rest of the list
-    if (live) slopes_of<MAG, LIM, QS>(Wk + orr, Wk1 + orr, Wk2 + orr, gz, k + 1, szn);
+    if (live) slopes_to<MAG, LIM, QS>(Wk + orr, Wk1 + orr, Wk2 + orr, gz, k + 1, szn, 1);
     constexpr int NSO = MT::OXY ? MT::NSXY - NC : MT::NSXY;  // items the other threads take
     for (int w = owner ? (MT::OXY ? NSO + tid : MT::NSXY) : h; w < (owner ? MT::NSXY : NSO);
          w += owner ? NC : NH) {
@@ -300,10 +288,8 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
       const int r = MT::pidx(si, sj);
       const int rm = ax == 0 ? MT::pidx(si - 1, sj) : MT::pidx(si, sj - 1);
       const int rp = ax == 0 ? MT::pidx(si + 1, sj) : MT::pidx(si, sj + 1);
-      double sl[NS];
-      slopes_of<MAG, LIM, QS>(Wk + rm, Wk + r, Wk + rp, G.g[ax], ax == 0 ? x0 + si : y0 + sj, sl);
-#pragma unroll
-      for (int q = 0; q < NS; q++) sm.S[q][w] = sl[q];
+      slopes_to<MAG, LIM, QS>(Wk + rm, Wk + r, Wk + rp, G.g[ax], ax == 0 ? x0 + si : y0 + sj, &sm.S[0][w],
+                              MT::NSXY);
     }
     __syncthreads();
     // ---- phase 2: face fluxes -------------------------------------------------
@@ -339,28 +325,17 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
       const AxisGeo& g = G.g[ax];
       const double dx1 = g.hr[gL + 2], dx2 = g.hl[gL + 3];
       const int cn = ax, c1 = ax + 1, c2 = (ax + 2) % 3;
-      double fl[9];
       const double* PL = Wk + rL;
       const double* PR = Wk + rR;
       const double* SLp = &sm.S[0][sL];
       const double* SRp = &sm.S[0][sR];
       constexpr int SS = MT::NSXY;
-      if (!face_flux_fast<MAG, QS>(PL, PR, SLp, SS, SRp, SS, dx1, dx2, cn, c1, c2, A.gamma, A.gm1, ch, fl)) {
+      // the flux goes straight into its conserved slots of F (put_flux)
+      if (!face_flux_fast<MAG, QS>(PL, PR, SLp, SS, SRp, SS, dx1, dx2, cn, c1, c2, A.gamma, A.gm1, ch, &sm.F[0][w],
+                                   MT::NFXY)) {
         int gi[3] = {x0 + fi, y0 + fj, k};
         gi[ax] = gL;
         record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);
-      }
-      // rotate back into the conserved slots (numflux.f90:186-198, 359-371)
-      sm.F[ICNT][w] = fl[0];
-      sm.F[IMO1 + cn][w] = fl[1];
-      sm.F[IMO1 + c1][w] = fl[2];
-      sm.F[IMO1 + c2][w] = fl[3];
-      sm.F[IENE][w] = fl[4];
-      if (MAG) {
-        sm.F[IMG1 + cn][w] = fl[5];
-        sm.F[IMG1 + c1][w] = fl[6];
-        sm.F[IMG1 + c2][w] = fl[7];
-        if (GLM) sm.F[I9WV][w] = fl[8];
       }
     }
     double dz[9];

@@ -37,7 +37,6 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
   constexpr int cn = AX, c1 = (AX + 1) % 3, c2 = (AX + 2) % 3;
   const AxisGeo& g = G.g[AX];
   const int tid = threadIdx.x;
-  constexpr int nsl = MAG ? NS : S_B;
 
   // ---- limited slopes of the tile +-1 along AX -------------------------------
   for (int w = tid; w < NSB; w += TL::NT) {
@@ -53,13 +52,13 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
     const int rm = TL::pidx(lm[0], lm[1], lm[2]);
     const int rp = TL::pidx(lp[0], lp[1], lp[2]);
     const int cg = lc[AX] + t0[AX];  // global coordinate along AX
-    double sl[NS];
+    // the slopes go straight to their shared-memory slots (rows of S)
     if (A.limiter == 1)
-      slopes_of<MAG, 1, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, sl);
+      slopes_to<MAG, 1, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, &sm.S[0][w], TL::NSB);
     else if (A.limiter == 2)
-      slopes_of<MAG, 2, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, sl);
+      slopes_to<MAG, 2, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, &sm.S[0][w], TL::NSB);
     else
-      slopes_of<MAG, 0, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, sl);
+      slopes_to<MAG, 0, TL::NR>(&sm.P[0][rm], &sm.P[0][r], &sm.P[0][rp], g, cg, &sm.S[0][w], TL::NSB);
     // passive-scalar slopes (interpolation.f90:135-141), not zeroed by the eint check
     if constexpr (TL::SP > 0) {
       for (int n = 0; n < A.nspc; n++) {
@@ -74,8 +73,6 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
         sm.S[NS + n][w] = du;
       }
     }
-#pragma unroll
-    for (int q = 0; q < nsl; q++) sm.S[q][w] = sl[q];
   }
   __syncthreads();
 
@@ -95,24 +92,13 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
     const int gL = t0[AX] + f - 1;
     const double dx1 = g.hr[gL + 2];  // xi(i)-x(i)
     const double dx2 = g.hl[gL + 3];  // x(i+1)-xi(i)
-    double fl[9];
+    // the flux goes straight into its conserved slots of F (put_flux:
+    // numflux.f90:186-198, 359-371, 531-543)
     if (!face_flux_fast<MAG, TL::NR>(&sm.P[0][rL], &sm.P[0][rR], &sm.S[0][sL], TL::NSB, &sm.S[0][sR], TL::NSB, dx1,
-                                     dx2, cn, c1, c2, A.gamma, A.gm1, ch, fl)) {
+                                     dx2, cn, c1, c2, A.gamma, A.gm1, ch, &sm.F[0][w], TL::NFB)) {
       int gi[3] = {t0[0] + fx, t0[1] + fy, t0[2] + fz};
       gi[AX] = gL;
       record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);  // numflux.f90:117 -> error_flux
-    }
-    // rotate back into the conserved slots (numflux.f90:186-198, 359-371, 531-543)
-    sm.F[ICNT][w] = fl[0];
-    sm.F[IMO1 + cn][w] = fl[1];
-    sm.F[IMO1 + c1][w] = fl[2];
-    sm.F[IMO1 + c2][w] = fl[3];
-    sm.F[IENE][w] = fl[4];
-    if (MAG) {
-      sm.F[IMG1 + cn][w] = fl[5];
-      sm.F[IMG1 + c1][w] = fl[6];
-      sm.F[IMG1 + c2][w] = fl[7];
-      if (GLM) sm.F[I9WV][w] = fl[8];
     }
     // boundary code 10: the inner z face carries the host's flux
     // (numflux.f90:566 -> fluxboundary.f90:42-87)
@@ -138,11 +124,12 @@ __device__ __forceinline__ void axis_pass(const GridDev& G, const StageArgs& A, 
             sumr = sumr + spr[n];
           }
         }
-        const double sg = fsign(0.5, fl[0]);
+        const double f0 = sm.F[ICNT][w];  // the mass flux this thread just wrote
+        const double sg = fsign(0.5, f0);
         const double fix = 1.0 / (suml * (0.5 + sg) + sumr * (0.5 - sg));
 #pragma unroll
         for (int n = 0; n < TL::SP; n++)
-          if (n < A.nspc) sm.F[9 + n][w] = fix * fl[0] * (spl[n] * (0.5 + sg) + spr[n] * (0.5 - sg));
+          if (n < A.nspc) sm.F[9 + n][w] = fix * f0 * (spl[n] * (0.5 + sg) + spr[n] * (0.5 - sg));
       }
     }
   }
