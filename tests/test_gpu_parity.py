@@ -10,6 +10,7 @@ with margin.
 import numpy as np
 import pytest
 
+from hormone_b200 import config, grid as G, ic
 from hormone_b200.sim import Simulation
 from oracle.oracle import Oracle
 
@@ -90,6 +91,28 @@ def test_orszag_tang_3d(limiter):
 def test_orszag_tang_3d_ragged_tiles():
     cfg, prims = cases.ot3d(13)
     run_pair(cfg, prims, 4)
+
+
+def test_march_z_chunks_and_ragged_columns():
+    """MHD with GLM on a 3-D grid whose z extent splits into several march
+    chunks (three here: 16, 16 and 8 planes) over ragged 16x8 column tiles
+    (20 x 12 cells), with a state that varies along every axis and periodic,
+    reflecting and outflow faces."""
+    cfg, prims = cases.riemann3d(n=(20, 12, 40), bc=(0, 3, 1))
+    run_pair(cfg, prims, 4)
+
+
+def test_march_z_chunks_hydro():
+    """The same chunking without magnetic fields (the march's hydro form),
+    with outflow faces on every side."""
+    ov = dict(ie=24, je=9, ke=36, mag_on=False, gamma=1.4, flux_limiter="modified_mc", t_end=0.2, dt_out=0.2,
+              courant=0.4)
+    for a in (1, 2, 3):
+        for tag in ("is", "os", "iv", "ov"):
+            ov[f"bc{a}{tag}"] = 1
+    cfg = config.resolve("blast", overrides=ov)
+    prims = ic.sedov(cfg, G.make_grid(cfg), energy=1.0, radius=0.2, p0=0.05)
+    run_pair(cfg, prims, 6)
 
 
 @pytest.mark.parametrize("bc_y", [0, 1])
