@@ -29,11 +29,13 @@
 
 namespace hmn {
 
-// biased exponent of x (bits 52..62)
-__device__ __forceinline__ unsigned fexp(double x) { return ((unsigned)__double2hiint(x) >> 20) & 0x7ffu; }
-
-// |x| in [2^-500, 2^500]: biased exponent in [523, 1523]
-__device__ __forceinline__ bool fin_range(double x) { return fexp(x) - 523u <= 1000u; }
+// |x| in [2^-500, 2^500]: biased exponent in [523, 1523].  The high word
+// shifted left by one drops the sign and puts the exponent in bits 21..31,
+// so the test is one shift-add and one unsigned compare.
+__device__ __forceinline__ bool fin_range(double x) {
+  const unsigned t = (unsigned)__double2hiint(x) << 1;
+  return t - (523u << 21) < (1001u << 21);
+}
 
 // approximate reciprocal (relative error below 2^-22 or so; refined below)
 __device__ __forceinline__ double rcp_approx(double b) {
@@ -56,7 +58,9 @@ __device__ __forceinline__ double rcp_nr(double b) {
 // RN(1/b); sets bad where b is out of range or has an all-ones significand
 __device__ __forceinline__ double recip_rn(double b, bool& bad) {
   const unsigned lo = (unsigned)__double2loint(b), hi = (unsigned)__double2hiint(b);
-  bad = bad || !fin_range(b) || (lo == 0xffffffffu && (hi & 0xfffffu) == 0xfffffu);
+  // all-ones significand: the low word and the 20 significand bits of the
+  // high word are all ones
+  bad = bad || !fin_range(b) || ((hi | 0xfff00000u) & lo) == 0xffffffffu;
   double y = rcp_approx(b);
   double e = __fma_rn(-b, y, 1.0);
   y = __fma_rn(y, e, y);
