@@ -7,9 +7,9 @@
 //   phase 1: computes, per column, the z slope of plane k+1 (one owner
 //            thread per column) and the x and y limited slopes of plane k
 //            (all threads);
-//   phase 2: computes the x and y HLLD face fluxes of plane k (all threads)
-//            and, per column, the z face flux k+1/2 and the z flux difference
-//            of cell k (owners);
+//   phase 2: computes, per column, the z face flux k+1/2 and the z flux
+//            difference of cell k (owners, first), and the x and y HLLD face
+//            fluxes of plane k (all threads);
 //   phase 3: applies the RK combination, the source and the primitive
 //            recovery to cell k of every column and writes U and P (owners),
 //            while the other threads stage plane k+3 into the slot plane k
@@ -293,8 +293,24 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
     }
     __syncthreads();
     // ---- phase 2: face fluxes -------------------------------------------------
-    // owners: one x-y face each (the last NC of the list), then the z face of
-    // their column; the other threads: the rest of the list
+    // owners: first the z face of their column (its slopes are at hand, and
+    // the z flux difference is then done before the x-y face call)
+    double dz[9];
+    if (live) {
+      double fz[9];
+      if (!z_face<MAG, MT>(Wk + orr, Wk1 + orr, sm, tid, szn, gz, k, A, ch, fz))
+        record_error(A.sc, kENEG_EINT, x0 + oi, y0 + oj, k);
+      const double idz = gz.idxi[k + 2];
+#pragma unroll
+      for (int q = 0; q < 9; q++) {
+        dz[q] = idz * (sm.FZ[q][tid] - fz[q]);
+        sm.FZ[q][tid] = fz[q];
+      }
+#pragma unroll
+      for (int q = 0; q < NS; q++) sm.SZ[q][tid] = szn[q];
+    }
+    // owners, then: one x-y face each (the last NC of the list); the other
+    // threads: the rest of the list
     constexpr int NFO = MT::OXY ? MT::NFXY - NC : MT::NFXY;
     for (int w = owner ? (MT::OXY ? NFO + tid : MT::NFXY) : h; w < (owner ? MT::NFXY : NFO);
          w += owner ? NC : NH) {
@@ -337,20 +353,6 @@ __global__ void __launch_bounds__(MT::NT, MT::MINB)
         gi[ax] = gL;
         record_error(A.sc, kENEG_EINT, gi[0], gi[1], gi[2]);
       }
-    }
-    double dz[9];
-    if (live) {
-      double fz[9];
-      if (!z_face<MAG, MT>(Wk + orr, Wk1 + orr, sm, tid, szn, gz, k, A, ch, fz))
-        record_error(A.sc, kENEG_EINT, x0 + oi, y0 + oj, k);
-      const double idz = gz.idxi[k + 2];
-#pragma unroll
-      for (int q = 0; q < 9; q++) {
-        dz[q] = idz * (sm.FZ[q][tid] - fz[q]);
-        sm.FZ[q][tid] = fz[q];
-      }
-#pragma unroll
-      for (int q = 0; q < NS; q++) sm.SZ[q][tid] = szn[q];
     }
     __syncthreads();
     // ---- phase 3: cell update (owners), staging of plane k+3 (the others) -------
