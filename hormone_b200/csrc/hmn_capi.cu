@@ -1526,10 +1526,7 @@ static int run_small(hmn_ctx* ctx, int max_steps) {
       if (ctx->solve[a] && (ctx->bc[a][io][0] >= 9 || ctx->bc[a][io][1] >= 9) && !ctx->G.dir[a][io])
         return HMN_EBADCFG;  // codes 9 and 10 need hmn_set_dirichlet first
   if (ctx->solve[2] && ctx->bc[2][0][0] == 10 && !ctx->fb) return HMN_EBADCFG;
-  if (!ctx->small_bar) {
-    CK(cudaMalloc((void**)&ctx->small_bar, 2 * sizeof(unsigned int)), "barrier");
-    CK(cudaMemsetAsync(ctx->small_bar, 0, 2 * sizeof(unsigned int), ctx->st), "barrier");
-  }
+  if (!ctx->small_bar) CK(cudaMalloc((void**)&ctx->small_bar, 2 * sizeof(unsigned int)), "barrier");
   const int rk = ctx->par.rktype;
   SmallRun R;
   memset(&R, 0, sizeof(R));
@@ -1547,6 +1544,8 @@ static int run_small(hmn_ctx* ctx, int max_steps) {
     R.nsteps = left < 4096 ? left : 4096;
     const int tn_before = ctx->sc_h->tn;
     int grid = 0;
+    // the barrier's arrival counter starts every launch at zero
+    CK(cudaMemsetAsync(ctx->small_bar, 0, sizeof(unsigned int), ctx->st), "barrier");
     CK(launch_small_run(ctx->G, R, ctx->mag != 0, ctx->glm != 0, ctx->G.sph.on != 0, ctx->tile, ctx->st, &grid),
        "small run");
     ctx->launches += 1;

@@ -133,7 +133,7 @@ struct StageArgs {
 struct SmallRun {
   StageArgs st[2][3];   // [primitive buffer of the step's state][RK stage - 1]
   DevScalars* sc;
-  unsigned int* bar;    // grid barrier: arrivals, generation (zero before the first use)
+  unsigned int* bar;    // grid barrier: the arrival counter (zeroed before every launch)
   double phifac0;       // pending phidamp factor for the first step's stage 1
   double damp;          // the factor of every later step's stage 1 (1 without GLM)
   int nsteps, ntiles, rk;

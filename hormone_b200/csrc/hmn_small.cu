@@ -17,9 +17,13 @@
 // the previous phase (halos, the scalars of the dt finalisation), and an
 // SM's L1 is not coherent with the others.  This translation unit is
 // therefore compiled with -Xptxas -dlcm=cg: its global loads are cached in
-// L2 only.  The barrier is a counter and a generation word in global memory
-// with release/acquire fences; a CTA that waits longer than a second
-// records HMN_ETIMEOUT and the launch returns.
+// L2 only.  The barrier is one arrival counter in global memory, zeroed by
+// the host before every launch and never reset inside it: a CTA's n-th
+// barrier (n from 0) is passed once the counter reaches (n + 1) x the grid,
+// so the last CTA to arrive learns from its own atomic that it need not
+// wait, and the others see that count on their next poll.  Release and
+// acquire fences order the phases' memory; a CTA that waits longer than a
+// second records HMN_ETIMEOUT and the launch returns.
 #include <cuda_runtime.h>
 
 #include "hmn_internal.h"
@@ -30,23 +34,20 @@ namespace {
 
 constexpr unsigned long long kBarrierWaitNs = 1000000000ull;
 
-// All CTAs of the launch meet here; false (with HMN_ETIMEOUT recorded) if
-// the others did not arrive within kBarrierWaitNs.
-__device__ __forceinline__ bool grid_sync(unsigned int* bar, DevScalars* sc) {
+// All CTAs of the launch meet here for the nb-th time (nb counts this CTA's
+// barriers from 0 and is advanced here); false (with HMN_ETIMEOUT recorded)
+// if the others did not arrive within kBarrierWaitNs.
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, DevScalars* sc, unsigned int& nb) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* gen = bar + 1;
-    const unsigned int g = *gen;
-    __threadfence();
+    const unsigned int target = (nb + 1u) * gridDim.x;
+    __threadfence();  // this CTA's writes before its arrival
     int good = 1;
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
+    if (atomicAdd(bar, 1u) + 1u != target) {
+      volatile unsigned int* cnt = bar;
       const unsigned long long t0 = global_ns();
-      while (*gen == g) {
+      while (*cnt < target) {
         if (global_ns() - t0 > kBarrierWaitNs) {
           record_error(sc, kETIMEOUT, -1, -1, -1);
           good = 0;
@@ -54,10 +55,11 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, DevScalars* sc) {
         }
       }
     }
-    __threadfence();
+    __threadfence();  // the others' writes before this CTA's next reads
     ok = good;
   }
   __syncthreads();
+  nb++;
   return ok != 0;
 }
 
@@ -74,6 +76,7 @@ __global__ void __launch_bounds__(TL::NT, 1)
   SmemT<TL>& sm = *reinterpret_cast<SmemT<TL>*>(smem_raw);
   DevScalars* sc = R.sc;
   if (*(volatile int*)&sc->done) return;
+  unsigned int nb = 0;  // barriers passed (the same count in every CTA)
   {  // CFL reduction and dt of the state entering the first step (cfl_kernel, cfl_finalize_kernel)
     const StageArgs& A0 = R.st[0][0];
     double my_dti = __longlong_as_double(0x7ff0000000000000LL), my_cf = 0.0;
@@ -89,9 +92,9 @@ __global__ void __launch_bounds__(TL::NT, 1)
     }
     cfl_block_reduce(my_dti, my_cf, sc);
   }
-  if (!grid_sync(R.bar, sc)) return;
+  if (!grid_sync(R.bar, sc, nb)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) finalize_dt(sc);
-  if (!grid_sync(R.bar, sc)) return;
+  if (!grid_sync(R.bar, sc, nb)) return;
   int par = 0;
   for (int step = 0; step < R.nsteps; step++) {
     // the fused RK stages (stage_kernel); the last one also reduces the
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(TL::NT, 1)
         }
         cfl_block_reduce(my_dti, my_cf, sc);
       }
-      if (!grid_sync(R.bar, sc)) return;
+      if (!grid_sync(R.bar, sc, nb)) return;
     }
     // the time advance (advance_kernel) and, while the run goes on, the next
     // step's dt from the reduction above (cfl_finalize_kernel)
@@ -125,7 +128,7 @@ __global__ void __launch_bounds__(TL::NT, 1)
       else
         finalize_dt(sc);
     }
-    if (!grid_sync(R.bar, sc)) return;
+    if (!grid_sync(R.bar, sc, nb)) return;
     if (*(volatile int*)&sc->done) return;  // every CTA reads it after the same barrier
     par ^= R.rk & 1;  // an odd number of stages leaves the state in the other primitive buffer
   }
