@@ -52,6 +52,8 @@ def parse():
                          "one at a time; serve: a Poisson request stream through the continuous-batching server; "
                          "polytrope: 192^3 self-gravitating polytrope with hyperbolic gravity")
     ap.add_argument("--boxes", type=int, default=512)
+    ap.add_argument("--schedule", default="",
+                    help="kh-batch: TILE,GRID,SWEEP for the 2-D kind instead of the autotuner's choice")
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--policy", choices=["fifo", "sjf", "priority"], default="priority",
@@ -624,7 +626,10 @@ def run_kh_batch(args, rank=0, world=1, local_rank=0):
     boxes = [(c, ic.kelvin_helmholtz(c, G.make_grid(c), r, b)) for i, (c, r, b) in enumerate(boxes) if i in set(mine)]
     cells = sum(int(np.prod(c["n"])) for c, _ in boxes)
     K = args.steps
-    sched = autotune.tune(boxes[:32], precision=args.precision, steps=2, cache=None)
+    if args.schedule:
+        sched = {1: tuple(int(x) for x in args.schedule.split(","))}
+    else:
+        sched = autotune.tune(boxes[:32], precision=args.precision, steps=2, cache=None)
     b = Batch(sum(footprint(c) for c, _ in boxes) + (1 << 26), max_sims=len(boxes) + 1, precision=args.precision)
     for c, p in boxes:
         assert b.add(c, p) is not None
