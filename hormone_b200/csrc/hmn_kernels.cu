@@ -305,12 +305,12 @@ cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool gl
   }
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_stage_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
   if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_stage_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, tm, st);
-  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_stage_tl<Tile<16, 16, 1, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_stage_tl<Tile<16, 1, 16, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_stage_tl<Tile<1, 16, 16, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_stage_tl<Tile<256, 1, 1, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_stage_tl<Tile<1, 256, 1, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_stage_tl<Tile<1, 1, 256, 288, 3>>(G, A, mag, glm, nullptr, st);
   return cudaErrorInvalidValue;
 }
 
@@ -472,9 +472,9 @@ cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
 
 using T3D = Tile<8, 8, 8, 640, 1>;
 using T3D4 = Tile<8, 8, 4, 384, 2>;
-using T2D = Tile<16, 16, 1, 288, 2>;
+using T2D = Tile<16, 16, 1, 288, 3>;
 using T2D8 = Tile<32, 8, 1, 320, 2>;
-using T1D = Tile<256, 1, 1, 288, 2>;
+using T1D = Tile<256, 1, 1, 288, 3>;
 
 // tile ids: 0 3-D 8x8x8 (640 threads), 1 3-D 8x8x4 (256 threads, 2 CTAs/SM),
 // 2 2-D 16x16, 3 2-D 32x8, 4 1-D 256.  batch_tile_kind gives the grid's

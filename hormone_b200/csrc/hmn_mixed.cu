@@ -507,12 +507,12 @@ cudaError_t launch_stage_mixed(const GridDev& G, const StageArgs& A, bool mag, b
   const int* t = A.tile;
   if (t[0] == 8 && t[1] == 8 && t[2] == 8) return launch_mixed_tl<Tile<8, 8, 8, 640, 1>>(G, A, mag, glm, tm, st);
   if (t[0] == 8 && t[1] == 8 && t[2] == 4) return launch_mixed_tl<Tile<8, 8, 4, 384, 2>>(G, A, mag, glm, tm, st);
-  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_mixed_tl<Tile<16, 16, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_mixed_tl<Tile<16, 1, 16, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_mixed_tl<Tile<1, 16, 16, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_mixed_tl<Tile<256, 1, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_mixed_tl<Tile<1, 256, 1, 288, 2>>(G, A, mag, glm, nullptr, st);
-  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_mixed_tl<Tile<1, 1, 256, 288, 2>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 16 && t[2] == 1) return launch_mixed_tl<Tile<16, 16, 1, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 16 && t[1] == 1 && t[2] == 16) return launch_mixed_tl<Tile<16, 1, 16, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 16 && t[2] == 16) return launch_mixed_tl<Tile<1, 16, 16, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 256 && t[1] == 1 && t[2] == 1) return launch_mixed_tl<Tile<256, 1, 1, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 256 && t[2] == 1) return launch_mixed_tl<Tile<1, 256, 1, 288, 3>>(G, A, mag, glm, nullptr, st);
+  if (t[0] == 1 && t[1] == 1 && t[2] == 256) return launch_mixed_tl<Tile<1, 1, 256, 288, 3>>(G, A, mag, glm, nullptr, st);
   return cudaErrorInvalidValue;
 }
 
@@ -535,9 +535,9 @@ __global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel_mixed(Sim
 
 using M3D = Tile<8, 8, 8, 640, 1>;
 using M3D4 = Tile<8, 8, 4, 384, 2>;
-using M2D = Tile<16, 16, 1, 288, 2>;
+using M2D = Tile<16, 16, 1, 288, 3>;
 using M2D8 = Tile<32, 8, 1, 320, 2>;
-using M1D = Tile<256, 1, 1, 288, 2>;
+using M1D = Tile<256, 1, 1, 288, 3>;
 
 template <bool MAG, bool GLM, class TL>
 static cudaError_t bm_attr_t() {
