@@ -473,7 +473,7 @@ cudaError_t launch_advance(DevScalars* sc, cudaStream_t st) {
 using T3D = Tile<8, 8, 8, 640, 1>;
 using T3D4 = Tile<8, 8, 4, 384, 2>;
 using T2D = Tile<16, 16, 1, 288, 3>;
-using T2D8 = Tile<32, 8, 1, 320, 2>;
+using T2D8 = Tile<32, 8, 1, 320, 3>;
 using T1D = Tile<256, 1, 1, 288, 3>;
 
 // tile ids: 0 3-D 8x8x8 (640 threads), 1 3-D 8x8x4 (256 threads, 2 CTAs/SM),

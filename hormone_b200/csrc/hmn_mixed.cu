@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(TL::NT, TL::MINB) batch_stage_kernel_mixed(Sim
 using M3D = Tile<8, 8, 8, 640, 1>;
 using M3D4 = Tile<8, 8, 4, 384, 2>;
 using M2D = Tile<16, 16, 1, 288, 3>;
-using M2D8 = Tile<32, 8, 1, 320, 2>;
+using M2D8 = Tile<32, 8, 1, 320, 3>;
 using M1D = Tile<256, 1, 1, 288, 3>;
 
 template <bool MAG, bool GLM, class TL>
