@@ -165,6 +165,14 @@ static void setup_tma(hmn_ctx* ctx) {
   ctx->tma_ok = ok ? 1 : 0;
 }
 
+// the stage tile of this grid (stage_tile), again once the coordinate
+// system is known: spherical grids take the smaller 3-D tile
+static void retile(hmn_ctx* ctx) {
+  stage_tile(ctx->solve, ctx->par.precision, ctx->par.nspc, ctx->tile, ctx->G.sph.on && ctx->G.sph.crd == 2);
+  for (int a = 0; a < 3; a++) ctx->tiles[a] = (ctx->n[a] + ctx->tile[a] - 1) / ctx->tile[a];
+  setup_tma(ctx);
+}
+
 static size_t ghosted_index(const hmn_ctx* c, int i, int j, int k) {
   const int g = c->ghost;
   const size_t sx = (size_t)c->n[0] + 2 * g, sy = (size_t)c->n[1] + 2 * g;
@@ -633,6 +641,7 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
   drop_run_graph(ctx);
   if (crdnt == 0) {
     ctx->G.sph = SphGeo{};
+    retile(ctx);
     return HMN_OK;
   }
   if (crdnt == 1) return set_cylindrical(ctx, mt);
@@ -689,6 +698,7 @@ extern "C" int hmn_set_metric(hmn_ctx* ctx, int crdnt, const hmn_metric* mt) {
   M.fac_k = ctx->n[2] == 1 ? 4.0 : 1.0;
   M.crd = 2;
   M.on = 1;
+  retile(ctx);
   cudaFree(ctx->sincbuf);  // the angular-momentum weights of hmn_evo
   ctx->sincbuf = nullptr;
   if (mt->sinc) {

@@ -191,7 +191,7 @@ enum : int { kOK = 0, kEINVAL = -1, kENEG_EINT = -2, kECUDA = -3, kEBADCFG = -4,
 
 namespace hmn {
 // launchers (hmn_kernels.cu)
-void stage_tile(const int solve[3], int precision, int nspc, int tile[3]);
+void stage_tile(const int solve[3], int precision, int nspc, int tile[3], bool sph = false);
 // tm: tensor maps of A.pin for TMA staging (3-D tiles; nullptr stages with plain loads)
 cudaError_t launch_stage(const GridDev& G, const StageArgs& A, bool mag, bool glm, const TmaMaps* tm,
                          cudaStream_t st);

@@ -217,7 +217,7 @@ static cudaError_t launch_stage_tl(const GridDev& G, const StageArgs& A, bool ma
 // SM) and 8x8x4 for the mixed form (two CTAs per SM), either one forced by
 // HMN_TILE3D=888 or 884, and 8x8x4 whenever there are passive scalars;
 // 2-D 16x16, 1-D 256
-void stage_tile(const int solve[3], int precision, int nspc, int tile[3]) {
+void stage_tile(const int solve[3], int precision, int nspc, int tile[3], bool sph) {
   const int dim = solve[0] + solve[1] + solve[2];
   for (int a = 0; a < 3; a++) tile[a] = 1;
   if (dim == 3 && nspc > 0) {  // the scalar planes only fit the smaller tile
@@ -225,8 +225,12 @@ void stage_tile(const int solve[3], int precision, int nspc, int tile[3]) {
     tile[1] = 8;
     tile[2] = 4;
   } else if (dim == 3) {
+    // 8x8x4 (two CTAs of 384 threads per SM) for the mixed form and for
+    // spherical grids (the 160x80x160 polytrope: 467 against 442 M
+    // zone-updates/s with 8x8x8); 8x8x8 for the FP64 tile otherwise, which
+    // 3-D Cartesian grids only use with the march switched off
     const char* env = getenv("HMN_TILE3D");
-    bool t884 = precision == 1;
+    bool t884 = precision == 1 || sph;
     if (env && env[0] == '8' && env[1] == '8' && (env[2] == '4' || env[2] == '8')) t884 = env[2] == '4';
     tile[0] = 8;
     tile[1] = 8;
